@@ -1,0 +1,150 @@
+/* inspire_b200.h -- C ABI of the B200-native InsPIRe PIR server.
+ *
+ * Part 1 is the server half of the reference's C ABI (SoraSuegami/InsPIRe-GPU
+ * src/capi.h:23-91), same names, same struct layouts, same flat array layouts
+ * and the same return codes, so an FFI consumer that linked the reference's
+ * GPU library links this one instead.  The client half of that header
+ * (ipir_query_build, ipir_extract, packing, compression) stays in the
+ * reference's CPU library and is not defined here.
+ *
+ * Part 2 holds additive entry points (prefix ipir_b200_) that the reference
+ * does not have: explicit streams, a device-resident staged pipeline, stage
+ * timers, precomp export, and the GPU primitives for parity checks.
+ *
+ * Values are residues mod the two 27-bit primes q0 = 94519297 and
+ * q1 = 95293441 carried in u64 (u32 for GPU-side primitives).  One server
+ * handle is single-threaded; distinct handles are independent.  No entry
+ * point aborts the process: CUDA failures come back as error codes, with
+ * the text in ipir_b200_last_error().
+ */
+#ifndef INSPIRE_B200_H
+#define INSPIRE_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ===================================================== part 1: server half */
+
+/* Opaque handle (reference src/capi.h:23). */
+typedef struct ipir_server ipir_server;
+
+/* Public parameters (reference src/capi.h:27-38). */
+typedef struct {
+    size_t n_entries;
+    size_t entry_bytes;
+    size_t db_rows;
+    size_t db_cols;
+    size_t n_packed;
+    size_t interp_d;
+    size_t num_cts;
+    size_t ring_n;
+    size_t d_eff;
+    uint8_t seed[64];
+} ipir_params;
+
+/* Capability report (reference src/capi.h:40-45). */
+typedef struct {
+    size_t max_batch;
+    size_t resident_bytes;
+    size_t device_free_bytes;
+    size_t num_cts;
+} ipir_caps;
+
+/* One query as views into caller-owned u64 arrays (reference src/capi.h:47-61):
+ *   lwe_b_limb0/1     db_rows values (mod q0 / q1)
+ *   ksk5_b, kskneg1_b d_eff*2*ring_n values, [digit][limb][coeff], coefficient form
+ *   rgsw              4*d_eff*2*ring_n values,
+ *                     [top_a | top_b | bot_a | bot_b][digit][limb][coeff], NTT form */
+typedef struct {
+    const uint64_t* lwe_b_limb0;
+    const uint64_t* lwe_b_limb1;
+    const uint64_t* ksk5_b;
+    const uint64_t* kskneg1_b;
+    const uint64_t* rgsw;
+} ipir_query_view;
+
+/* Build a server for one database generation (replaces reference
+ * src/capi.h:76-80 / src/capi.cu:51-87).  db: db_rows*db_cols u16 values in
+ * [0, 65535), row-major.  db_rows_or_zero == 0 picks db_rows = 32768.
+ * crs_seed_or_null: 64-byte CRS seed or NULL for a fresh one.  Returns NULL
+ * on error (bad geometry, CUDA failure, out of memory). */
+ipir_server* ipir_server_create(size_t n_entries, size_t entry_bytes, size_t db_rows_or_zero,
+                                size_t max_batch, const uint16_t* db, const uint8_t* crs_seed_or_null,
+                                ipir_params* out_params);
+
+/* Reference src/capi.h:82 / src/capi.cu:89-96. */
+void ipir_server_caps(const ipir_server* srv, ipir_caps* out);
+
+/* Answer count <= max_batch queries (reference src/capi.h:84-89 /
+ * src/capi.cu:98-126).  out_resp: count*num_cts*4*ring_n u64,
+ * [query][ct][a | b][limb][coeff], NTT form.  Returns 0 on success, 1 null
+ * argument, 2 count > max_batch, 3 null view field (nothing written on 1-3),
+ * 4 CUDA failure (the reference exits the process instead). */
+int ipir_answer_batch(ipir_server* srv, const ipir_query_view* queries, size_t count, uint64_t* out_resp);
+
+/* Reference src/capi.h:91. */
+void ipir_server_destroy(ipir_server* srv);
+
+/* ===================================================== part 2: additive */
+
+/* Text of the calling thread's last failure ("" if none). */
+const char* ipir_b200_last_error(void);
+
+/* Geometry exactly as the reference's setup() (src/params.cpp:23-68) plus
+ * this server's layout checks; seed left zero.  Returns 0, or nonzero when
+ * the geometry is rejected (text in ipir_b200_last_error). */
+int ipir_b200_setup(size_t n_entries, size_t entry_bytes, size_t db_rows_or_zero, ipir_params* out);
+
+/* Run this handle's work on the caller's CUDA stream (cudaStream_t cast to
+ * void*; NULL restores the handle's own stream). */
+int ipir_b200_set_stream(ipir_server* srv, void* cuda_stream);
+
+/* Device-resident pipeline split in three: stage copies count queries into
+ * the device slots (async on the handle's stream); run launches the answer
+ * kernels on the staged slots; fetch copies the responses (same layout as
+ * ipir_answer_batch) to the host and synchronises.  Return codes as
+ * ipir_answer_batch. */
+int ipir_b200_stage_queries(ipir_server* srv, const ipir_query_view* queries, size_t count);
+int ipir_b200_run(ipir_server* srv, size_t count);
+int ipir_b200_fetch_responses(ipir_server* srv, size_t count, uint64_t* out_resp);
+int ipir_b200_sync(ipir_server* srv);
+
+/* Stage timers (CUDA events on the handle's stream), off by default.
+ * stage_times writes up to n floats (ms) of the last run:
+ * [qprep, matvec, collapse, finalize, horner]. */
+int ipir_b200_enable_stage_timing(ipir_server* srv, int on);
+int ipir_b200_stage_times(const ipir_server* srv, float* ms_out, size_t n);
+
+/* Copy one group's precomputed tensors to the host (u32, NTT form, the
+ * reference's per-group layouts, src/protocol.h:14-17):
+ *   a [limb][N], d_plus / d_minus [limb][step<1023][digit][N],
+ *   d_final [limb][digit][N].  Any pointer may be NULL. */
+int ipir_b200_export_precomp(const ipir_server* srv, size_t group, uint32_t* a, uint32_t* d_plus,
+                             uint32_t* d_minus, uint32_t* d_final);
+/* Copy rows [row0, row0+nrows) of the encoded device DB to the host. */
+int ipir_b200_export_db(const ipir_server* srv, size_t row0, size_t nrows, uint16_t* out);
+
+/* GPU primitives on host buffers (current device), the kernels the server
+ * runs.  ntt: in-place forward (inverse = 0) or inverse NTT of n polys of
+ * 2048 residues; poly i is mod q_((i / limb_run) & 1).  decomp: n polys
+ * [i][limb][2048] coefficient form -> [i][digit][limb][2048] (reference
+ * src/ring.cpp:205-246, digits 1..2 of base 2^18). */
+int ipir_b200_ntt(uint32_t* polys, size_t n, int limb_run, int inverse);
+int ipir_b200_decomp(const uint32_t* in, uint32_t* out, size_t n);
+
+/* Host SHAKE-256 and the CRS expand_seed of reference src/ring.cpp:252-279
+ * (out: [limb][2048] u32). */
+int ipir_b200_shake256(const uint8_t* in, size_t inlen, uint8_t* out, size_t outlen);
+int ipir_b200_expand_seed(const uint8_t* seed64, const char* domain, uint64_t index, uint32_t* out);
+
+/* Synthetic database for benchmarks and tests: out[k] = splitmix64(seed ^ k)
+ * mod 65535 for k < count, filled on all host threads. */
+int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INSPIRE_B200_H */

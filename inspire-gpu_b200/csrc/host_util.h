@@ -1,0 +1,34 @@
+// host_util.h -- host helpers shared by the server's C++ and C entry points.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include "ipb_common.cuh"
+
+namespace ipb {
+
+constexpr size_t kSeedBytes = 64;
+constexpr size_t kDefaultDbRows = 32768;  // src/params.cpp:17-21
+constexpr size_t kDmax = 256;             // src/params.cpp:10
+constexpr size_t kPBits = 15;
+
+// Public parameters, field for field the reference's PublicParams
+// (src/params.h:49-58).
+struct Params {
+    size_t n_entries;
+    size_t w;
+    size_t db_rows;
+    size_t db_cols;
+    size_t n_packed;
+    size_t D;
+    size_t num_cts;
+    uint8_t seed[kSeedBytes];
+};
+
+void shake256(const uint8_t* in, size_t inlen, uint8_t* out, size_t outlen);
+void expand_seed(const uint8_t seed[kSeedBytes], const char* domain, uint64_t index, uint32_t* out);
+void build_tables(DevTables& T);
+// 0 on success; otherwise an error code and *why (static string).
+int setup_geometry(size_t n_entries, size_t w, size_t db_rows, Params* out, const char** why);
+
+}  // namespace ipb

@@ -1,0 +1,77 @@
+// ipb_launch.h -- host-side launch wrappers for the server's CUDA kernels.
+// Every wrapper enqueues on the given stream and returns the launch status;
+// none of them synchronises or allocates.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ipb {
+
+struct DevTables;
+
+// ---------------------------------------------------------------- online
+// Flat per-query device input (u64, the capi.h flat query layout):
+//   [b0: rows][b1: rows][ksk5: blk][kskneg1: blk][rgsw: 4 blk],  blk = 2*2*N.
+// qprep: keys [q][key(2)][limb][digit][N] NTT form, rgsw32 [q][4][digit][limb][N].
+cudaError_t launch_qprep(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
+                         uint32_t* keys, uint32_t* rgsw32, int nq, cudaStream_t s);
+
+// Mat-vec row-split partials part[q][chunk][limb][cols] for nq <= 4 queries
+// sharing one DB stream.  chunks must divide rows.
+cudaError_t launch_matvec(const uint16_t* db, size_t rows, size_t cols, int chunks,
+                          const uint64_t* qraw, size_t qstride, const DevTables* T,
+                          uint32_t* part, size_t part_qstride, int nq, cudaStream_t s);
+
+// Tensor pass: cpart[q][g][chunk][limb][N] = sum over the chunk's
+// (direction, step) units of D (.) K5[perm].  nq <= 8 queries share the stream.
+cudaError_t launch_collapse(const uint32_t* dp, const uint32_t* dm, size_t groups,
+                            const uint32_t* keys, size_t key_qstride, int nchunks,
+                            uint32_t* cpart, size_t cpart_qstride, int nq, const DevTables* T,
+                            cudaStream_t s);
+
+// packed_b[q][g][limb][N] = NTT(sum_y mvpart) - sum_ch cpart - Dfinal (.) Kn1.
+cudaError_t launch_finalize(const uint32_t* mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
+                            const uint32_t* cpart, size_t cpart_qstride, int cchunks,
+                            const uint32_t* df, const uint32_t* keys, size_t key_qstride,
+                            const DevTables* T, uint32_t* packed_b, size_t pb_qstride,
+                            size_t groups, int nq, cudaStream_t s);
+
+// Horner chains, one CTA per (ct, query): resp[q][ct][a|b][limb][N] u64.
+cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
+                          const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
+                          size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s);
+
+// ---------------------------------------------------------------- preprocess
+// Encode pass over the rows [0, nrows) of a chunk: levels [l0, l0+nl) of the
+// inverse DFT over Z_P[X]/(X^N+1) across each ct-block of d_act polys.
+// first: source is `src` (raw, gathered in bit-reversed order) else in place.
+cudaError_t launch_encode_pass(const uint16_t* src, uint16_t* dst, size_t nrows, size_t cols,
+                               size_t d_act, int logd, int l0, int nl, bool first, bool last,
+                               uint32_t d_inv, cudaStream_t s);
+
+// a-side for group g: V[limb][p][j] = N^-1 * (sum_r NTT(col_j,r) (.) crs_r)[N-1-p].
+cudaError_t launch_a_side(const uint16_t* db, size_t rows, size_t cols, size_t g,
+                          const uint32_t* crs, const DevTables* T, uint32_t* V, cudaStream_t s);
+// Column NTTs: T[limb][p][m] = NTT_j(V[limb][p][j])[m].
+cudaError_t launch_col_ntt(const uint32_t* V, const DevTables* T, uint32_t* Tout, cudaStream_t s);
+// a_post[k][dir][limb][i] = T[limb][perm_{+-5^k}(i)][i].
+cudaError_t launch_embed_gather(const uint32_t* Tin, uint32_t* a_post, cudaStream_t s);
+// CollapseA chains for groups [0, ngroups): one CTA per (group, direction).
+cudaError_t launch_collapse_a(const uint32_t* a_post, size_t ap_gstride, const uint32_t* k5,
+                              const DevTables* T, uint32_t* dp, uint32_t* dm, uint32_t* ends,
+                              size_t ngroups, cudaStream_t s);
+// Final CollapseOne per group -> D_final, a.
+cudaError_t launch_collapse_final(const uint32_t* ends, const uint32_t* kn1, const DevTables* T,
+                                  uint32_t* df, uint32_t* pre_a, size_t ngroups, cudaStream_t s);
+
+// ---------------------------------------------------------------- primitives
+// In-place forward/inverse NTT of n polys of N u32 (< q); limb of poly i is
+// (i / limb_run) & 1.
+cudaError_t launch_ntt_batch(uint32_t* polys, size_t n, int limb_run, bool inverse,
+                             const DevTables* T, cudaStream_t s);
+// Gadget decomposition of n polys: in [i][limb][N] coeff form -> out [i][digit][limb][N].
+cudaError_t launch_decomp(const uint32_t* in, uint32_t* out, size_t n, const DevTables* T,
+                          cudaStream_t s);
+
+}  // namespace ipb

@@ -1,0 +1,511 @@
+// online.cu -- per-query kernels of the B200 InsPIRe server.
+//
+// One answer (gpu_answer / gpu_answer_batch, reference src/gpu_protocol.cu:
+// 1121-1535) runs five launches on one stream:
+//   qprep     key-switching keys to NTT form, RGSW to u32 residues
+//   matvec    r_l[j] = sum_i db[i][j] * b_l[i] mod q_l   (DB pass, HBM bound)
+//   collapse  tensor pass: sum_{dir,s,j} D[s][j][i] * K5[j][perm_s(i)]
+//   finalize  per group: NTT(r slice) - tensor partials - D_final (.) Kneg1
+//   horner    one persistent CTA per response ciphertext runs the whole
+//             ExtProd chain (INTT, decomp, NTT, MAC) in shared memory
+// All arithmetic is exact mod q_l, so every output equals the reference's.
+#include "ipb_common.cuh"
+#include "ipb_launch.h"
+
+namespace ipb {
+
+namespace {
+
+__device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
+    uint32_t r = 1, b = 5;
+    while (e) {
+        if (e & 1) r = (r * b) & (2 * kN - 1);
+        b = (b * b) & (2 * kN - 1);
+        e >>= 1;
+    }
+    return r;
+}
+constexpr uint32_t kInv5 = 3277;  // 5^-1 mod 2N (5 * 3277 = 4*4096 + 1)
+
+__device__ __forceinline__ void ld8(const uint32_t* p, uint32_t (&v)[8]) {
+    uint4 a = *reinterpret_cast<const uint4*>(p);
+    uint4 b = *reinterpret_cast<const uint4*>(p + 4);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void st8(uint32_t* p, const uint32_t (&v)[8]) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(v[0], v[1], v[2], v[3]);
+    *reinterpret_cast<uint4*>(p + 4) = make_uint4(v[4], v[5], v[6], v[7]);
+}
+
+// ------------------------------------------------------------------ qprep
+// grid (nq, 12): y < 8 -> one key poly NTT (key, digit, limb); y >= 8 -> a
+// quarter of the RGSW u64 -> u32 reduction.  The client sends KSK b-parts in
+// coefficient form and RGSW in NTT form (capi.h:47-54); the reference NTTs the
+// keys on the server (src/gpu_protocol.cu:1059-1094).  Inputs are reduced
+// mod q (identical to the reference on canonical inputs).
+__global__ void __launch_bounds__(256) qprep_kernel(const uint64_t* __restrict__ qraw, size_t qstride,
+                                                    size_t rows, const DevTables* __restrict__ T,
+                                                    uint32_t* __restrict__ keys,
+                                                    uint32_t* __restrict__ rgsw32) {
+    __shared__ __align__(16) uint32_t sbuf[2 * kN];
+    const int b = blockIdx.x, y = blockIdx.y;
+    const uint32_t t = threadIdx.x;
+    const uint64_t* qr = qraw + (size_t)b * qstride;
+    const size_t blk = (size_t)kDeff * 2 * kN;
+    if (y < 8) {
+        const int key = y >> 2, j = (y >> 1) & 1, l = y & 1;
+        const LimbTables& L = T->limb[l];
+        const uint64_t* src = qr + 2 * rows + key * blk + (size_t)(j * 2 + l) * kN;
+        uint32_t r[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) r[e] = mod_u64(src[t + 256 * e], L.cr, L.q);
+        ntt_fwd(r, sbuf, L.fwd, L.q, t, 0);
+        uint32_t* dst = keys + (size_t)b * (4 * kDeff * kN) + (size_t)((key * 2 + l) * kDeff + j) * kN;
+        st8(dst + 8 * t, r);
+    } else {
+        const uint64_t* src = qr + 2 * rows + 2 * blk;
+        uint32_t* dst = rgsw32 + (size_t)b * 4 * blk;
+        const size_t q4 = blk;  // 4*blk elements split over 4 CTAs
+        for (size_t i = (size_t)(y - 8) * q4 + t; i < (size_t)(y - 7) * q4; i += 256) {
+            const int l = (int)((i / kN) & 1);
+            dst[i] = mod_u64(src[i], T->limb[l].cr, T->limb[l].q);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ matvec
+// Row-split dual-limb mat-vec.  CTA (x, y): columns [x*256*CPT, +256*CPT),
+// rows [y*rpc, +rpc).  Each thread streams CPT u16 columns with one 16- or
+// 8-byte load per row and keeps 2*BT*CPT u64 accumulators; the query words
+// of the chunk are reduced mod q once into shared memory.  Products are
+// < 2^43, so rpc <= 2^20 rows need no intermediate reduction.
+template <int BT, int CPT>
+__global__ void __launch_bounds__(256) matvec_kernel(const uint16_t* __restrict__ db, size_t rows, size_t cols,
+                                                     int rpc, const uint64_t* __restrict__ qraw, size_t qstride,
+                                                     const DevTables* __restrict__ T, uint32_t* __restrict__ part,
+                                                     size_t part_qstride, int nq) {
+    extern __shared__ __align__(16) uint32_t sb[];  // [BT][2][rpc]
+    const int chunk = blockIdx.y;
+    const size_t r0 = (size_t)chunk * rpc;
+    for (int b = 0; b < BT; ++b) {
+        const int src = b < nq ? b : 0;
+        for (int l = 0; l < 2; ++l) {
+            const uint64_t* qb = qraw + (size_t)src * qstride + (size_t)l * rows + r0;
+            for (int i = threadIdx.x; i < rpc; i += 256)
+                sb[(b * 2 + l) * rpc + i] = mod_u64(qb[i], T->limb[l].cr, T->limb[l].q);
+        }
+    }
+    __syncthreads();
+    const size_t col0 = ((size_t)blockIdx.x * 256 + threadIdx.x) * CPT;
+    uint64_t acc[BT][2][CPT];
+#pragma unroll
+    for (int b = 0; b < BT; ++b)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) { acc[b][0][c] = 0; acc[b][1][c] = 0; }
+    const uint16_t* p = db + r0 * cols + col0;
+#pragma unroll 4
+    for (int i = 0; i < rpc; ++i) {
+        uint32_t w[CPT / 2];
+        if (CPT == 8) {
+            uint4 v = __ldcs(reinterpret_cast<const uint4*>(p + (size_t)i * cols));
+            w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+        } else {
+            uint2 v = __ldcs(reinterpret_cast<const uint2*>(p + (size_t)i * cols));
+            w[0] = v.x; w[1] = v.y;
+        }
+#pragma unroll
+        for (int b = 0; b < BT; ++b) {
+            const uint32_t b0 = sb[(b * 2 + 0) * rpc + i];
+            const uint32_t b1 = sb[(b * 2 + 1) * rpc + i];
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+                const uint32_t d = (c & 1) ? (w[c >> 1] >> 16) : (w[c >> 1] & 0xFFFFu);
+                acc[b][0][c] += (uint64_t)d * b0;
+                acc[b][1][c] += (uint64_t)d * b1;
+            }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < BT; ++b) {
+        if (b >= nq) break;
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            uint32_t o[CPT];
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) o[c] = mod_u64(acc[b][l][c], T->limb[l].cr, T->limb[l].q);
+            uint32_t* dst = part + (size_t)b * part_qstride + ((size_t)chunk * 2 + l) * cols + col0;
+            if (CPT == 8) {
+                *reinterpret_cast<uint4*>(dst) = make_uint4(o[0], o[1], o[2], o[3]);
+                *reinterpret_cast<uint4*>(dst + 4) = make_uint4(o[4 % CPT], o[5 % CPT], o[6 % CPT], o[7 % CPT]);
+            } else {
+                *reinterpret_cast<uint4*>(dst) = make_uint4(o[0], o[1], o[2], o[3]);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ collapse
+// Tensor pass (InspiRINGOnline, reference src/gpu_online.cu:593-714): for
+// group g, limb l and a chunk of the 2*1023 (direction, step) units,
+//   cpart[i] = sum_units sum_j D[s][j][i] * K5[j][perm_t(i)]  mod q,
+// t = 5^(N/2-2-s) (forward) or 2N - 5^(N/2-2-s) (conjugate), as the
+// reference's permutation tables (src/gpu_protocol.cu:189-213).  The slot
+// permutation is computed in registers (no table).  Thread t owns slots
+// x = t + 256e: lanes then differ in the low five bits of x, which makes the
+// gathers K5[perm_t(x)] hit 32 distinct shared-memory banks for every t.
+// BT queries share each D element read from HBM.
+template <int BT>
+__global__ void __launch_bounds__(256) collapse_kernel(const uint32_t* __restrict__ dp,
+                                                       const uint32_t* __restrict__ dm,
+                                                       const uint32_t* __restrict__ keys, size_t key_qstride,
+                                                       int nchunks, uint32_t* __restrict__ cpart,
+                                                       size_t cpart_qstride, int nq,
+                                                       const DevTables* __restrict__ T) {
+    extern __shared__ __align__(16) uint32_t sk[];  // [BT][digit][N]
+    const int g = blockIdx.x, l = blockIdx.y, ch = blockIdx.z;
+    const uint32_t t = threadIdx.x;
+    const uint32_t q = T->limb[l].q;
+    const uint64_t cr = T->limb[l].cr;
+    for (int b = 0; b < BT; ++b) {
+        const int src = b < nq ? b : 0;
+        const uint32_t* kp = keys + (size_t)src * key_qstride + (size_t)(l * kDeff) * kN;  // key 0 = ksk5
+        for (int i = t; i < kDeff * kN; i += 256) sk[b * kDeff * kN + i] = kp[i];
+    }
+    __syncthreads();
+    const int units = 2 * kSteps;
+    const int per = (units + nchunks - 1) / nchunks;
+    const int u0 = ch * per, u1 = min(units, u0 + per);
+    uint32_t odd[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) odd[e] = 2 * brev11(t + 256 * e) + 1;
+    uint64_t acc[BT][8];
+#pragma unroll
+    for (int b = 0; b < BT; ++b)
+#pragma unroll
+        for (int e = 0; e < 8; ++e) acc[b][e] = 0;
+    const size_t gstride = (size_t)2 * kSteps * kDeff * kN;
+    int dir = u0 >= kSteps;
+    int s = dir ? u0 - kSteps : u0;
+    uint32_t tf = pow5_mod2n(kHalf - 2 - s);
+    int cnt = 0;
+    for (int u = u0; u < u1; ++u) {
+        if (s == kSteps) { dir = 1; s = 0; tf = pow5_mod2n(kHalf - 2); }
+        const uint32_t tt = dir ? ((2 * kN - tf) & (2 * kN - 1)) : tf;
+        const uint32_t* D = (dir ? dm : dp) + (size_t)g * gstride + (size_t)(l * kSteps + s) * kDeff * kN;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const uint32_t x = t + 256 * e;
+            const uint32_t pi = perm_from_odd(tt, odd[e]);
+            const uint64_t d0 = __ldcs(D + x);
+            const uint64_t d1 = __ldcs(D + kN + x);
+#pragma unroll
+            for (int b = 0; b < BT; ++b)
+                acc[b][e] += d0 * sk[(b * kDeff + 0) * kN + pi] + d1 * sk[(b * kDeff + 1) * kN + pi];
+        }
+        if (++cnt == 256) {
+            cnt = 0;
+#pragma unroll
+            for (int b = 0; b < BT; ++b)
+#pragma unroll
+                for (int e = 0; e < 8; ++e) acc[b][e] = mod_u64(acc[b][e], cr, q);
+        }
+        ++s;
+        tf = (tf * kInv5) & (2 * kN - 1);
+    }
+#pragma unroll
+    for (int b = 0; b < BT; ++b) {
+        if (b >= nq) break;
+        uint32_t* dst = cpart + (size_t)b * cpart_qstride + (((size_t)g * nchunks + ch) * 2 + l) * kN;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) dst[t + 256 * e] = mod_u64(acc[b][e], cr, q);
+    }
+}
+
+// ------------------------------------------------------------------ finalize
+// Per (group, limb, query): b = NTT(sum of the mat-vec partials of the
+// group's N columns) - tensor partials - sum_j D_final[j] (.) Kneg1[j]
+// (reference src/gpu_protocol.cu:1233-1274, src/gpu_online.cu:547-559).
+__global__ void __launch_bounds__(256) finalize_kernel(
+    const uint32_t* __restrict__ mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
+    const uint32_t* __restrict__ cpart, size_t cpart_qstride, int cchunks,
+    const uint32_t* __restrict__ df, const uint32_t* __restrict__ keys, size_t key_qstride,
+    const DevTables* __restrict__ T, uint32_t* __restrict__ packed_b, size_t pb_qstride) {
+    __shared__ __align__(16) uint32_t sbuf[2 * kN];
+    const int g = blockIdx.x, l = blockIdx.y, b = blockIdx.z;
+    const uint32_t t = threadIdx.x;
+    const LimbTables& L = T->limb[l];
+    uint32_t r[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const size_t x = (size_t)g * kN + t + 256 * e;
+        uint64_t s = 0;
+        const uint32_t* mp = mvpart + (size_t)b * mv_qstride + (size_t)l * cols + x;
+        for (int y = 0; y < mv_chunks; ++y) s += mp[(size_t)y * 2 * cols];
+        r[e] = mod_u64(s, L.cr, L.q);
+    }
+    ntt_fwd(r, sbuf, L.fwd, L.q, t, 0);
+    uint64_t cs[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) cs[e] = 0;
+    for (int ch = 0; ch < cchunks; ++ch) {
+        uint32_t v[8];
+        ld8(cpart + (size_t)b * cpart_qstride + (((size_t)g * cchunks + ch) * 2 + l) * kN + 8 * t, v);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) cs[e] += v[e];
+    }
+    uint32_t d0[8], d1[8], k0[8], k1[8];
+    ld8(df + ((size_t)g * 2 + l) * kDeff * kN + 8 * t, d0);
+    ld8(df + (((size_t)g * 2 + l) * kDeff + 1) * kN + 8 * t, d1);
+    const uint32_t* kn = keys + (size_t)b * key_qstride + (size_t)((1 * 2 + l) * kDeff) * kN;  // key 1 = kskneg1
+    ld8(kn + 8 * t, k0);
+    ld8(kn + kN + 8 * t, k1);
+    uint32_t o[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const uint32_t fin = mod_u64((uint64_t)d0[e] * k0[e] + (uint64_t)d1[e] * k1[e], L.cr, L.q);
+        const uint32_t sub = add_mod(mod_u64(cs[e], L.cr, L.q), fin, L.q);
+        o[e] = sub_mod(r[e], sub, L.q);
+    }
+    st8(packed_b + (size_t)b * pb_qstride + ((size_t)g * 2 + l) * kN + 8 * t, o);
+}
+
+// ------------------------------------------------------------------ horner
+// HornerEval (reference src/crypto.cpp:264-279, src/gpu_protocol.cu:1300-1334):
+// acc = packed[start+L-1]; for i = L-2..0: acc = ExtProd(rgsw, acc) + packed[start+i].
+// One CTA of four 256-thread NTT groups runs a whole chain; group (p, l)
+// owns polynomial p (0 = a, 1 = b) in limb l.  Per step: inverse NTT, CRT
+// exchange with the partner limb through shared memory, gadget digits,
+// two forward NTTs, the RGSW multiply-accumulate (digits of a meet the top
+// row, digits of b the bottom row) and a cross-group sum.  The chain never
+// leaves the SM; the reference spends ~12 launches per step.
+constexpr size_t kHornerSmem = 4 * kN * sizeof(uint2) + (4 * 2 * kN + 2 * 2 * kN + 2 * 2 * kN) * sizeof(uint32_t);
+
+__global__ void __launch_bounds__(1024, 1) horner_kernel(const uint32_t* __restrict__ pre_a,
+                                                         const uint32_t* __restrict__ packed_b, size_t pb_qstride,
+                                                         const uint32_t* __restrict__ rgsw32,
+                                                         const DevTables* __restrict__ T, size_t groups,
+                                                         size_t d_act, uint64_t* __restrict__ resp,
+                                                         size_t resp_qstride) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint2* tw = reinterpret_cast<uint2*>(smem);                       // [fwd0|fwd1|inv0|inv1][N]
+    uint32_t* nbuf = reinterpret_cast<uint32_t*>(smem + 4 * kN * sizeof(uint2));  // [4][2][N]
+    uint32_t* xcoef = nbuf + 4 * 2 * kN;                              // [p][l][N]
+    uint32_t* xch = xcoef + 2 * 2 * kN;                               // [p][l][N]
+    const int ct = blockIdx.x, b = blockIdx.y;
+    const int gp = threadIdx.x >> 8, p = gp >> 1, l = gp & 1;
+    const uint32_t t = threadIdx.x & 255;
+    const int bar = 1 + gp;
+    for (int i = threadIdx.x; i < kN; i += 1024) {
+        tw[i] = T->limb[0].fwd[i];
+        tw[kN + i] = T->limb[1].fwd[i];
+        tw[2 * kN + i] = T->limb[0].inv[i];
+        tw[3 * kN + i] = T->limb[1].inv[i];
+    }
+    __syncthreads();
+    const LimbTables& L = T->limb[l];
+    const uint32_t q = L.q;
+    const uint2* twf = tw + l * kN;
+    const uint2* twi = tw + (2 + l) * kN;
+    uint32_t* mybuf = nbuf + gp * 2 * kN;
+    const size_t start = (size_t)ct * d_act;
+    const size_t len = (start + d_act <= groups) ? d_act : groups - start;
+    const uint32_t* pbq = packed_b + (size_t)b * pb_qstride;
+    auto src_of = [&](size_t i) -> const uint32_t* {
+        return p ? pbq + (i * 2 + l) * kN : pre_a + (i * 2 + l) * kN;
+    };
+    uint32_t acc[8];
+    ld8(src_of(start + len - 1) + 8 * t, acc);
+    const uint32_t* rg = rgsw32 + (size_t)b * (4 * kDeff * 2 * kN);
+    const uint32_t* Ra0 = rg + (size_t)(((2 * p + 0) * kDeff + 0) * 2 + l) * kN;
+    const uint32_t* Ra1 = rg + (size_t)(((2 * p + 0) * kDeff + 1) * 2 + l) * kN;
+    const uint32_t* Rb0 = rg + (size_t)(((2 * p + 1) * kDeff + 0) * 2 + l) * kN;
+    const uint32_t* Rb1 = rg + (size_t)(((2 * p + 1) * kDeff + 1) * 2 + l) * kN;
+    uint32_t* xc_me = xcoef + (p * 2 + l) * kN;
+    const uint32_t* xc_ot = xcoef + (p * 2 + (1 - l)) * kN;
+    uint32_t* xch_out = xch + ((1 - p) * 2 + l) * kN;
+    const uint32_t* xch_in = xch + (p * 2 + l) * kN;
+    for (long i = (long)len - 2; i >= 0; --i) {
+        ntt_inv(acc, mybuf, twi, q, L.inv_n, L.inv_n_p, t, bar);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) xc_me[t + 256 * e] = acc[e];
+        __syncthreads();
+        uint32_t d0[8], d1[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const uint32_t o = xc_ot[t + 256 * e];
+            int64_t s1, s2;
+            decomp2(l ? o : acc[e], l ? acc[e] : o, *T, s1, s2);
+            d0[e] = signed_res(s1, q);
+            d1[e] = signed_res(s2, q);
+        }
+        ntt_fwd(d0, mybuf, twf, q, t, bar);
+        ntt_fwd(d1, mybuf, twf, q, t, bar);
+        uint32_t a0[8], a1[8], b0[8], b1[8];
+        ld8(Ra0 + 8 * t, a0);
+        ld8(Ra1 + 8 * t, a1);
+        ld8(Rb0 + 8 * t, b0);
+        ld8(Rb1 + 8 * t, b1);
+        uint32_t own[8], oth[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const uint32_t ca = mod_u64((uint64_t)d0[e] * a0[e] + (uint64_t)d1[e] * a1[e], L.cr, q);
+            const uint32_t cb = mod_u64((uint64_t)d0[e] * b0[e] + (uint64_t)d1[e] * b1[e], L.cr, q);
+            own[e] = p ? cb : ca;
+            oth[e] = p ? ca : cb;
+        }
+        st8(xch_out + 8 * t, oth);
+        __syncthreads();
+        uint32_t o2[8], pk[8];
+        ld8(xch_in + 8 * t, o2);
+        ld8(src_of(start + (size_t)i) + 8 * t, pk);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) acc[e] = add_mod(add_mod(own[e], o2[e], q), pk[e], q);
+    }
+    uint64_t* dst = resp + (size_t)b * resp_qstride + ((size_t)ct * 4 + p * 2 + l) * kN + 8 * t;
+#pragma unroll
+    for (int e = 0; e < 8; e += 2)
+        *reinterpret_cast<ulonglong2*>(dst + e) = make_ulonglong2(acc[e], acc[e + 1]);
+}
+
+// ------------------------------------------------------------------ primitives
+__global__ void __launch_bounds__(1024) ntt_batch_kernel(uint32_t* polys, size_t n, int limb_run, bool inverse,
+                                                         const DevTables* __restrict__ T) {
+    extern __shared__ __align__(16) uint32_t nb[];
+    const int gp = threadIdx.x >> 8;
+    const uint32_t t = threadIdx.x & 255;
+    const size_t idx = (size_t)blockIdx.x * 4 + gp;
+    if (idx >= n) return;  // whole group leaves; only group-local barriers follow
+    const int l = (int)((idx / (size_t)limb_run) & 1);
+    const LimbTables& L = T->limb[l];
+    uint32_t* pp = polys + idx * kN;
+    uint32_t r[8];
+    if (!inverse) {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) r[e] = pp[t + 256 * e];
+        ntt_fwd(r, nb + gp * 2 * kN, L.fwd, L.q, t, 1 + gp);
+        st8(pp + 8 * t, r);
+    } else {
+        ld8(pp + 8 * t, r);
+        ntt_inv(r, nb + gp * 2 * kN, L.inv, L.q, L.inv_n, L.inv_n_p, t, 1 + gp);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) pp[t + 256 * e] = r[e];
+    }
+}
+
+__global__ void decomp_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, size_t n,
+                              const DevTables* __restrict__ T) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n * kN) return;
+    const size_t i = k / kN, x = k % kN;
+    int64_t s1, s2;
+    decomp2(in[(i * 2) * kN + x], in[(i * 2 + 1) * kN + x], *T, s1, s2);
+    uint32_t* o = out + i * kDeff * 2 * kN;
+    o[(0 * 2 + 0) * kN + x] = signed_res(s1, kQ0);
+    o[(0 * 2 + 1) * kN + x] = signed_res(s1, kQ1);
+    o[(1 * 2 + 0) * kN + x] = signed_res(s2, kQ0);
+    o[(1 * 2 + 1) * kN + x] = signed_res(s2, kQ1);
+}
+
+}  // namespace
+
+// ==================================================================== wrappers
+cudaError_t launch_qprep(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
+                         uint32_t* keys, uint32_t* rgsw32, int nq, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    qprep_kernel<<<dim3(nq, 12), 256, 0, s>>>(qraw, qstride, rows, T, keys, rgsw32);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_matvec(const uint16_t* db, size_t rows, size_t cols, int chunks, const uint64_t* qraw,
+                          size_t qstride, const DevTables* T, uint32_t* part, size_t part_qstride, int nq,
+                          cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    if (nq > 4 || chunks <= 0 || rows % (size_t)chunks) return cudaErrorInvalidValue;
+    const int rpc = (int)(rows / chunks);
+    if (rpc > (1 << 20)) return cudaErrorInvalidValue;
+    const int bt = nq == 1 ? 1 : (nq == 2 ? 2 : 4);
+    const size_t smem = (size_t)bt * 2 * rpc * sizeof(uint32_t);
+    cudaError_t e;
+    if (bt == 1) {
+        auto k = matvec_kernel<1, 8>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k<<<dim3((unsigned)(cols / 2048), chunks), 256, smem, s>>>(db, rows, cols, rpc, qraw, qstride, T, part,
+                                                                   part_qstride, nq);
+    } else if (bt == 2) {
+        auto k = matvec_kernel<2, 4>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k<<<dim3((unsigned)(cols / 1024), chunks), 256, smem, s>>>(db, rows, cols, rpc, qraw, qstride, T, part,
+                                                                   part_qstride, nq);
+    } else {
+        auto k = matvec_kernel<4, 4>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k<<<dim3((unsigned)(cols / 1024), chunks), 256, smem, s>>>(db, rows, cols, rpc, qraw, qstride, T, part,
+                                                                   part_qstride, nq);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_collapse(const uint32_t* dp, const uint32_t* dm, size_t groups, const uint32_t* keys,
+                              size_t key_qstride, int nchunks, uint32_t* cpart, size_t cpart_qstride, int nq,
+                              const DevTables* T, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    if (nq > 8 || nchunks <= 0) return cudaErrorInvalidValue;
+    const int bt = nq == 1 ? 1 : (nq == 2 ? 2 : (nq <= 4 ? 4 : 8));
+    const size_t smem = (size_t)bt * kDeff * kN * sizeof(uint32_t);
+    dim3 grid((unsigned)groups, 2, nchunks);
+    cudaError_t e;
+#define IPB_COLLAPSE(BTV)                                                                              \
+    {                                                                                                  \
+        auto k = collapse_kernel<BTV>;                                                                 \
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e; \
+        k<<<grid, 256, smem, s>>>(dp, dm, keys, key_qstride, nchunks, cpart, cpart_qstride, nq, T);     \
+    }
+    if (bt == 1) IPB_COLLAPSE(1)
+    else if (bt == 2) IPB_COLLAPSE(2)
+    else if (bt == 4) IPB_COLLAPSE(4)
+    else IPB_COLLAPSE(8)
+#undef IPB_COLLAPSE
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const uint32_t* mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
+                            const uint32_t* cpart, size_t cpart_qstride, int cchunks, const uint32_t* df,
+                            const uint32_t* keys, size_t key_qstride, const DevTables* T, uint32_t* packed_b,
+                            size_t pb_qstride, size_t groups, int nq, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    finalize_kernel<<<dim3((unsigned)groups, 2, nq), 256, 0, s>>>(mvpart, mv_qstride, mv_chunks, cols, cpart,
+                                                                  cpart_qstride, cchunks, df, keys, key_qstride,
+                                                                  T, packed_b, pb_qstride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
+                          const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
+                          size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(horner_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kHornerSmem);
+    if (e) return e;
+    horner_kernel<<<dim3((unsigned)num_cts, nq), 1024, kHornerSmem, s>>>(pre_a, packed_b, pb_qstride, rgsw32, T,
+                                                                          groups, d_act, resp, resp_qstride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ntt_batch(uint32_t* polys, size_t n, int limb_run, bool inverse, const DevTables* T,
+                             cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const size_t smem = 4 * 2 * kN * sizeof(uint32_t);
+    cudaError_t e = cudaFuncSetAttribute(ntt_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e) return e;
+    ntt_batch_kernel<<<(unsigned)((n + 3) / 4), 1024, smem, s>>>(polys, n, limb_run, inverse, T);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decomp(const uint32_t* in, uint32_t* out, size_t n, const DevTables* T, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    decomp_kernel<<<(unsigned)((n * kN + 255) / 256), 256, 0, s>>>(in, out, n, T);
+    return cudaGetLastError();
+}
+
+}  // namespace ipb

@@ -1,0 +1,745 @@
+// server.cpp -- host orchestration of the B200 InsPIRe server: preprocess,
+// server context, answer pipeline, caps, and the C / C++ entry points.
+//
+// Reference counterparts: src/gpu_protocol.cu (GpuServerCtx, gpu_preprocess,
+// gpu_setup_server, answer_one, gpu_answer_batch, caps, free) and
+// src/capi.cu (the C ABI server half).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "host_util.h"
+#include "inspire_b200.h"
+#include "inspire_b200.hpp"
+#include "ipb_launch.h"
+
+namespace ipb {
+
+namespace {
+thread_local std::string g_last_error;
+
+struct CudaFailure : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+[[noreturn]] void cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "CUDA error %d (%s) at %s:%d in %s", (int)e, cudaGetErrorString(e), file, line,
+                  what);
+    throw CudaFailure(buf);
+}
+#define IPB_CK(call)                                                      \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) ::ipb::cuda_fail(e_, #call, __FILE__, __LINE__);  \
+    } while (0)
+
+// Device allocation list freed together.
+struct DevArena {
+    std::vector<void*> ptrs;
+    size_t bytes = 0;
+    template <class T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        const size_t b = count * sizeof(T);
+        IPB_CK(cudaMalloc(&p, b ? b : 16));
+        ptrs.push_back(p);
+        bytes += b;
+        return static_cast<T*>(p);
+    }
+    void free_all() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+        bytes = 0;
+    }
+};
+
+const DevTables& host_tables() {
+    static DevTables T;
+    static std::once_flag once;
+    std::call_once(once, [] { build_tables(T); });
+    return T;
+}
+
+DevTables* upload_tables(DevArena& A, cudaStream_t s) {
+    DevTables* d = A.alloc<DevTables>(1);
+    IPB_CK(cudaMemcpyAsync(d, &host_tables(), sizeof(DevTables), cudaMemcpyHostToDevice, s));
+    return d;
+}
+
+uint32_t inv_mod_p(uint32_t d) {  // d^-1 mod 65535 (d a power of two)
+    int64_t old_r = d, r = kP, old_s = 1, s = 0;
+    while (r) {
+        int64_t qq = old_r / r, t = r;
+        r = old_r - qq * r; old_r = t;
+        t = s; s = old_s - qq * s; old_s = t;
+    }
+    return (uint32_t)((old_s % (int64_t)kP + kP) % kP);
+}
+
+constexpr size_t kGroupStrideD = (size_t)2 * kSteps * kDeff * kN;  // u32 per group, D_plus / D_minus
+constexpr size_t kGroupStrideF = (size_t)2 * kDeff * kN;
+constexpr size_t kGroupStrideA = (size_t)2 * kN;
+constexpr size_t kBlk = (size_t)kDeff * 2 * kN;                    // one KSK / RGSW part
+constexpr size_t kKeyStride = 4 * kDeff * kN;                      // keys per query (u32)
+constexpr size_t kRgswStride = 4 * kBlk;                           // rgsw32 per query (u32)
+}  // namespace
+
+// --------------------------------------------------------------- precomp state
+struct Precomp {
+    Params pp{};
+    int device = 0;
+    DevArena arena;  // owns everything below
+    DevTables* tables = nullptr;
+    uint16_t* db = nullptr;
+    uint32_t* pre_a = nullptr;
+    uint32_t* pre_dp = nullptr;
+    uint32_t* pre_dm = nullptr;
+    uint32_t* pre_df = nullptr;
+    bool adopted = false;
+    ~Precomp() {
+        if (!adopted) {
+            cudaSetDevice(device);
+            arena.free_all();
+        }
+    }
+};
+
+// gpu_preprocess (reference src/gpu_protocol.cu:535-817) on one stream.
+static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s) {
+    const Params& pp = P.pp;
+    const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
+    const size_t d_act = std::min(pp.D, G);
+    DevArena& A = P.arena;
+    P.tables = upload_tables(A, s);
+    P.db = A.alloc<uint16_t>(R * C);
+    P.pre_a = A.alloc<uint32_t>(G * kGroupStrideA);
+    P.pre_dp = A.alloc<uint32_t>(G * kGroupStrideD);
+    P.pre_dm = A.alloc<uint32_t>(G * kGroupStrideD);
+    P.pre_df = A.alloc<uint32_t>(G * kGroupStrideF);
+
+    DevArena tmp;
+    try {
+        // ---- encode (in-place inverse DFT over D_act column polys per row block)
+        if (d_act <= 1) {
+            IPB_CK(cudaMemcpyAsync(P.db, db_host, R * C * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        } else {
+            int logd = 0;
+            while (((size_t)1 << logd) < d_act) ++logd;
+            const int nlA = std::min(logd, 4), nlB = logd - nlA;
+            const uint32_t dinv = inv_mod_p((uint32_t)d_act);
+            const size_t row_bytes = C * sizeof(uint16_t);
+            const size_t chunk_rows = std::max<size_t>(1, std::min<size_t>(R, (size_t)(256u << 20) / row_bytes));
+            uint16_t* staging = tmp.alloc<uint16_t>(chunk_rows * C);
+            for (size_t r0 = 0; r0 < R; r0 += chunk_rows) {
+                const size_t nr = std::min(chunk_rows, R - r0);
+                IPB_CK(cudaMemcpyAsync(staging, db_host + r0 * C, nr * row_bytes, cudaMemcpyHostToDevice, s));
+                IPB_CK(launch_encode_pass(staging, P.db + r0 * C, nr, C, d_act, logd, 0, nlA, true, nlB == 0, dinv, s));
+                if (nlB > 0)
+                    IPB_CK(launch_encode_pass(nullptr, P.db + r0 * C, nr, C, d_act, logd, nlA, nlB, false, true, dinv, s));
+            }
+        }
+        // ---- CRS polys a~_r = NTT(tau_{2N-1}(expand_seed("rlwe", r)))  (src/gpu_protocol.cu:569-582)
+        const size_t n_r = R / kN;
+        std::vector<uint32_t> h_crs(n_r * 2 * kN);
+        {
+            std::vector<uint32_t> a(2 * kN);
+            for (size_t r = 0; r < n_r; ++r) {
+                expand_seed(pp.seed, "rlwe", r, a.data());
+                for (int l = 0; l < 2; ++l) {
+                    const uint32_t q = l ? kQ1 : kQ0;
+                    uint32_t* o = h_crs.data() + (r * 2 + l) * kN;
+                    const uint32_t* in = a.data() + (size_t)l * kN;
+                    o[0] = in[0];
+                    for (size_t i = 1; i < (size_t)kN; ++i) o[i] = in[kN - i] ? q - in[kN - i] : 0;
+                }
+            }
+        }
+        uint32_t* crs = tmp.alloc<uint32_t>(n_r * 2 * kN);
+        IPB_CK(cudaMemcpyAsync(crs, h_crs.data(), h_crs.size() * 4, cudaMemcpyHostToDevice, s));
+        IPB_CK(launch_ntt_batch(crs, 2 * n_r, 1, false, P.tables, s));
+        // ---- ExpandKSK_a sources: K5[j] = expand_seed("ksk", 5*100+j+1), Kn1[j] with (2N-1)*100+j+1
+        //      layout [key][limb][digit][N], NTT form (src/gpu_protocol.cu:364-474)
+        std::vector<uint32_t> h_k(2 * 2 * kDeff * kN);
+        {
+            std::vector<uint32_t> a(2 * kN);
+            for (int key = 0; key < 2; ++key)
+                for (int j = 0; j < kDeff; ++j) {
+                    const uint64_t idx = key == 0 ? 5ull * 100 + j + 1 : (uint64_t)(2 * kN - 1) * 100 + j + 1;
+                    expand_seed(pp.seed, "ksk", idx, a.data());
+                    for (int l = 0; l < 2; ++l)
+                        std::memcpy(h_k.data() + (((size_t)key * 2 + l) * kDeff + j) * kN, a.data() + (size_t)l * kN,
+                                    kN * 4);
+                }
+        }
+        uint32_t* kk = tmp.alloc<uint32_t>(h_k.size());
+        IPB_CK(cudaMemcpyAsync(kk, h_k.data(), h_k.size() * 4, cudaMemcpyHostToDevice, s));
+        IPB_CK(launch_ntt_batch(kk, 2 * 2 * kDeff, kDeff, false, P.tables, s));
+        const uint32_t* k5 = kk;
+        const uint32_t* kn1 = kk + 2 * kDeff * kN;
+        // ---- per group: a-side -> column NTTs -> ring-embed gather; CollapseA in waves
+        uint32_t* V = tmp.alloc<uint32_t>((size_t)2 * kN * kN);
+        uint32_t* Tm = tmp.alloc<uint32_t>((size_t)2 * kN * kN);
+        const size_t ap_gstride = (size_t)kHalf * 2 * 2 * kN;
+        const size_t wave = std::min<size_t>(G, 256);
+        uint32_t* a_post = tmp.alloc<uint32_t>(wave * ap_gstride);
+        uint32_t* ends = tmp.alloc<uint32_t>(wave * 2 * 2 * kN);
+        for (size_t w0 = 0; w0 < G; w0 += wave) {
+            const size_t nw = std::min(wave, G - w0);
+            for (size_t g = w0; g < w0 + nw; ++g) {
+                IPB_CK(launch_a_side(P.db, R, C, g, crs, P.tables, V, s));
+                IPB_CK(launch_col_ntt(V, P.tables, Tm, s));
+                IPB_CK(launch_embed_gather(Tm, a_post + (g - w0) * ap_gstride, s));
+            }
+            IPB_CK(launch_collapse_a(a_post, ap_gstride, k5, P.tables, P.pre_dp + w0 * kGroupStrideD,
+                                     P.pre_dm + w0 * kGroupStrideD, ends, nw, s));
+            IPB_CK(launch_collapse_final(ends, kn1, P.tables, P.pre_df + w0 * kGroupStrideF,
+                                         P.pre_a + w0 * kGroupStrideA, nw, s));
+        }
+        IPB_CK(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        tmp.free_all();
+        throw;
+    }
+    tmp.free_all();
+}
+
+// --------------------------------------------------------------- server
+struct Server {
+    Params pp{};
+    int device = 0;
+    size_t max_batch = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::shared_ptr<Precomp> pre;
+    DevArena arena;
+    uint64_t* qraw = nullptr;
+    uint32_t* keys = nullptr;
+    uint32_t* rgsw32 = nullptr;
+    uint32_t* mvpart = nullptr;
+    uint32_t* cpart = nullptr;
+    uint32_t* packed_b = nullptr;
+    uint64_t* resp = nullptr;
+    size_t qstride = 0, mv_qstride = 0, cpart_qstride = 0, pb_qstride = 0, resp_qstride = 0;
+    int mv_chunks = 1, c_chunks = 1;
+    size_t staged = 0;
+    bool timing = false;
+    cudaEvent_t ev[6] = {};
+    float stage_ms[5] = {};
+    size_t resident_bytes = 0;
+
+    ~Server() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        arena.free_all();
+        if (pre) {
+            pre->adopted = false;  // Precomp frees the DB and tensors
+            pre.reset();
+        }
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+static int pick_pow2_chunks(size_t target, size_t maxv) {
+    size_t c = 1;
+    while (c < target && c * 2 <= maxv) c *= 2;
+    return (int)c;
+}
+
+static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_t max_batch) {
+    if (max_batch == 0) throw std::invalid_argument("gpu_setup_server: max_batch must be >= 1");
+    if (!pre || pre->adopted) throw std::invalid_argument("gpu_setup_server: preprocess data missing or adopted");
+    auto S = std::make_unique<Server>();
+    S->pp = pp;
+    S->device = pre->device;
+    IPB_CK(cudaSetDevice(S->device));
+    S->max_batch = max_batch;
+    IPB_CK(cudaStreamCreateWithFlags(&S->own_stream, cudaStreamNonBlocking));
+    S->stream = S->own_stream;
+    const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
+    S->qstride = 2 * R + 6 * kBlk;
+    const size_t tiles = C / 2048;
+    S->mv_chunks = pick_pow2_chunks((592 + tiles - 1) / tiles, std::max<size_t>(1, R / 256));
+    // <= 4096 rows per chunk keeps the staged query words (4 queries x 2
+    // limbs x rows x 4 B) within 128 KB of shared memory.
+    while (R / (size_t)S->mv_chunks > 4096) S->mv_chunks *= 2;
+    S->c_chunks = (int)std::clamp<size_t>((1184 + 2 * G - 1) / (2 * G), 2, 64);
+    S->mv_qstride = (size_t)S->mv_chunks * 2 * C;
+    S->cpart_qstride = G * (size_t)S->c_chunks * 2 * kN;
+    S->pb_qstride = G * 2 * kN;
+    S->resp_qstride = pp.num_cts * 4 * kN;
+    DevArena& A = S->arena;
+    S->qraw = A.alloc<uint64_t>(max_batch * S->qstride);
+    S->keys = A.alloc<uint32_t>(max_batch * kKeyStride);
+    S->rgsw32 = A.alloc<uint32_t>(max_batch * kRgswStride);
+    S->mvpart = A.alloc<uint32_t>(max_batch * S->mv_qstride);
+    S->cpart = A.alloc<uint32_t>(max_batch * S->cpart_qstride);
+    S->packed_b = A.alloc<uint32_t>(max_batch * S->pb_qstride);
+    S->resp = A.alloc<uint64_t>(max_batch * S->resp_qstride);
+    for (auto& e : S->ev) IPB_CK(cudaEventCreate(&e));
+    pre->adopted = true;
+    S->resident_bytes = pre->arena.bytes + A.bytes;
+    S->pre = std::move(pre);
+    return S.release();
+}
+
+static void stage_queries(Server* S, const ipir_query_view* qs, size_t count) {
+    IPB_CK(cudaSetDevice(S->device));
+    const size_t R = S->pp.db_rows;
+    for (size_t i = 0; i < count; ++i) {
+        uint64_t* d = S->qraw + i * S->qstride;
+        const ipir_query_view& v = qs[i];
+        IPB_CK(cudaMemcpyAsync(d, v.lwe_b_limb0, R * 8, cudaMemcpyHostToDevice, S->stream));
+        IPB_CK(cudaMemcpyAsync(d + R, v.lwe_b_limb1, R * 8, cudaMemcpyHostToDevice, S->stream));
+        IPB_CK(cudaMemcpyAsync(d + 2 * R, v.ksk5_b, kBlk * 8, cudaMemcpyHostToDevice, S->stream));
+        IPB_CK(cudaMemcpyAsync(d + 2 * R + kBlk, v.kskneg1_b, kBlk * 8, cudaMemcpyHostToDevice, S->stream));
+        IPB_CK(cudaMemcpyAsync(d + 2 * R + 2 * kBlk, v.rgsw, 4 * kBlk * 8, cudaMemcpyHostToDevice, S->stream));
+    }
+    S->staged = count;
+}
+
+static void run_pipeline(Server* S, size_t count) {
+    IPB_CK(cudaSetDevice(S->device));
+    const Params& pp = S->pp;
+    const Precomp& P = *S->pre;
+    const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
+    const size_t d_act = std::min(pp.D, G);
+    cudaStream_t st = S->stream;
+    const int nq = (int)count;
+    if (S->timing) IPB_CK(cudaEventRecord(S->ev[0], st));
+    IPB_CK(launch_qprep(S->qraw, S->qstride, R, P.tables, S->keys, S->rgsw32, nq, st));
+    if (S->timing) IPB_CK(cudaEventRecord(S->ev[1], st));
+    for (size_t c0 = 0; c0 < count; c0 += 4) {
+        const int n = (int)std::min<size_t>(4, count - c0);
+        IPB_CK(launch_matvec(P.db, R, C, S->mv_chunks, S->qraw + c0 * S->qstride, S->qstride, P.tables,
+                             S->mvpart + c0 * S->mv_qstride, S->mv_qstride, n, st));
+    }
+    if (S->timing) IPB_CK(cudaEventRecord(S->ev[2], st));
+    for (size_t c0 = 0; c0 < count; c0 += 8) {
+        const int n = (int)std::min<size_t>(8, count - c0);
+        IPB_CK(launch_collapse(P.pre_dp, P.pre_dm, G, S->keys + c0 * kKeyStride, kKeyStride, S->c_chunks,
+                               S->cpart + c0 * S->cpart_qstride, S->cpart_qstride, n, P.tables, st));
+    }
+    if (S->timing) IPB_CK(cudaEventRecord(S->ev[3], st));
+    IPB_CK(launch_finalize(S->mvpart, S->mv_qstride, S->mv_chunks, C, S->cpart, S->cpart_qstride, S->c_chunks,
+                           P.pre_df, S->keys, kKeyStride, P.tables, S->packed_b, S->pb_qstride, G, nq, st));
+    if (S->timing) IPB_CK(cudaEventRecord(S->ev[4], st));
+    IPB_CK(launch_horner(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts, S->resp,
+                         S->resp_qstride, nq, st));
+    if (S->timing) IPB_CK(cudaEventRecord(S->ev[5], st));
+}
+
+static void fetch(Server* S, size_t count, uint64_t* out) {
+    IPB_CK(cudaSetDevice(S->device));
+    IPB_CK(cudaMemcpyAsync(out, S->resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, S->stream));
+    IPB_CK(cudaStreamSynchronize(S->stream));
+    if (S->timing)
+        for (int i = 0; i < 5; ++i) IPB_CK(cudaEventElapsedTime(&S->stage_ms[i], S->ev[i], S->ev[i + 1]));
+}
+
+static int validate_batch(const Server* S, const ipir_query_view* qs, size_t count, const void* out) {
+    if (!S || !qs || !out) return 1;
+    if (count > S->max_batch) return 2;
+    for (size_t i = 0; i < count; ++i) {
+        const ipir_query_view& v = qs[i];
+        if (!v.lwe_b_limb0 || !v.lwe_b_limb1 || !v.ksk5_b || !v.kskneg1_b || !v.rgsw) return 3;
+    }
+    return 0;
+}
+
+static std::shared_ptr<Precomp> run_preprocess(const Params& pp, const uint16_t* db) {
+    if (!db) throw std::invalid_argument("gpu_preprocess: null db");
+    auto P = std::make_shared<Precomp>();
+    P->pp = pp;
+    IPB_CK(cudaGetDevice(&P->device));
+    cudaStream_t s = nullptr;
+    IPB_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    try {
+        preprocess_into(*P, db, s);
+    } catch (...) {
+        cudaStreamDestroy(s);
+        throw;
+    }
+    cudaStreamDestroy(s);
+    return P;
+}
+
+}  // namespace ipb
+
+// ======================================================================= C++ API
+namespace inspire_b200 {
+
+struct PreprocessState {
+    std::shared_ptr<ipb::Precomp> p;
+};
+struct GpuServerCtx {
+    ipb::Server* s;
+};
+
+static ipb::Params to_ipb(const PublicParams& pp) {
+    ipb::Params p{};
+    p.n_entries = pp.N_entries;
+    p.w = pp.w;
+    p.db_rows = pp.db_rows;
+    p.db_cols = pp.db_cols;
+    p.n_packed = pp.n_packed;
+    p.D = pp.D;
+    p.num_cts = pp.num_cts;
+    std::memcpy(p.seed, pp.seed.data(), SEED_BYTES);
+    return p;
+}
+
+static void check_geometry(const PublicParams& pp) {
+    ipb::Params chk{};
+    const char* why = nullptr;
+    if (ipb::setup_geometry(pp.N_entries, pp.w, pp.db_rows, &chk, &why) != 0) throw std::invalid_argument(why);
+    if (chk.db_cols != pp.db_cols || chk.n_packed != pp.n_packed || chk.D != pp.D || chk.num_cts != pp.num_cts)
+        throw std::invalid_argument("PublicParams inconsistent with setup()");
+}
+
+PublicParams setup(size_t N_entries, size_t w) { return setup(N_entries, w, ipb::kDefaultDbRows); }
+
+PublicParams setup(size_t N_entries, size_t w, size_t db_rows_override) {
+    ipb::Params p{};
+    const char* why = nullptr;
+    if (ipb::setup_geometry(N_entries, w, db_rows_override, &p, &why) != 0) throw std::invalid_argument(why);
+    PublicParams pp;
+    pp.N_entries = p.n_entries;
+    pp.w = p.w;
+    pp.db_rows = p.db_rows;
+    pp.db_cols = p.db_cols;
+    pp.n_packed = p.n_packed;
+    pp.D = p.D;
+    pp.num_cts = p.num_cts;
+    std::random_device rd;  // src/params.cpp:63-65
+    std::mt19937_64 rng(rd());
+    for (auto& b : pp.seed) b = (uint8_t)(rng() & 0xFF);
+    return pp;
+}
+
+PreprocessData gpu_preprocess(const PublicParams& pp, const uint16_t* db) {
+    check_geometry(pp);
+    PreprocessData d;
+    d.state = std::make_shared<PreprocessState>();
+    d.state->p = ipb::run_preprocess(to_ipb(pp), db);
+    return d;
+}
+
+GpuServerCtx* gpu_setup_server(const PublicParams& pp, const PreprocessData& precomp) {
+    return gpu_setup_server(pp, precomp, GpuServerConfig{});
+}
+
+GpuServerCtx* gpu_setup_server(const PublicParams& pp, const PreprocessData& precomp, const GpuServerConfig& cfg) {
+    if (!precomp.state) throw std::invalid_argument("gpu_setup_server: empty PreprocessData");
+    // Ownership of the device buffers moves to the context, as in the
+    // reference (src/gpu_protocol.cu:856-885).
+    std::shared_ptr<ipb::Precomp> p = std::move(precomp.state->p);
+    auto* ctx = new GpuServerCtx{ipb::make_server(to_ipb(pp), std::move(p), cfg.max_batch)};
+    return ctx;
+}
+
+GpuServerCaps gpu_server_caps(const GpuServerCtx* ctx) {
+    GpuServerCaps c{};
+    if (!ctx) return c;
+    c.max_batch = ctx->s->max_batch;
+    c.resident_bytes = ctx->s->resident_bytes;
+    c.num_cts = ctx->s->pp.num_cts;
+    size_t fr = 0, tot = 0;
+    cudaSetDevice(ctx->s->device);
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) c.device_free_bytes = fr;
+    return c;
+}
+
+void gpu_answer_batch(GpuServerCtx* ctx, const ipir_query_view* queries, size_t count, uint64_t* out) {
+    if (!ctx) throw std::invalid_argument("gpu_answer_batch: null ctx");
+    int rc = ipb::validate_batch(ctx->s, queries, count, out);
+    if (rc == 2) throw std::invalid_argument("gpu_answer_batch: count exceeds max_batch");
+    if (rc) throw std::invalid_argument("gpu_answer_batch: null argument");
+    if (count == 0) return;
+    ipb::stage_queries(ctx->s, queries, count);
+    ipb::run_pipeline(ctx->s, count);
+    ipb::fetch(ctx->s, count, out);
+}
+
+void gpu_answer(GpuServerCtx* ctx, const ipir_query_view& q, uint64_t* out) { gpu_answer_batch(ctx, &q, 1, out); }
+
+void gpu_free_server(GpuServerCtx* ctx) {
+    if (!ctx) return;
+    delete ctx->s;
+    delete ctx;
+}
+
+}  // namespace inspire_b200
+
+// ======================================================================= C ABI
+struct ipir_server {
+    ipb::Server* s;
+};
+
+namespace {
+template <class F>
+int guarded(F&& f, int fail_code) {
+    try {
+        return f();
+    } catch (const std::exception& e) {
+        ipb::g_last_error = e.what();
+    } catch (...) {
+        ipb::g_last_error = "unknown error";
+    }
+    return fail_code;
+}
+void fill_params(const ipb::Params& pp, ipir_params* o) {
+    o->n_entries = pp.n_entries;
+    o->entry_bytes = pp.w;
+    o->db_rows = pp.db_rows;
+    o->db_cols = pp.db_cols;
+    o->n_packed = pp.n_packed;
+    o->interp_d = pp.D;
+    o->num_cts = pp.num_cts;
+    o->ring_n = ipb::kN;
+    o->d_eff = ipb::kDeff;
+    std::memcpy(o->seed, pp.seed, 64);
+}
+}  // namespace
+
+extern "C" {
+
+const char* ipir_b200_last_error(void) { return ipb::g_last_error.c_str(); }
+
+int ipir_b200_setup(size_t n_entries, size_t entry_bytes, size_t db_rows_or_zero, ipir_params* out) {
+    if (!out) return 1;
+    ipb::Params pp{};
+    const char* why = nullptr;
+    int rc = ipb::setup_geometry(n_entries, entry_bytes, db_rows_or_zero, &pp, &why);
+    if (rc) {
+        ipb::g_last_error = why ? why : "setup failed";
+        return rc;
+    }
+    fill_params(pp, out);
+    return 0;
+}
+
+ipir_server* ipir_server_create(size_t n_entries, size_t entry_bytes, size_t db_rows_or_zero, size_t max_batch,
+                                const uint16_t* db, const uint8_t* crs_seed_or_null, ipir_params* out_params) {
+    if (!db || !out_params || max_batch == 0) {
+        ipb::g_last_error = "ipir_server_create: null argument or max_batch == 0";
+        return nullptr;
+    }
+    ipir_server* result = nullptr;
+    guarded(
+        [&]() -> int {
+            ipb::Params pp{};
+            const char* why = nullptr;
+            if (ipb::setup_geometry(n_entries, entry_bytes, db_rows_or_zero, &pp, &why) != 0)
+                throw std::invalid_argument(why);
+            if (crs_seed_or_null) {
+                std::memcpy(pp.seed, crs_seed_or_null, 64);
+            } else {
+                std::random_device rd;
+                std::mt19937_64 rng(rd());
+                for (auto& b : pp.seed) b = (uint8_t)(rng() & 0xFF);
+            }
+            auto P = ipb::run_preprocess(pp, db);
+            std::unique_ptr<ipb::Server> S(ipb::make_server(pp, std::move(P), max_batch));
+            fill_params(pp, out_params);
+            result = new ipir_server{S.release()};
+            return 0;
+        },
+        1);
+    return result;
+}
+
+void ipir_server_caps(const ipir_server* srv, ipir_caps* out) {
+    if (!srv || !out) return;
+    inspire_b200::GpuServerCtx ctx{srv->s};
+    auto c = inspire_b200::gpu_server_caps(&ctx);
+    out->max_batch = c.max_batch;
+    out->resident_bytes = c.resident_bytes;
+    out->device_free_bytes = c.device_free_bytes;
+    out->num_cts = c.num_cts;
+}
+
+int ipir_answer_batch(ipir_server* srv, const ipir_query_view* queries, size_t count, uint64_t* out_resp) {
+    if (!srv) return 1;
+    int rc = ipb::validate_batch(srv->s, queries, count, out_resp);
+    if (rc) return rc;
+    if (count == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            ipb::stage_queries(srv->s, queries, count);
+            ipb::run_pipeline(srv->s, count);
+            ipb::fetch(srv->s, count, out_resp);
+            return 0;
+        },
+        4);
+}
+
+void ipir_server_destroy(ipir_server* srv) {
+    if (!srv) return;
+    delete srv->s;
+    delete srv;
+}
+
+int ipir_b200_set_stream(ipir_server* srv, void* stream) {
+    if (!srv) return 1;
+    srv->s->stream = stream ? static_cast<cudaStream_t>(stream) : srv->s->own_stream;
+    return 0;
+}
+
+int ipir_b200_stage_queries(ipir_server* srv, const ipir_query_view* queries, size_t count) {
+    if (!srv) return 1;
+    int rc = ipb::validate_batch(srv->s, queries, count, queries);
+    if (rc) return rc;
+    return guarded([&]() -> int { ipb::stage_queries(srv->s, queries, count); return 0; }, 4);
+}
+
+int ipir_b200_run(ipir_server* srv, size_t count) {
+    if (!srv) return 1;
+    if (count > srv->s->max_batch) return 2;
+    if (count == 0) return 0;
+    return guarded([&]() -> int { ipb::run_pipeline(srv->s, count); return 0; }, 4);
+}
+
+int ipir_b200_fetch_responses(ipir_server* srv, size_t count, uint64_t* out) {
+    if (!srv || !out) return 1;
+    if (count > srv->s->max_batch) return 2;
+    return guarded([&]() -> int { ipb::fetch(srv->s, count, out); return 0; }, 4);
+}
+
+int ipir_b200_sync(ipir_server* srv) {
+    if (!srv) return 1;
+    return guarded([&]() -> int { IPB_CK(cudaStreamSynchronize(srv->s->stream)); return 0; }, 4);
+}
+
+int ipir_b200_enable_stage_timing(ipir_server* srv, int on) {
+    if (!srv) return 1;
+    srv->s->timing = on != 0;
+    return 0;
+}
+
+int ipir_b200_stage_times(const ipir_server* srv, float* ms_out, size_t n) {
+    if (!srv || !ms_out) return 1;
+    for (size_t i = 0; i < n && i < 5; ++i) ms_out[i] = srv->s->stage_ms[i];
+    return 0;
+}
+
+int ipir_b200_export_precomp(const ipir_server* srv, size_t group, uint32_t* a, uint32_t* d_plus, uint32_t* d_minus,
+                             uint32_t* d_final) {
+    if (!srv) return 1;
+    const ipb::Server* S = srv->s;
+    if (group >= S->pp.n_packed) return 2;
+    return guarded(
+        [&]() -> int {
+            IPB_CK(cudaSetDevice(S->device));
+            const ipb::Precomp& P = *S->pre;
+            if (a) IPB_CK(cudaMemcpy(a, P.pre_a + group * ipb::kGroupStrideA, ipb::kGroupStrideA * 4, cudaMemcpyDeviceToHost));
+            if (d_plus) IPB_CK(cudaMemcpy(d_plus, P.pre_dp + group * ipb::kGroupStrideD, ipb::kGroupStrideD * 4, cudaMemcpyDeviceToHost));
+            if (d_minus) IPB_CK(cudaMemcpy(d_minus, P.pre_dm + group * ipb::kGroupStrideD, ipb::kGroupStrideD * 4, cudaMemcpyDeviceToHost));
+            if (d_final) IPB_CK(cudaMemcpy(d_final, P.pre_df + group * ipb::kGroupStrideF, ipb::kGroupStrideF * 4, cudaMemcpyDeviceToHost));
+            return 0;
+        },
+        4);
+}
+
+int ipir_b200_export_db(const ipir_server* srv, size_t row0, size_t nrows, uint16_t* out) {
+    if (!srv || !out) return 1;
+    const ipb::Server* S = srv->s;
+    if (row0 + nrows > S->pp.db_rows) return 2;
+    return guarded(
+        [&]() -> int {
+            IPB_CK(cudaSetDevice(S->device));
+            IPB_CK(cudaMemcpy(out, S->pre->db + row0 * S->pp.db_cols, nrows * S->pp.db_cols * 2, cudaMemcpyDeviceToHost));
+            return 0;
+        },
+        4);
+}
+
+int ipir_b200_ntt(uint32_t* polys, size_t n, int limb_run, int inverse) {
+    if (!polys || limb_run <= 0) return 1;
+    if (n == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            ipb::DevArena A;
+            try {
+                ipb::DevTables* T = ipb::upload_tables(A, 0);
+                uint32_t* d = A.alloc<uint32_t>(n * ipb::kN);
+                IPB_CK(cudaMemcpy(d, polys, n * ipb::kN * 4, cudaMemcpyHostToDevice));
+                IPB_CK(ipb::launch_ntt_batch(d, n, limb_run, inverse != 0, T, 0));
+                IPB_CK(cudaMemcpy(polys, d, n * ipb::kN * 4, cudaMemcpyDeviceToHost));
+            } catch (...) {
+                A.free_all();
+                throw;
+            }
+            A.free_all();
+            return 0;
+        },
+        4);
+}
+
+int ipir_b200_decomp(const uint32_t* in, uint32_t* out, size_t n) {
+    if (!in || !out) return 1;
+    if (n == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            ipb::DevArena A;
+            try {
+                ipb::DevTables* T = ipb::upload_tables(A, 0);
+                uint32_t* di = A.alloc<uint32_t>(n * 2 * ipb::kN);
+                uint32_t* dout = A.alloc<uint32_t>(n * ipb::kDeff * 2 * ipb::kN);
+                IPB_CK(cudaMemcpy(di, in, n * 2 * ipb::kN * 4, cudaMemcpyHostToDevice));
+                IPB_CK(ipb::launch_decomp(di, dout, n, T, 0));
+                IPB_CK(cudaMemcpy(out, dout, n * ipb::kDeff * 2 * ipb::kN * 4, cudaMemcpyDeviceToHost));
+            } catch (...) {
+                A.free_all();
+                throw;
+            }
+            A.free_all();
+            return 0;
+        },
+        4);
+}
+
+int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed) {
+    if (!out && count) return 1;
+    // splitmix64(seed ^ k) mod 65535 at flat index k, on all host threads.
+    const unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    const size_t per = (count + nt - 1) / nt;
+    for (unsigned w = 0; w < nt; ++w)
+        th.emplace_back([=] {
+            const size_t k0 = (size_t)w * per, k1 = std::min(count, k0 + per);
+            for (size_t k = k0; k < k1; ++k) {
+                uint64_t x = (seed ^ k) + 0x9e3779b97f4a7c15ULL;
+                x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+                x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+                x ^= x >> 31;
+                out[k] = (uint16_t)(x % 65535u);
+            }
+        });
+    for (auto& t : th) t.join();
+    return 0;
+}
+
+int ipir_b200_shake256(const uint8_t* in, size_t inlen, uint8_t* out, size_t outlen) {
+    if ((!in && inlen) || (!out && outlen)) return 1;
+    ipb::shake256(in, inlen, out, outlen);
+    return 0;
+}
+
+int ipir_b200_expand_seed(const uint8_t* seed64, const char* domain, uint64_t index, uint32_t* out) {
+    if (!seed64 || !domain || !out) return 1;
+    return guarded([&]() -> int { ipb::expand_seed(seed64, domain, index, out); return 0; }, 2);
+}
+
+}  // extern "C"

@@ -1,0 +1,339 @@
+"""Python host binding of the B200-native InsPIRe PIR server.
+
+A thin ctypes layer over ``libinspire_b200.so`` (the C ABI declared in
+``include/inspire_b200.h``), mirroring the reference's server C ABI
+(SoraSuegami/InsPIRe-GPU src/capi.h:23-91): ``ipir_server_create``,
+``ipir_server_caps``, ``ipir_answer_batch``, ``ipir_server_destroy``, with the
+same flat layouts:
+
+* query   ``[b0: db_rows][b1: db_rows][ksk5: blk][kskneg1: blk][rgsw: 4 blk]``
+  u64, ``blk = d_eff * 2 * ring_n`` (``ipir_query_view_from_flat``,
+  reference src/capi.h:109-116);
+* response ``[ct][a|b][limb][coeff]`` u64 per query, NTT form.
+
+There is no CPU fallback: every computation runs in the CUDA library, and
+importing this module fails loudly when the library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libinspire_b200.so")
+
+RING_N = 2048
+D_EFF = 2
+Q0, Q1 = 94519297, 95293441
+P = 65535
+NSTEPS = 1023
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `make -C inspire-gpu_b200` "
+                      "(there is no CPU fallback)")
+_L = C.CDLL(LIB_PATH)
+
+u64p = C.POINTER(C.c_uint64)
+u32p = C.POINTER(C.c_uint32)
+u16p = C.POINTER(C.c_uint16)
+u8p = C.POINTER(C.c_uint8)
+
+
+class IpirParams(C.Structure):
+    _fields_ = [("n_entries", C.c_size_t), ("entry_bytes", C.c_size_t), ("db_rows", C.c_size_t),
+                ("db_cols", C.c_size_t), ("n_packed", C.c_size_t), ("interp_d", C.c_size_t),
+                ("num_cts", C.c_size_t), ("ring_n", C.c_size_t), ("d_eff", C.c_size_t),
+                ("seed", C.c_uint8 * 64)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "seed"}
+        d["seed"] = bytes(self.seed)
+        return d
+
+
+class IpirCaps(C.Structure):
+    _fields_ = [("max_batch", C.c_size_t), ("resident_bytes", C.c_size_t),
+                ("device_free_bytes", C.c_size_t), ("num_cts", C.c_size_t)]
+
+
+class IpirQueryView(C.Structure):
+    _fields_ = [("lwe_b_limb0", u64p), ("lwe_b_limb1", u64p), ("ksk5_b", u64p),
+                ("kskneg1_b", u64p), ("rgsw", u64p)]
+
+
+_L.ipir_server_create.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, u16p, u8p,
+                                  C.POINTER(IpirParams)]
+_L.ipir_server_create.restype = C.c_void_p
+_L.ipir_server_caps.argtypes = [C.c_void_p, C.POINTER(IpirCaps)]
+_L.ipir_server_caps.restype = None
+_L.ipir_answer_batch.argtypes = [C.c_void_p, C.POINTER(IpirQueryView), C.c_size_t, u64p]
+_L.ipir_answer_batch.restype = C.c_int
+_L.ipir_server_destroy.argtypes = [C.c_void_p]
+_L.ipir_server_destroy.restype = None
+_L.ipir_b200_last_error.restype = C.c_char_p
+_L.ipir_b200_setup.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(IpirParams)]
+_L.ipir_b200_setup.restype = C.c_int
+_L.ipir_b200_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+_L.ipir_b200_stage_queries.argtypes = [C.c_void_p, C.POINTER(IpirQueryView), C.c_size_t]
+_L.ipir_b200_run.argtypes = [C.c_void_p, C.c_size_t]
+_L.ipir_b200_fetch_responses.argtypes = [C.c_void_p, C.c_size_t, u64p]
+_L.ipir_b200_sync.argtypes = [C.c_void_p]
+_L.ipir_b200_enable_stage_timing.argtypes = [C.c_void_p, C.c_int]
+_L.ipir_b200_stage_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_size_t]
+_L.ipir_b200_export_precomp.argtypes = [C.c_void_p, C.c_size_t, u32p, u32p, u32p, u32p]
+_L.ipir_b200_export_db.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, u16p]
+_L.ipir_b200_ntt.argtypes = [u32p, C.c_size_t, C.c_int, C.c_int]
+_L.ipir_b200_decomp.argtypes = [u32p, u32p, C.c_size_t]
+_L.ipir_b200_shake256.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t]
+_L.ipir_b200_expand_seed.argtypes = [u8p, C.c_char_p, C.c_uint64, u32p]
+_L.ipir_b200_fill_db.argtypes = [u16p, C.c_size_t, C.c_uint64]
+
+EXPORTED = [
+    "ipir_server_create", "ipir_server_caps", "ipir_answer_batch", "ipir_server_destroy",
+    "ipir_b200_last_error", "ipir_b200_setup", "ipir_b200_set_stream", "ipir_b200_stage_queries",
+    "ipir_b200_run", "ipir_b200_fetch_responses", "ipir_b200_sync", "ipir_b200_enable_stage_timing",
+    "ipir_b200_stage_times", "ipir_b200_export_precomp", "ipir_b200_export_db", "ipir_b200_ntt",
+    "ipir_b200_decomp", "ipir_b200_shake256", "ipir_b200_expand_seed", "ipir_b200_fill_db",
+]
+
+
+class InspireError(RuntimeError):
+    pass
+
+
+def last_error():
+    return _L.ipir_b200_last_error().decode()
+
+
+def _ptr(a, t):
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data_as(t)
+
+
+def library_handle():
+    return _L
+
+
+def setup(n_entries, entry_bytes, db_rows=0):
+    """Geometry of the reference's setup() (src/params.cpp:23-68).  Raises
+    ValueError where the reference throws std::invalid_argument."""
+    p = IpirParams()
+    rc = _L.ipir_b200_setup(n_entries, entry_bytes, db_rows, C.byref(p))
+    if rc:
+        raise ValueError(last_error())
+    return p.as_dict()
+
+
+def query_u64s(params):
+    return 2 * params["db_rows"] + 6 * D_EFF * 2 * RING_N
+
+
+def response_u64s(params):
+    return params["num_cts"] * 4 * RING_N
+
+
+def query_view_from_flat(params, flat):
+    """View into a flat query (reference ipir_query_view_from_flat,
+    src/capi_client.cpp:81-93).  ``flat`` must stay alive while the view is used."""
+    flat = np.ascontiguousarray(flat, dtype=np.uint64)
+    if flat.size != query_u64s(params):
+        raise ValueError(f"flat query has {flat.size} u64, expected {query_u64s(params)}")
+    R = params["db_rows"]
+    blk = D_EFF * 2 * RING_N
+    base = flat.ctypes.data
+    v = IpirQueryView()
+    v.lwe_b_limb0 = C.cast(base, u64p)
+    v.lwe_b_limb1 = C.cast(base + 8 * R, u64p)
+    v.ksk5_b = C.cast(base + 8 * (2 * R), u64p)
+    v.kskneg1_b = C.cast(base + 8 * (2 * R + blk), u64p)
+    v.rgsw = C.cast(base + 8 * (2 * R + 2 * blk), u64p)
+    return v
+
+
+class Server:
+    """One database generation on the current CUDA device (reference
+    ipir_server_create / GpuServerCtx)."""
+
+    def __init__(self, n_entries, entry_bytes, db, db_rows=0, max_batch=16, crs_seed=None):
+        db = np.ascontiguousarray(db, dtype=np.uint16)
+        p = IpirParams()
+        seed = None
+        if crs_seed is not None:
+            if len(crs_seed) != 64:
+                raise ValueError("crs_seed must be 64 bytes")
+            seed = np.frombuffer(bytes(crs_seed), np.uint8).copy()
+        h = _L.ipir_server_create(n_entries, entry_bytes, db_rows, max_batch, _ptr(db, u16p),
+                                  _ptr(seed, u8p) if seed is not None else None, C.byref(p))
+        if not h:
+            raise InspireError(f"ipir_server_create failed: {last_error()}")
+        self._h = h
+        self.params = p.as_dict()
+        self.max_batch = max_batch
+
+    def _check(self):
+        if not self._h:
+            raise InspireError("server destroyed")
+
+    def caps(self):
+        self._check()
+        c = IpirCaps()
+        _L.ipir_server_caps(self._h, C.byref(c))
+        return {f: getattr(c, f) for f, _ in c._fields_}
+
+    def _views(self, queries):
+        flats = [np.ascontiguousarray(q, dtype=np.uint64) for q in queries]
+        arr = (IpirQueryView * max(1, len(flats)))()
+        for i, f in enumerate(flats):
+            arr[i] = query_view_from_flat(self.params, f)
+        return arr, flats
+
+    def answer_batch(self, queries, out=None):
+        """queries: list of flat u64 queries -> (count, num_cts*4*N) u64 responses."""
+        self._check()
+        views, keep = self._views(queries)
+        n = len(keep)
+        if out is None:
+            out = np.zeros((n, response_u64s(self.params)), np.uint64)
+        rc = _L.ipir_answer_batch(self._h, views, n, _ptr(out, u64p))
+        if rc:
+            raise InspireError(f"ipir_answer_batch rc={rc}: {last_error()}")
+        return out
+
+    def answer(self, query):
+        return self.answer_batch([query])[0]
+
+    def answer_batch_rc(self, views, count, out):
+        """Raw C call returning the reference's code (tests of the error contract)."""
+        return _L.ipir_answer_batch(self._h, views, count, _ptr(out, u64p) if out is not None else None)
+
+    # device-resident pipeline --------------------------------------------
+    def set_stream(self, stream_handle):
+        self._check()
+        _L.ipir_b200_set_stream(self._h, C.c_void_p(stream_handle or 0))
+
+    def stage(self, queries):
+        self._check()
+        views, keep = self._views(queries)
+        self._staged_keep = keep
+        rc = _L.ipir_b200_stage_queries(self._h, views, len(keep))
+        if rc:
+            raise InspireError(f"stage rc={rc}: {last_error()}")
+
+    def stage_views(self, views, count):
+        rc = _L.ipir_b200_stage_queries(self._h, views, count)
+        if rc:
+            raise InspireError(f"stage rc={rc}: {last_error()}")
+
+    def run(self, count):
+        self._check()
+        rc = _L.ipir_b200_run(self._h, count)
+        if rc:
+            raise InspireError(f"run rc={rc}: {last_error()}")
+
+    def fetch(self, count, out=None):
+        self._check()
+        if out is None:
+            out = np.zeros((count, response_u64s(self.params)), np.uint64)
+        rc = _L.ipir_b200_fetch_responses(self._h, count, _ptr(out, u64p))
+        if rc:
+            raise InspireError(f"fetch rc={rc}: {last_error()}")
+        return out
+
+    def sync(self):
+        self._check()
+        if _L.ipir_b200_sync(self._h):
+            raise InspireError(last_error())
+
+    def enable_stage_timing(self, on=True):
+        _L.ipir_b200_enable_stage_timing(self._h, 1 if on else 0)
+
+    def stage_times(self):
+        a = (C.c_float * 5)()
+        _L.ipir_b200_stage_times(self._h, a, 5)
+        return dict(zip(["qprep", "matvec", "collapse", "finalize", "horner"], list(a)))
+
+    def export_precomp(self, group):
+        self._check()
+        a = np.zeros(2 * RING_N, np.uint32)
+        dp = np.zeros(2 * NSTEPS * D_EFF * RING_N, np.uint32)
+        dm = np.zeros_like(dp)
+        df = np.zeros(2 * D_EFF * RING_N, np.uint32)
+        rc = _L.ipir_b200_export_precomp(self._h, group, _ptr(a, u32p), _ptr(dp, u32p),
+                                         _ptr(dm, u32p), _ptr(df, u32p))
+        if rc:
+            raise InspireError(f"export_precomp rc={rc}: {last_error()}")
+        return a, dp, dm, df
+
+    def export_db(self, row0, nrows):
+        self._check()
+        out = np.zeros(nrows * self.params["db_cols"], np.uint16)
+        rc = _L.ipir_b200_export_db(self._h, row0, nrows, _ptr(out, u16p))
+        if rc:
+            raise InspireError(f"export_db rc={rc}: {last_error()}")
+        return out
+
+    def close(self):
+        if self._h:
+            _L.ipir_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ primitives
+def ntt(polys, limb_run=1, inverse=False):
+    """GPU forward/inverse NTT of (n, 2048) u32 residues; poly i is mod
+    q_((i // limb_run) & 1)."""
+    a = np.ascontiguousarray(polys, dtype=np.uint32).copy()
+    n = a.size // RING_N
+    rc = _L.ipir_b200_ntt(_ptr(a, u32p), n, limb_run, 1 if inverse else 0)
+    if rc:
+        raise InspireError(f"ipir_b200_ntt rc={rc}: {last_error()}")
+    return a
+
+
+def decomp(polys):
+    """GPU gadget decomposition: (n, 2, 2048) coefficient form -> (n, 2, 2, 2048)
+    [digit][limb]."""
+    a = np.ascontiguousarray(polys, dtype=np.uint32)
+    n = a.size // (2 * RING_N)
+    out = np.zeros(n * D_EFF * 2 * RING_N, np.uint32)
+    rc = _L.ipir_b200_decomp(_ptr(a, u32p), _ptr(out, u32p), n)
+    if rc:
+        raise InspireError(f"ipir_b200_decomp rc={rc}: {last_error()}")
+    return out
+
+
+def shake256(data, outlen):
+    src = np.frombuffer(bytes(data), np.uint8).copy() if len(data) else np.zeros(1, np.uint8)
+    out = np.zeros(max(outlen, 1), np.uint8)
+    _L.ipir_b200_shake256(_ptr(src, u8p), len(data), _ptr(out, u8p), outlen)
+    return out[:outlen].tobytes()
+
+
+def expand_seed(seed, domain, index):
+    s = np.frombuffer(bytes(seed), np.uint8).copy()
+    out = np.zeros(2 * RING_N, np.uint32)
+    rc = _L.ipir_b200_expand_seed(_ptr(s, u8p), domain.encode(), index, _ptr(out, u32p))
+    if rc:
+        raise InspireError(last_error())
+    return out
+
+
+def fill_db(count, seed, out=None):
+    """Synthetic DB: splitmix64(seed ^ k) mod 65535 (host, all threads)."""
+    if out is None:
+        out = np.empty(count, np.uint16)
+    _L.ipir_b200_fill_db(_ptr(out, u16p), count, seed)
+    return out

@@ -1,0 +1,74 @@
+"""gpu_answer_batch contract (reference tests/test_gpu_batch.cu): batch ==
+independent single answers bit-exact, slot-exact extract, caps consistent,
+rerun reproducible, partial batches, duplicate indices with fresh keys;
+plus the C-ABI error codes with nothing written (tests/test_capi.cu:110-114)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cases import get_case
+
+pytestmark = pytest.mark.gpu
+
+IDX = [0, 42, 1000, 100000, 524287, 0, 42, 1000, 100000, 524287]
+
+
+@pytest.fixture(scope="module")
+def batch_env():
+    import inspire_b200 as ib
+    c = get_case("batch")
+    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=10, crs_seed=c.seed)
+    qs, sts = [], []
+    for k, idx in enumerate(IDX):
+        q, st = c.query(idx, 3000 + k)   # fresh key material per query
+        qs.append(q)
+        sts.append(st)
+    yield c, srv, qs, sts
+    srv.close()
+
+
+def test_caps(batch_env):
+    c, srv, _, _ = batch_env
+    caps = srv.caps()
+    assert caps["max_batch"] == 10 and caps["num_cts"] == c.ncts and caps["resident_bytes"] > 0
+    assert caps["device_free_bytes"] > 0
+
+
+def test_batch_equals_singles_and_oracle(batch_env):
+    c, srv, qs, sts = batch_env
+    singles = np.stack([srv.answer(q) for q in qs])
+    batch = srv.answer_batch(qs)
+    assert (batch == singles).all()
+    for i in (0, 4, 9):
+        assert (batch[i] == c.oracle_answer(qs[i])).all(), i
+    for i, st in enumerate(sts):
+        assert (st.extract(batch[i]) == c.expected_slots(IDX[i])).all(), i
+    # duplicate indices, fresh keys: different ciphertexts, same plaintext
+    assert not (batch[0] == batch[5]).all()
+    again = srv.answer_batch(qs)
+    assert (again == batch).all()
+    for n in (3, 2):
+        part = srv.answer_batch(qs[:n])
+        assert (part == singles[:n]).all()
+
+
+def test_capi_error_codes_write_nothing(batch_env):
+    import inspire_b200 as ib
+    c, srv, qs, _ = batch_env
+    views = (ib.IpirQueryView * 11)()
+    keep = [np.ascontiguousarray(q) for q in qs] + [np.ascontiguousarray(qs[0])]
+    for i, f in enumerate(keep):
+        views[i] = ib.query_view_from_flat(srv.params, f)
+    out = np.full((11, ib.response_u64s(srv.params)), 7, np.uint64)
+    assert srv.answer_batch_rc(views, 11, out) == 2          # count > max_batch
+    assert (out == 7).all()
+    bad = (ib.IpirQueryView * 2)()
+    bad[0] = views[0]
+    bad[1] = views[1]
+    bad[1].rgsw = C.cast(0, ib.u64p)
+    assert srv.answer_batch_rc(bad, 2, out) == 3             # null view field
+    assert (out == 7).all()
+    assert srv.answer_batch_rc(views, 1, None) == 1          # null output
+    assert srv.answer_batch_rc(views, 0, out) == 0           # empty batch is a no-op
+    assert (out == 7).all()

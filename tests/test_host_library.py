@@ -1,0 +1,86 @@
+"""Host-side checks of the product library without a GPU: it loads, exports
+every symbol include/*.h declares, and its host logic (setup geometry,
+SHAKE-256, expand_seed, synthetic DB) matches the reference / standard."""
+import hashlib
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle_lib import REPO, crs_seed_from
+
+
+def header_symbols():
+    txt = open(os.path.join(REPO, "include", "inspire_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(ipir_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    import inspire_b200 as ib
+    L = ib.library_handle()
+    syms = header_symbols()
+    assert "ipir_server_create" in syms and "ipir_answer_batch" in syms
+    for s in syms:
+        assert hasattr(L, s), s
+    assert sorted(ib.EXPORTED) == syms
+
+
+def test_library_is_sm100a_only():
+    out = os.popen(f"/usr/local/cuda/bin/cuobjdump --list-elf "
+                   f"{os.path.join(REPO, 'inspire-gpu_b200', 'libinspire_b200.so')} 2>&1").read()
+    archs = set(re.findall(r"sm_(\d+a?)", out))
+    assert archs == {"100a"}, archs
+
+
+def test_reference_client_symbols_not_defined():
+    import inspire_b200 as ib
+    L = ib.library_handle()
+    for s in ("ipir_query_build", "ipir_extract", "ipir_query_pack"):
+        assert not hasattr(L, s), s
+
+
+@pytest.mark.parametrize("args", [(65536, 30, 0), (256, 120, 2048), (262144, 120, 2048),
+                                  (1 << 25, 30, 0), (1 << 29, 30, 0), (1 << 22, 960, 0),
+                                  (1 << 31, 30, 0), (1000, 30, 0), (5, 2, 2048)])
+def test_setup_matches_reference(ref, args):
+    import inspire_b200 as ib
+    p = ib.setup(*args)
+    assert [p[k] for k in ("n_entries", "entry_bytes", "db_rows", "db_cols", "n_packed",
+                           "interp_d", "num_cts")] == ref.setup(*args)
+
+
+@pytest.mark.parametrize("args", [(1 << 25, 32, 0), (1 << 22, 1024, 0), (196608, 120, 2048), (25165824, 120, 2048)])
+def test_setup_rejects_what_reference_rejects(ref, args):
+    import inspire_b200 as ib
+    with pytest.raises(ValueError):
+        ref.setup(*args)
+    with pytest.raises(ValueError):
+        ib.setup(*args)
+
+
+def test_shake256_matches_hashlib():
+    import inspire_b200 as ib
+    for n in (0, 1, 135, 136, 137, 272, 500):
+        d = bytes((i * 7 + 3) & 0xFF for i in range(n))
+        for ol in (1, 32, 136, 137, 4096):
+            assert ib.shake256(d, ol) == hashlib.shake_256(d).digest(ol), (n, ol)
+
+
+def test_expand_seed_matches_reference(ref):
+    import inspire_b200 as ib
+    seed = crs_seed_from(9)
+    for dom, idx in (("rlwe", 0), ("rlwe", 31), ("ksk", 502), ("ksk", 409501)):
+        assert (ib.expand_seed(seed, dom, idx).astype(np.uint64) == ref.expand_seed(seed, dom, idx)).all()
+
+
+def test_fill_db_matches_oracle(oracle):
+    import inspire_b200 as ib
+    assert (ib.fill_db(100003, 11) == oracle.fill_db(100003, 11)).all()
+
+
+def test_server_create_rejects_bad_args_without_gpu_work():
+    import inspire_b200 as ib
+    with pytest.raises(ib.InspireError):
+        ib.Server(1 << 25, 32, np.zeros(16, np.uint16))   # geometry rejected before any device call
