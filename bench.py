@@ -231,7 +231,10 @@ def run_ours(args):
     srv = ib.Server(args.n_entries, args.entry_bytes, db, max_batch=max(B, 1), crs_seed=seed)
     t_pre = time.perf_counter() - t0
     del db
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the handle of torch's default stream is 0, which the
+    # C ABI reads as "the server's own stream".
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     srv.set_stream(stream.cuda_stream)
     qn = ib.query_u64s(params)
     rn = ib.response_u64s(params)
@@ -338,7 +341,7 @@ def run_ours(args):
         "db_pass_gbs": db_bytes / (mv1 * 1e-3) / 1e9,
         "stage_ms_b1": st1[-1], "stage_ms_batch": stB[-1],
         "preprocess_s": t_pre,
-        "roofline": {"kernel": "matvec_kernel<1,8> (DB pass, batch 1)", "bound": "hbm",
+        "roofline": {"kernel": ("mv_tc_kernel (tcgen05 int8 DB pass, batch 1)" if os.environ.get("IPB_MATVEC", "tc") != "simt" else "matvec_kernel<1,8> (DB pass, batch 1)"), "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None,
                      "alg_bytes_per_launch": alg_bytes},

@@ -23,6 +23,19 @@ cudaError_t launch_matvec(const uint16_t* db, size_t rows, size_t cols, int chun
                           const uint64_t* qraw, size_t qstride, const DevTables* T,
                           uint32_t* part, size_t part_qstride, int nq, cudaStream_t s);
 
+// Tensor-core mat-vec (tcgen05 kind::i8).  qplanes writes the byte planes
+// planes[8q + 4l + k][rows] of nq queries; launch_matvec_tc runs nq <= 32
+// queries whose planes start at `planes`, writing part[q][chunk][limb][cols]
+// with chunks = rows / kchunk_rows.  *err receives a nonzero code if a
+// pipeline wait times out.
+size_t mv_tc_planes_bytes(size_t rows, int max_queries);
+int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms);
+cudaError_t launch_qplanes(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
+                           uint8_t* planes, int nq, cudaStream_t s);
+cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const uint8_t* planes, int nq,
+                             const DevTables* T, uint32_t* part, size_t part_qstride, int* err, int num_sms,
+                             int kchunk_rows, cudaStream_t s);
+
 // Tensor pass: cpart[q][g][chunk][limb][N] = sum over the chunk's
 // (direction, step) units of D (.) K5[perm].  nq <= 8 queries share the stream.
 cudaError_t launch_collapse(const uint32_t* dp, const uint32_t* dm, size_t groups,

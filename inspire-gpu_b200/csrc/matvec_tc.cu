@@ -1,0 +1,385 @@
+// matvec_tc.cu -- exact database x query mat-vec on the tcgen05 tensor cores.
+//
+//   r_l[q][j] = sum_i db[i][j] * b_{q,l}[i]  mod q_l      (reference src/gpu_online.cu:23-175)
+//
+// The row-major u16 DB is read, unchanged, as a u8 matrix A'[m'][i] with
+// m' = 2j + byte (lo byte at even m', hi byte at odd m'): consecutive m' are
+// contiguous, i.e. an MN-major operand.  Each query word b < 2^27 is split
+// into 4 bytes; B[n][i] with n = 8q + 4l + k holds byte k of b_{q,l}[i]
+// (K-major rows built by qplanes_kernel).  One tcgen05.mma.kind::i8 chain
+// accumulates D[m'][n] = sum_i A'[m'][i] B[n][i] in s32 TMEM.  With K <= 32768
+// rows per chunk every D entry is <= 255*255*32768 < 2^31: exact.  The
+// epilogue forms sum_k 256^k (D[2j][n_k] + 256 D[2j+1][n_k]), which is the
+// exact integer sum_i db[i][j] b[i] (< 2^58), and reduces it mod q_l.  All
+// arithmetic stays exact, so the result equals the reference's.
+//
+// CTA roles (256 threads): warp 0 issues TMA loads (DB tile 256 x 128 rows as
+// two 128-byte boxes, query planes N x 128), warp 1 allocates TMEM and one
+// thread issues the MMAs, warps 4..7 drain TMEM (tcgen05.ld) and write
+// partial sums.  Stages are recycled through mbarriers; every wait is
+// bounded and reports a timeout through *err instead of hanging.
+#include <cuda.h>
+
+#include "ipb_common.cuh"
+#include "ipb_launch.h"
+
+namespace ipb {
+
+namespace {
+
+constexpr int kKT = 128;          // DB rows per pipeline stage (bytes of K)
+constexpr int kMT = 256;          // m' rows per tile (two M = 128 MMAs)
+constexpr int kKChunk = 32768;    // rows per exact s32 accumulation
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait; false (and *err set) on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* err, int code) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it)
+        if (mbar_try(b, parity)) return true;
+    atomicCAS(err, 0, code);
+    return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor (SWIZZLE_128B, sm_100 version bits).
+__device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_u32(p) >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;   // version = 1 (Blackwell)
+    d |= (uint64_t)2 << 61;   // layout = SWIZZLE_128B
+    return d;
+}
+// Instruction descriptor: kind::i8, D s32, A u8 MN-major, B u8 K-major, M = 128.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+    return (2u << 4) | (0u << 7) | (0u << 10) | (1u << 15) | (0u << 16) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct TcParams {
+    uint32_t* part;        // [q][chunk][limb][cols]
+    size_t part_qstride;
+    size_t cols;
+    int nq;                // queries in this pass (<= 32)
+    int npad;              // N (multiple of 16, <= 256)
+    int n_mtiles;
+    int n_kchunks;
+    int kchunk_rows;
+    int stages;
+    int acc_stages;
+    uint32_t tmem_cols;
+    int* err;
+    const DevTables* T;
+};
+
+__global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ CUtensorMap map_a,
+                                                       const __grid_constant__ CUtensorMap map_b, TcParams P) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int S = P.stages;
+    const uint32_t a_bytes = kKT * 128;              // one 128-byte m' box x 128 rows
+    const uint32_t b_bytes = (uint32_t)P.npad * 128;
+    const uint32_t stage_bytes = 2 * a_bytes + b_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + S;
+    uint64_t* tfull = bars + 2 * S;
+    uint64_t* tempty = bars + 2 * S + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 4);
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128); }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(P.tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int n_items = P.n_mtiles * P.n_kchunks;
+    const int ktiles = P.kchunk_rows / kKT;
+
+    if (warp == 0) {
+        // ---------------- TMA producer
+        if (lane == 0) {
+            int s = 0;
+            uint32_t ph = 0;
+            for (int item = blockIdx.x; item < n_items && !abort_flag; item += gridDim.x) {
+                const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
+                const int m0 = mt * kMT;
+                for (int kt = 0; kt < ktiles; ++kt) {
+                    if (!mbar_wait(&empty[s], ph ^ 1, P.err, 1)) { abort_flag = 1; break; }
+                    uint8_t* st = smem + (size_t)s * stage_bytes;
+                    mbar_expect_tx(&full[s], stage_bytes);
+                    const int k0 = kc * P.kchunk_rows + kt * kKT;
+                    tma_load_2d(st, &map_a, &full[s], m0, k0);
+                    tma_load_2d(st + a_bytes, &map_a, &full[s], m0 + 128, k0);
+                    tma_load_2d(st + 2 * a_bytes, &map_b, &full[s], k0, 0);
+                    if (++s == S) { s = 0; ph ^= 1; }
+                }
+            }
+            // drain: every issued stage must be consumed before the CTA exits
+            for (int i = 0; i < S; ++i) {
+                mbar_wait(&empty[s], ph ^ 1, P.err, 2);
+                if (++s == S) { s = 0; ph ^= 1; }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = idesc_i8(P.npad);
+            int s = 0, as = 0;
+            uint32_t ph = 0, aph = 0;
+            for (int item = blockIdx.x; item < n_items && !abort_flag; item += gridDim.x) {
+                if (!mbar_wait(&tempty[as], aph ^ 1, P.err, 3)) { abort_flag = 1; break; }
+                tc_fence_after();
+                const uint32_t d0 = tmem_base + (uint32_t)(as * 2 * P.npad);
+                for (int kt = 0; kt < ktiles; ++kt) {
+                    if (!mbar_wait(&full[s], ph, P.err, 4)) { abort_flag = 1; break; }
+                    tc_fence_after();
+                    const uint8_t* st = smem + (size_t)s * stage_bytes;
+#pragma unroll
+                    for (int kk = 0; kk < kKT / 32; ++kk) {
+                        // A: MN-major, rows of 128 bytes, 8-row swizzle atoms (SBO 1024 B);
+                        // K advances 32 rows = 4096 bytes per MMA.
+                        const uint64_t a0 = smem_desc(st + kk * 4096, 0, 1024);
+                        const uint64_t a1 = smem_desc(st + a_bytes + kk * 4096, 0, 1024);
+                        // B: K-major, 128-byte rows, 8-row groups 1024 B apart; K advances 32 bytes.
+                        const uint64_t b = smem_desc(st + 2 * a_bytes + kk * 32, 16, 1024);
+                        const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+                        mma_i8(d0, a0, b, idesc, acc);
+                        mma_i8(d0 + (uint32_t)P.npad, a1, b, idesc, acc);
+                    }
+                    mma_commit(&empty[s]);
+                    if (++s == S) { s = 0; ph ^= 1; }
+                }
+                mma_commit(&tfull[as]);
+                if (++as == P.acc_stages) { as = 0; aph ^= 1; }
+            }
+        }
+    } else if (warp >= 4) {
+        // ---------------- epilogue: TMEM -> u64 dot products -> mod q
+        const int wq = warp & 3;
+        const uint32_t lane_base = (uint32_t)(wq * 32) << 16;
+        int as = 0;
+        uint32_t aph = 0;
+        const uint64_t cr0 = P.T->limb[0].cr, cr1 = P.T->limb[1].cr;
+        for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+            if (!mbar_wait(&tfull[as], aph, P.err, 5)) { abort_flag = 1; break; }
+            tc_fence_after();
+            const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
+            for (int mb = 0; mb < 2; ++mb) {
+                const size_t j = ((size_t)mt * kMT + mb * 128 + wq * 32 + lane) >> 1;
+                for (int q = 0; q < P.nq; ++q) {
+                    uint32_t v[8];
+                    tmem_ld8(tmem_base + lane_base + (uint32_t)(as * 2 * P.npad + mb * P.npad + 8 * q), v);
+                    uint32_t h[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) h[e] = __shfl_down_sync(0xffffffffu, v[e], 1);
+                    if ((lane & 1) == 0) {
+                        uint64_t r[2];
+#pragma unroll
+                        for (int l = 0; l < 2; ++l) {
+                            uint64_t s = 0;
+#pragma unroll
+                            for (int k = 0; k < 4; ++k)
+                                s += ((uint64_t)v[4 * l + k] + ((uint64_t)h[4 * l + k] << 8)) << (8 * k);
+                            r[l] = s;
+                        }
+                        uint32_t* dst = P.part + (size_t)q * P.part_qstride + (size_t)kc * 2 * P.cols + j;
+                        dst[0] = mod_u64(r[0], cr0, kQ0);
+                        dst[P.cols] = mod_u64(r[1], cr1, kQ1);
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[as]);
+            if (++as == P.acc_stages) { as = 0; aph ^= 1; }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(P.tmem_cols));
+    }
+}
+
+// Byte planes of the query words: planes[8q + 4l + k][i] = byte k of (b_{q,l}[i] mod q_l).
+__global__ void __launch_bounds__(256) qplanes_kernel(const uint64_t* __restrict__ qraw, size_t qstride, size_t rows,
+                                                      const DevTables* __restrict__ T, uint8_t* __restrict__ planes) {
+    const int q = blockIdx.y;
+    const size_t i4 = ((size_t)blockIdx.x * 256 + threadIdx.x) * 4;
+    if (i4 >= rows) return;
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+        const uint64_t* src = qraw + (size_t)q * qstride + (size_t)l * rows + i4;
+        uint32_t w[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) w[c] = mod_u64(src[c], T->limb[l].cr, T->limb[l].q);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint32_t packed = 0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) packed |= ((w[c] >> (8 * k)) & 0xFFu) << (8 * c);
+            *reinterpret_cast<uint32_t*>(planes + ((size_t)(8 * q + 4 * l + k)) * rows + i4) = packed;
+        }
+    }
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) == cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+}  // namespace
+
+size_t mv_tc_planes_bytes(size_t rows, int max_queries) { return (size_t)8 * max_queries * rows + 16 * rows; }
+
+cudaError_t launch_qplanes(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T, uint8_t* planes,
+                           int nq, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    if (rows % 1024) return cudaErrorInvalidValue;
+    qplanes_kernel<<<dim3((unsigned)(rows / 1024), nq), 256, 0, s>>>(qraw, qstride, rows, T, planes);
+    return cudaGetLastError();
+}
+
+// nq <= 32 queries whose planes start at `planes` (rows bytes per plane row).
+int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms) {
+    // Rows per exact s32 accumulation: at most 32768, halved while the
+    // (m'-tile, chunk) work items would leave SMs idle.
+    size_t kc = rows < (size_t)kKChunk ? rows : (size_t)kKChunk;
+    const size_t mtiles = (2 * cols) / kMT;
+    while (mtiles * (rows / kc) < (size_t)(2 * num_sms) && kc > 1024 && kc % 2 == 0) kc /= 2;
+    return (int)kc;
+}
+
+cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const uint8_t* planes, int nq,
+                             const DevTables* T, uint32_t* part, size_t part_qstride, int* err, int num_sms,
+                             int kchunk_rows, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    if (nq > 32 || rows % kKT || cols % 128) return cudaErrorInvalidValue;
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    const int npad = ((8 * nq + 15) / 16) * 16;
+    const int kchunk = kchunk_rows;
+    if (kchunk <= 0 || kchunk > kKChunk || kchunk % kKT || rows % (size_t)kchunk) return cudaErrorInvalidValue;
+    CUtensorMap ma, mb;
+    {
+        cuuint64_t dims[2] = {(cuuint64_t)(2 * cols), (cuuint64_t)rows};
+        cuuint64_t strides[1] = {(cuuint64_t)(2 * cols)};
+        cuuint32_t box[2] = {128, (cuuint32_t)kKT};
+        cuuint32_t es[2] = {1, 1};
+        if (enc(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)db, dims, strides, box, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    }
+    {
+        cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)npad};
+        cuuint64_t strides[1] = {(cuuint64_t)rows};
+        cuuint32_t box[2] = {128, (cuuint32_t)npad};
+        cuuint32_t es[2] = {1, 1};
+        if (enc(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)planes, dims, strides, box, es,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    }
+    TcParams P{};
+    P.part = part;
+    P.part_qstride = part_qstride;
+    P.cols = cols;
+    P.nq = nq;
+    P.npad = npad;
+    P.n_mtiles = (int)((2 * cols) / kMT);
+    P.kchunk_rows = kchunk;
+    P.n_kchunks = (int)(rows / kchunk);
+    P.acc_stages = (4 * npad <= 512) ? 2 : 1;
+    uint32_t need = (uint32_t)(P.acc_stages * 2 * npad);
+    uint32_t tc = 32;
+    while (tc < need) tc <<= 1;
+    P.tmem_cols = tc;
+    P.err = err;
+    P.T = T;
+    const size_t stage_bytes = 2 * (size_t)kKT * 128 + (size_t)npad * 128;
+    const size_t budget = 200 * 1024;
+    P.stages = (int)std::min<size_t>(8, budget / stage_bytes);
+    if (P.stages < 2) return cudaErrorInvalidValue;
+    const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
+    cudaError_t e = cudaFuncSetAttribute(mv_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e) return e;
+    const int items = P.n_mtiles * P.n_kchunks;
+    const int grid = std::min(items, std::max(1, num_sms));
+    mv_tc_kernel<<<grid, 256, smem, s>>>(ma, mb, P);
+    return cudaGetLastError();
+}
+
+}  // namespace ipb

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -229,8 +230,14 @@ struct Server {
     uint32_t* cpart = nullptr;
     uint32_t* packed_b = nullptr;
     uint64_t* resp = nullptr;
+    uint8_t* planes = nullptr;   // query byte planes for the tensor-core mat-vec
+    int* d_err = nullptr;        // device error word (pipeline wait timeouts)
     size_t qstride = 0, mv_qstride = 0, cpart_qstride = 0, pb_qstride = 0, resp_qstride = 0;
     int mv_chunks = 1, c_chunks = 1;
+    bool use_tc = true;          // tcgen05 mat-vec (IPB_MATVEC=simt selects the CUDA-core kernel)
+    int num_sms = 148;
+    int tc_kchunk_rows = 0, tc_kchunks = 1;
+    int last_mv_chunks = 1;
     size_t staged = 0;
     bool timing = false;
     cudaEvent_t ev[6] = {};
@@ -275,7 +282,11 @@ static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_
     // limbs x rows x 4 B) within 128 KB of shared memory.
     while (R / (size_t)S->mv_chunks > 4096) S->mv_chunks *= 2;
     S->c_chunks = (int)std::clamp<size_t>((1184 + 2 * G - 1) / (2 * G), 2, 64);
-    S->mv_qstride = (size_t)S->mv_chunks * 2 * C;
+    IPB_CK(cudaDeviceGetAttribute(&S->num_sms, cudaDevAttrMultiProcessorCount, S->device));
+    if (const char* m = std::getenv("IPB_MATVEC")) S->use_tc = std::strcmp(m, "simt") != 0;
+    S->tc_kchunk_rows = matvec_tc_kchunk_rows(R, C, S->num_sms);
+    S->tc_kchunks = (int)(R / (size_t)S->tc_kchunk_rows);
+    S->mv_qstride = (size_t)std::max(S->mv_chunks, S->tc_kchunks) * 2 * C;
     S->cpart_qstride = G * (size_t)S->c_chunks * 2 * kN;
     S->pb_qstride = G * 2 * kN;
     S->resp_qstride = pp.num_cts * 4 * kN;
@@ -287,6 +298,10 @@ static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_
     S->cpart = A.alloc<uint32_t>(max_batch * S->cpart_qstride);
     S->packed_b = A.alloc<uint32_t>(max_batch * S->pb_qstride);
     S->resp = A.alloc<uint64_t>(max_batch * S->resp_qstride);
+    S->planes = A.alloc<uint8_t>(mv_tc_planes_bytes(R, (int)max_batch));
+    IPB_CK(cudaMemset(S->planes, 0, mv_tc_planes_bytes(R, (int)max_batch)));
+    S->d_err = A.alloc<int>(1);
+    IPB_CK(cudaMemset(S->d_err, 0, sizeof(int)));
     for (auto& e : S->ev) IPB_CK(cudaEventCreate(&e));
     pre->adopted = true;
     S->resident_bytes = pre->arena.bytes + A.bytes;
@@ -320,10 +335,21 @@ static void run_pipeline(Server* S, size_t count) {
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[0], st));
     IPB_CK(launch_qprep(S->qraw, S->qstride, R, P.tables, S->keys, S->rgsw32, nq, st));
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[1], st));
-    for (size_t c0 = 0; c0 < count; c0 += 4) {
-        const int n = (int)std::min<size_t>(4, count - c0);
-        IPB_CK(launch_matvec(P.db, R, C, S->mv_chunks, S->qraw + c0 * S->qstride, S->qstride, P.tables,
-                             S->mvpart + c0 * S->mv_qstride, S->mv_qstride, n, st));
+    if (S->use_tc) {
+        IPB_CK(launch_qplanes(S->qraw, S->qstride, R, P.tables, S->planes, nq, st));
+        for (size_t c0 = 0; c0 < count; c0 += 32) {
+            const int n = (int)std::min<size_t>(32, count - c0);
+            IPB_CK(launch_matvec_tc(P.db, R, C, S->planes + 8 * c0 * R, n, P.tables, S->mvpart + c0 * S->mv_qstride,
+                                    S->mv_qstride, S->d_err, S->num_sms, S->tc_kchunk_rows, st));
+        }
+        S->last_mv_chunks = S->tc_kchunks;
+    } else {
+        for (size_t c0 = 0; c0 < count; c0 += 4) {
+            const int n = (int)std::min<size_t>(4, count - c0);
+            IPB_CK(launch_matvec(P.db, R, C, S->mv_chunks, S->qraw + c0 * S->qstride, S->qstride, P.tables,
+                                 S->mvpart + c0 * S->mv_qstride, S->mv_qstride, n, st));
+        }
+        S->last_mv_chunks = S->mv_chunks;
     }
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[2], st));
     for (size_t c0 = 0; c0 < count; c0 += 8) {
@@ -332,7 +358,7 @@ static void run_pipeline(Server* S, size_t count) {
                                S->cpart + c0 * S->cpart_qstride, S->cpart_qstride, n, P.tables, st));
     }
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[3], st));
-    IPB_CK(launch_finalize(S->mvpart, S->mv_qstride, S->mv_chunks, C, S->cpart, S->cpart_qstride, S->c_chunks,
+    IPB_CK(launch_finalize(S->mvpart, S->mv_qstride, S->last_mv_chunks, C, S->cpart, S->cpart_qstride, S->c_chunks,
                            P.pre_df, S->keys, kKeyStride, P.tables, S->packed_b, S->pb_qstride, G, nq, st));
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[4], st));
     IPB_CK(launch_horner(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts, S->resp,
@@ -340,10 +366,22 @@ static void run_pipeline(Server* S, size_t count) {
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[5], st));
 }
 
+// A kernel whose pipeline wait ran out of iterations leaves a code in the
+// device error word; report it (the responses are then not valid).
+static void check_device_error(Server* S) {
+    int e = 0;
+    IPB_CK(cudaMemcpy(&e, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        IPB_CK(cudaMemset(S->d_err, 0, sizeof(int)));
+        throw std::runtime_error("device pipeline wait timed out (code " + std::to_string(e) + ")");
+    }
+}
+
 static void fetch(Server* S, size_t count, uint64_t* out) {
     IPB_CK(cudaSetDevice(S->device));
     IPB_CK(cudaMemcpyAsync(out, S->resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, S->stream));
     IPB_CK(cudaStreamSynchronize(S->stream));
+    check_device_error(S);
     if (S->timing)
         for (int i = 0; i < 5; ++i) IPB_CK(cudaEventElapsedTime(&S->stage_ms[i], S->ev[i], S->ev[i + 1]));
 }
