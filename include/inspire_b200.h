@@ -140,6 +140,19 @@ int ipir_b200_decomp(const uint32_t* in, uint32_t* out, size_t n);
 int ipir_b200_shake256(const uint8_t* in, size_t inlen, uint8_t* out, size_t outlen);
 int ipir_b200_expand_seed(const uint8_t* seed64, const char* domain, uint64_t index, uint32_t* out);
 
+/* Standalone exact mat-vec on the tensor cores (the DB pass of the answer,
+ * reference src/gpu_online.cu:23-175 gpu_matvec_dual / _batched), on device
+ * pointers: out[q][limb][c] = sum_i db[i][c] * (queries[q][limb][i] mod q_limb)
+ * mod q_limb for q < count.  db: rows x cols u16 row-major; queries:
+ * count x [2][rows] u64; out: count x [2][cols] u32.  rows a multiple of
+ * 1024 (of 32768 above 32768), cols a multiple of 128.  Scratch (query byte
+ * planes, K-chunk partials, tables) is allocated on the first call per
+ * device and grown on demand; calls on one device must not overlap.
+ * Enqueued on `stream`; with sync != 0 the call waits and reports a device
+ * wait timeout as 5.  Returns 0, 1 null argument, 2 bad shape, 4 CUDA error. */
+int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
+                     uint32_t* out, void* stream, int sync);
+
 /* Synthetic database for benchmarks and tests: out[k] = splitmix64(seed ^ k)
  * mod 65535 for k < count, filled on all host threads. */
 int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed);

@@ -30,5 +30,7 @@ void expand_seed(const uint8_t seed[kSeedBytes], const char* domain, uint64_t in
 void build_tables(DevTables& T);
 // 0 on success; otherwise an error code and *why (static string).
 int setup_geometry(size_t n_entries, size_t w, size_t db_rows, Params* out, const char** why);
+// Sets the calling thread's text for ipir_b200_last_error().
+void set_last_error(const char* msg);
 
 }  // namespace ipb

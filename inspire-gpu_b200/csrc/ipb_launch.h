@@ -36,6 +36,10 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
                              const DevTables* T, uint32_t* part, size_t part_qstride, int* err, int num_sms,
                              int kchunk_rows, cudaStream_t s);
 
+// out[q][limb][cols] = sum over chunks of part[q][chunk][limb][cols] mod q.
+cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, int chunks, size_t cols,
+                                   const DevTables* T, uint32_t* out, size_t out_qstride, int nq, cudaStream_t s);
+
 // Tensor pass: cpart[q][g][chunk][limb][N] = sum over the chunk's
 // (direction, step) units of D (.) K5[perm].  nq <= 8 queries share the stream.
 cudaError_t launch_collapse(const uint32_t* dp, const uint32_t* dm, size_t groups,

@@ -284,6 +284,20 @@ __global__ void __launch_bounds__(256) qplanes_kernel(const uint64_t* __restrict
     }
 }
 
+// out[q][l][c] = sum over K-chunks of part[q][chunk][l][c]  mod q_l.
+__global__ void __launch_bounds__(256) mv_chunk_reduce_kernel(const uint32_t* __restrict__ part, size_t part_qstride,
+                                                              int chunks, size_t cols, const DevTables* __restrict__ T,
+                                                              uint32_t* __restrict__ out, size_t out_qstride) {
+    const int q = blockIdx.y;
+    const size_t idx = (size_t)blockIdx.x * 256 + threadIdx.x;
+    if (idx >= 2 * cols) return;
+    const int l = (int)(idx / cols);
+    const size_t c = idx % cols;
+    uint64_t s = 0;
+    for (int ch = 0; ch < chunks; ++ch) s += part[(size_t)q * part_qstride + ((size_t)ch * 2 + l) * cols + c];
+    out[(size_t)q * out_qstride + (size_t)l * cols + c] = mod_u64(s, T->limb[l].cr, T->limb[l].q);
+}
+
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -303,6 +317,14 @@ EncodeTiledFn encode_fn() {
 }  // namespace
 
 size_t mv_tc_planes_bytes(size_t rows, int max_queries) { return (size_t)8 * max_queries * rows + 16 * rows; }
+
+cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, int chunks, size_t cols,
+                                   const DevTables* T, uint32_t* out, size_t out_qstride, int nq, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    mv_chunk_reduce_kernel<<<dim3((unsigned)((2 * cols + 255) / 256), nq), 256, 0, s>>>(part, part_qstride, chunks,
+                                                                                         cols, T, out, out_qstride);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_qplanes(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T, uint8_t* planes,
                            int nq, cudaStream_t s) {
@@ -383,3 +405,4 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
 }
 
 }  // namespace ipb
+

@@ -94,6 +94,8 @@ constexpr size_t kKeyStride = 4 * kDeff * kN;                      // keys per q
 constexpr size_t kRgswStride = 4 * kBlk;                           // rgsw32 per query (u32)
 }  // namespace
 
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 // --------------------------------------------------------------- precomp state
 struct Precomp {
     Params pp{};
@@ -743,6 +745,81 @@ int ipir_b200_decomp(const uint32_t* in, uint32_t* out, size_t n) {
                 throw;
             }
             A.free_all();
+            return 0;
+        },
+        4);
+}
+
+namespace {
+// Scratch of ipir_b200_matvec, cached per device and grown on demand.
+struct MvScratch {
+    ipb::DevArena arena;
+    ipb::DevTables* T = nullptr;
+    int* err = nullptr;
+    uint8_t* planes = nullptr;
+    size_t planes_cap = 0;
+    uint32_t* part = nullptr;
+    size_t part_cap = 0;
+};
+std::mutex g_mv_mu;
+MvScratch g_mv[64];
+}  // namespace
+
+int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
+                     uint32_t* out, void* stream, int sync) {
+    if (!db || !queries || !out) return 1;
+    if (count == 0) return 0;
+    if (rows == 0 || rows % 1024 || cols == 0 || cols % 128 || (rows > 32768 && rows % 32768)) {
+        ipb::g_last_error = "ipir_b200_matvec: rows must be a multiple of 1024 (of 32768 above 32768), "
+                            "cols a multiple of 128";
+        return 2;
+    }
+    return guarded(
+        [&]() -> int {
+            int dev = 0, sms = 0;
+            IPB_CK(cudaGetDevice(&dev));
+            if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
+            IPB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            cudaStream_t s = static_cast<cudaStream_t>(stream);
+            std::lock_guard<std::mutex> lk(g_mv_mu);
+            MvScratch& M = g_mv[dev];
+            if (!M.T) {
+                M.T = ipb::upload_tables(M.arena, 0);
+                M.err = M.arena.alloc<int>(1);
+                IPB_CK(cudaMemset(M.err, 0, sizeof(int)));
+                IPB_CK(cudaDeviceSynchronize());  // tables visible to any stream
+            }
+            const size_t kchunk = rows < 32768 ? rows : 32768;
+            const int chunks = (int)(rows / kchunk);
+            const size_t pbytes = ipb::mv_tc_planes_bytes(rows, (int)count);
+            if (pbytes > M.planes_cap) {
+                M.planes = M.arena.alloc<uint8_t>(pbytes);
+                M.planes_cap = pbytes;
+            }
+            const size_t pq = (size_t)chunks * 2 * cols;
+            if (chunks > 1 && pq * count > M.part_cap) {
+                M.part = M.arena.alloc<uint32_t>(pq * count);
+                M.part_cap = pq * count;
+            }
+            IPB_CK(ipb::launch_qplanes(queries, 2 * rows, rows, M.T, M.planes, (int)count, s));
+            for (size_t q0 = 0; q0 < count; q0 += 32) {
+                const int n = (int)std::min<size_t>(32, count - q0);
+                uint32_t* dst = chunks == 1 ? out + q0 * 2 * cols : M.part + q0 * pq;
+                IPB_CK(ipb::launch_matvec_tc(db, rows, cols, M.planes + 8 * q0 * rows, n, M.T, dst,
+                                             chunks == 1 ? 2 * cols : pq, M.err, sms, (int)kchunk, s));
+            }
+            if (chunks > 1)
+                IPB_CK(ipb::launch_mv_chunk_reduce(M.part, pq, chunks, cols, M.T, out, 2 * cols, (int)count, s));
+            if (sync) {
+                IPB_CK(cudaStreamSynchronize(s));
+                int e = 0;
+                IPB_CK(cudaMemcpy(&e, M.err, sizeof(int), cudaMemcpyDeviceToHost));
+                if (e) {
+                    IPB_CK(cudaMemset(M.err, 0, sizeof(int)));
+                    ipb::g_last_error = "ipir_b200_matvec: device pipeline wait timed out";
+                    return 5;
+                }
+            }
             return 0;
         },
         4);

@@ -87,6 +87,8 @@ _L.ipir_b200_decomp.argtypes = [u32p, u32p, C.c_size_t]
 _L.ipir_b200_shake256.argtypes = [u8p, C.c_size_t, u8p, C.c_size_t]
 _L.ipir_b200_expand_seed.argtypes = [u8p, C.c_char_p, C.c_uint64, u32p]
 _L.ipir_b200_fill_db.argtypes = [u16p, C.c_size_t, C.c_uint64]
+_L.ipir_b200_matvec.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
+                                C.c_void_p, C.c_int]
 
 EXPORTED = [
     "ipir_server_create", "ipir_server_caps", "ipir_answer_batch", "ipir_server_destroy",
@@ -94,6 +96,7 @@ EXPORTED = [
     "ipir_b200_run", "ipir_b200_fetch_responses", "ipir_b200_sync", "ipir_b200_enable_stage_timing",
     "ipir_b200_stage_times", "ipir_b200_export_precomp", "ipir_b200_export_db", "ipir_b200_ntt",
     "ipir_b200_decomp", "ipir_b200_shake256", "ipir_b200_expand_seed", "ipir_b200_fill_db",
+    "ipir_b200_matvec",
 ]
 
 
@@ -337,3 +340,13 @@ def fill_db(count, seed, out=None):
         out = np.empty(count, np.uint16)
     _L.ipir_b200_fill_db(_ptr(out, u16p), count, seed)
     return out
+
+
+def matvec(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0, sync=True):
+    """Exact tensor-core mat-vec on device pointers (ints):
+    out[q][limb][c] = sum_i db[i][c] * queries[q][limb][i] mod q_limb."""
+    rc = _L.ipir_b200_matvec(C.c_void_p(db_ptr), rows, cols, C.c_void_p(queries_ptr), count,
+                             C.c_void_p(out_ptr), C.c_void_p(stream or 0), 1 if sync else 0)
+    if rc:
+        raise InspireError(f"ipir_b200_matvec rc={rc}: {last_error()}")
+
