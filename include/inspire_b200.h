@@ -153,6 +153,24 @@ int ipir_b200_expand_seed(const uint8_t* seed64, const char* domain, uint64_t in
 int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
                      uint32_t* out, void* stream, int sync);
 
+/* Same result as ipir_b200_matvec, for callers that may not allocate device
+ * memory: processes whose device memory belongs to an allocator or pool they
+ * must not bypass, or code that cannot afford cudaMalloc's implicit device
+ * synchronisation.  No counterpart in the reference.  It allocates nothing:
+ * its scratch (tables, error word, query byte planes) is a fixed ~2.7 MB
+ * array in the library's device image, which every GPU that loads the
+ * library keeps until the process exits.  Limits: rows a multiple of 1024
+ * and <= 32768, count <= 8, cols a multiple of 128; larger shapes return 2
+ * with the reason in ipir_b200_last_error().  The first call on a device
+ * resolves the array's device address and writes the NTT tables into it:
+ * make that first call before any stream capture.  All calls share the one
+ * array, so calls whose GPU work overlaps (other streams, other threads)
+ * race; serialise them.  The call synchronises `stream` and returns 0, 1
+ * null argument, 2 shape beyond the limits, 4 CUDA error, 5 device wait
+ * timeout. */
+int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries,
+                             size_t count, uint32_t* out, void* stream);
+
 /* Synthetic database for benchmarks and tests: out[k] = splitmix64(seed ^ k)
  * mod 65535 for k < count, filled on all host threads. */
 int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed);

@@ -89,6 +89,8 @@ _L.ipir_b200_expand_seed.argtypes = [u8p, C.c_char_p, C.c_uint64, u32p]
 _L.ipir_b200_fill_db.argtypes = [u16p, C.c_size_t, C.c_uint64]
 _L.ipir_b200_matvec.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                 C.c_void_p, C.c_int]
+_L.ipir_b200_matvec_noalloc.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t,
+                                        C.c_void_p, C.c_void_p]
 
 EXPORTED = [
     "ipir_server_create", "ipir_server_caps", "ipir_answer_batch", "ipir_server_destroy",
@@ -96,7 +98,7 @@ EXPORTED = [
     "ipir_b200_run", "ipir_b200_fetch_responses", "ipir_b200_sync", "ipir_b200_enable_stage_timing",
     "ipir_b200_stage_times", "ipir_b200_export_precomp", "ipir_b200_export_db", "ipir_b200_ntt",
     "ipir_b200_decomp", "ipir_b200_shake256", "ipir_b200_expand_seed", "ipir_b200_fill_db",
-    "ipir_b200_matvec",
+    "ipir_b200_matvec", "ipir_b200_matvec_noalloc",
 ]
 
 
@@ -350,3 +352,10 @@ def matvec(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0, sync=True)
     if rc:
         raise InspireError(f"ipir_b200_matvec rc={rc}: {last_error()}")
 
+
+def matvec_noalloc_rc(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0):
+    """ipir_b200_matvec_noalloc on device pointers; returns the C return code.
+    Allocates nothing: its scratch is a fixed array in the library (rows <=
+    32768, count <= 8); the first call on a device sets it up."""
+    return _L.ipir_b200_matvec_noalloc(C.c_void_p(db_ptr), rows, cols, C.c_void_p(queries_ptr), count,
+                                       C.c_void_p(out_ptr), C.c_void_p(stream or 0))
