@@ -40,19 +40,24 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
 cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, int chunks, size_t cols,
                                    const DevTables* T, uint32_t* out, size_t out_qstride, int nq, cudaStream_t s);
 
-// Tensor pass: cpart[q][g][chunk][limb][N] = sum over the chunk's
-// (direction, step) units of D (.) K5[perm].  nq <= 8 queries share the stream.
-cudaError_t launch_collapse(const uint32_t* dp, const uint32_t* dm, size_t groups,
-                            const uint32_t* keys, size_t key_qstride, int nchunks,
-                            uint32_t* cpart, size_t cpart_qstride, int nq, const DevTables* T,
-                            cudaStream_t s);
+// Tensor pass on tcgen05 (tensorpass_tc.cu).  Dt: re-laid-out D tensors
+// [l][i][g*4 + a][4096] u8; Gt: per-batch permuted-key planes; tp_out:
+// [l][i][q][g] u32 for the nq_total queries of the batch.
+size_t tp_dt_bytes(size_t groups);
+size_t tp_gt_bytes(int max_pass);
+int tp_pass_queries(size_t groups);
+cudaError_t launch_dt_transpose(const uint32_t* dp, const uint32_t* dm, size_t g0, size_t nw, size_t G, uint8_t* Dt,
+                                cudaStream_t s);
+cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp, uint32_t* dm, cudaStream_t s);
+cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
+                               int nq_total, int q0, uint8_t* Gt, uint32_t* tp_out, int* err, int num_sms,
+                               cudaStream_t s);
 
-// packed_b[q][g][limb][N] = NTT(sum_y mvpart) - sum_ch cpart - Dfinal (.) Kn1.
+// packed_b[q][g][limb][N] = NTT(sum_y mvpart) - tp_out - Dfinal (.) Kn1.
 cudaError_t launch_finalize(const uint32_t* mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
-                            const uint32_t* cpart, size_t cpart_qstride, int cchunks,
-                            const uint32_t* df, const uint32_t* keys, size_t key_qstride,
-                            const DevTables* T, uint32_t* packed_b, size_t pb_qstride,
-                            size_t groups, int nq, cudaStream_t s);
+                            const uint32_t* tp_out, const uint32_t* df, const uint32_t* keys, size_t key_qstride,
+                            const DevTables* T, uint32_t* packed_b, size_t pb_qstride, size_t groups, int nq,
+                            cudaStream_t s);
 
 // Horner chains, one CTA per (ct, query): resp[q][ct][a|b][limb][N] u64.
 cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,

@@ -1,10 +1,10 @@
 // online.cu -- per-query kernels of the B200 InsPIRe server.
 //
 // One answer (gpu_answer / gpu_answer_batch, reference src/gpu_protocol.cu:
-// 1121-1535) runs five launches on one stream:
+// 1121-1535) runs these launches on one stream:
 //   qprep     key-switching keys to NTT form, RGSW to u32 residues
 //   matvec    r_l[j] = sum_i db[i][j] * b_l[i] mod q_l   (DB pass, HBM bound)
-//   collapse  tensor pass: sum_{dir,s,j} D[s][j][i] * K5[j][perm_s(i)]
+//   tensor pass (tensorpass_tc.cu): sum_{dir,s,j} D[s][j][i] * K5[j][perm_s(i)]
 //   finalize  per group: NTT(r slice) - tensor partials - D_final (.) Kneg1
 //   horner    one persistent CTA per response ciphertext runs the whole
 //             ExtProd chain (INTT, decomp, NTT, MAC) in shared memory
@@ -145,90 +145,14 @@ __global__ void __launch_bounds__(256) matvec_kernel(const uint16_t* __restrict_
     }
 }
 
-// ------------------------------------------------------------------ collapse
-// Tensor pass (InspiRINGOnline, reference src/gpu_online.cu:593-714): for
-// group g, limb l and a chunk of the 2*1023 (direction, step) units,
-//   cpart[i] = sum_units sum_j D[s][j][i] * K5[j][perm_t(i)]  mod q,
-// t = 5^(N/2-2-s) (forward) or 2N - 5^(N/2-2-s) (conjugate), as the
-// reference's permutation tables (src/gpu_protocol.cu:189-213).  The slot
-// permutation is computed in registers (no table).  Thread t owns slots
-// x = t + 256e: lanes then differ in the low five bits of x, which makes the
-// gathers K5[perm_t(x)] hit 32 distinct shared-memory banks for every t.
-// BT queries share each D element read from HBM.
-template <int BT>
-__global__ void __launch_bounds__(256) collapse_kernel(const uint32_t* __restrict__ dp,
-                                                       const uint32_t* __restrict__ dm,
-                                                       const uint32_t* __restrict__ keys, size_t key_qstride,
-                                                       int nchunks, uint32_t* __restrict__ cpart,
-                                                       size_t cpart_qstride, int nq,
-                                                       const DevTables* __restrict__ T) {
-    extern __shared__ __align__(16) uint32_t sk[];  // [BT][digit][N]
-    const int g = blockIdx.x, l = blockIdx.y, ch = blockIdx.z;
-    const uint32_t t = threadIdx.x;
-    const uint32_t q = T->limb[l].q;
-    const uint64_t cr = T->limb[l].cr;
-    for (int b = 0; b < BT; ++b) {
-        const int src = b < nq ? b : 0;
-        const uint32_t* kp = keys + (size_t)src * key_qstride + (size_t)(l * kDeff) * kN;  // key 0 = ksk5
-        for (int i = t; i < kDeff * kN; i += 256) sk[b * kDeff * kN + i] = kp[i];
-    }
-    __syncthreads();
-    const int units = 2 * kSteps;
-    const int per = (units + nchunks - 1) / nchunks;
-    const int u0 = ch * per, u1 = min(units, u0 + per);
-    uint32_t odd[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) odd[e] = 2 * brev11(t + 256 * e) + 1;
-    uint64_t acc[BT][8];
-#pragma unroll
-    for (int b = 0; b < BT; ++b)
-#pragma unroll
-        for (int e = 0; e < 8; ++e) acc[b][e] = 0;
-    const size_t gstride = (size_t)2 * kSteps * kDeff * kN;
-    int dir = u0 >= kSteps;
-    int s = dir ? u0 - kSteps : u0;
-    uint32_t tf = pow5_mod2n(kHalf - 2 - s);
-    int cnt = 0;
-    for (int u = u0; u < u1; ++u) {
-        if (s == kSteps) { dir = 1; s = 0; tf = pow5_mod2n(kHalf - 2); }
-        const uint32_t tt = dir ? ((2 * kN - tf) & (2 * kN - 1)) : tf;
-        const uint32_t* D = (dir ? dm : dp) + (size_t)g * gstride + (size_t)(l * kSteps + s) * kDeff * kN;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const uint32_t x = t + 256 * e;
-            const uint32_t pi = perm_from_odd(tt, odd[e]);
-            const uint64_t d0 = __ldcs(D + x);
-            const uint64_t d1 = __ldcs(D + kN + x);
-#pragma unroll
-            for (int b = 0; b < BT; ++b)
-                acc[b][e] += d0 * sk[(b * kDeff + 0) * kN + pi] + d1 * sk[(b * kDeff + 1) * kN + pi];
-        }
-        if (++cnt == 256) {
-            cnt = 0;
-#pragma unroll
-            for (int b = 0; b < BT; ++b)
-#pragma unroll
-                for (int e = 0; e < 8; ++e) acc[b][e] = mod_u64(acc[b][e], cr, q);
-        }
-        ++s;
-        tf = (tf * kInv5) & (2 * kN - 1);
-    }
-#pragma unroll
-    for (int b = 0; b < BT; ++b) {
-        if (b >= nq) break;
-        uint32_t* dst = cpart + (size_t)b * cpart_qstride + (((size_t)g * nchunks + ch) * 2 + l) * kN;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) dst[t + 256 * e] = mod_u64(acc[b][e], cr, q);
-    }
-}
-
 // ------------------------------------------------------------------ finalize
 // Per (group, limb, query): b = NTT(sum of the mat-vec partials of the
-// group's N columns) - tensor partials - sum_j D_final[j] (.) Kneg1[j]
+// group's N columns) - tensor pass - sum_j D_final[j] (.) Kneg1[j]
 // (reference src/gpu_protocol.cu:1233-1274, src/gpu_online.cu:547-559).
+// The tensor pass result is tp_out[l][i][q][g] (tensorpass_tc.cu).
 __global__ void __launch_bounds__(256) finalize_kernel(
     const uint32_t* __restrict__ mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
-    const uint32_t* __restrict__ cpart, size_t cpart_qstride, int cchunks,
+    const uint32_t* __restrict__ tp_out, int nq_total, int groups,
     const uint32_t* __restrict__ df, const uint32_t* __restrict__ keys, size_t key_qstride,
     const DevTables* __restrict__ T, uint32_t* __restrict__ packed_b, size_t pb_qstride) {
     __shared__ __align__(16) uint32_t sbuf[2 * kN];
@@ -245,15 +169,10 @@ __global__ void __launch_bounds__(256) finalize_kernel(
         r[e] = mod_u64(s, L.cr, L.q);
     }
     ntt_fwd(r, sbuf, L.fwd, L.q, t, 0);
-    uint64_t cs[8];
+    uint32_t cs[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) cs[e] = 0;
-    for (int ch = 0; ch < cchunks; ++ch) {
-        uint32_t v[8];
-        ld8(cpart + (size_t)b * cpart_qstride + (((size_t)g * cchunks + ch) * 2 + l) * kN + 8 * t, v);
-#pragma unroll
-        for (int e = 0; e < 8; ++e) cs[e] += v[e];
-    }
+    for (int e = 0; e < 8; ++e)
+        cs[e] = tp_out[(((size_t)l * kN + 8 * t + e) * nq_total + b) * groups + g];
     uint32_t d0[8], d1[8], k0[8], k1[8];
     ld8(df + ((size_t)g * 2 + l) * kDeff * kN + 8 * t, d0);
     ld8(df + (((size_t)g * 2 + l) * kDeff + 1) * kN + 8 * t, d1);
@@ -264,7 +183,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         const uint32_t fin = mod_u64((uint64_t)d0[e] * k0[e] + (uint64_t)d1[e] * k1[e], L.cr, L.q);
-        const uint32_t sub = add_mod(mod_u64(cs[e], L.cr, L.q), fin, L.q);
+        const uint32_t sub = add_mod(cs[e], fin, L.q);
         o[e] = sub_mod(r[e], sub, L.q);
     }
     st8(packed_b + (size_t)b * pb_qstride + ((size_t)g * 2 + l) * kN + 8 * t, o);
@@ -446,37 +365,14 @@ cudaError_t launch_matvec(const uint16_t* db, size_t rows, size_t cols, int chun
     return cudaGetLastError();
 }
 
-cudaError_t launch_collapse(const uint32_t* dp, const uint32_t* dm, size_t groups, const uint32_t* keys,
-                              size_t key_qstride, int nchunks, uint32_t* cpart, size_t cpart_qstride, int nq,
-                              const DevTables* T, cudaStream_t s) {
-    if (nq <= 0) return cudaSuccess;
-    if (nq > 8 || nchunks <= 0) return cudaErrorInvalidValue;
-    const int bt = nq == 1 ? 1 : (nq == 2 ? 2 : (nq <= 4 ? 4 : 8));
-    const size_t smem = (size_t)bt * kDeff * kN * sizeof(uint32_t);
-    dim3 grid((unsigned)groups, 2, nchunks);
-    cudaError_t e;
-#define IPB_COLLAPSE(BTV)                                                                              \
-    {                                                                                                  \
-        auto k = collapse_kernel<BTV>;                                                                 \
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e; \
-        k<<<grid, 256, smem, s>>>(dp, dm, keys, key_qstride, nchunks, cpart, cpart_qstride, nq, T);     \
-    }
-    if (bt == 1) IPB_COLLAPSE(1)
-    else if (bt == 2) IPB_COLLAPSE(2)
-    else if (bt == 4) IPB_COLLAPSE(4)
-    else IPB_COLLAPSE(8)
-#undef IPB_COLLAPSE
-    return cudaGetLastError();
-}
-
 cudaError_t launch_finalize(const uint32_t* mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
-                            const uint32_t* cpart, size_t cpart_qstride, int cchunks, const uint32_t* df,
-                            const uint32_t* keys, size_t key_qstride, const DevTables* T, uint32_t* packed_b,
-                            size_t pb_qstride, size_t groups, int nq, cudaStream_t s) {
+                            const uint32_t* tp_out, const uint32_t* df, const uint32_t* keys, size_t key_qstride,
+                            const DevTables* T, uint32_t* packed_b, size_t pb_qstride, size_t groups, int nq,
+                            cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    finalize_kernel<<<dim3((unsigned)groups, 2, nq), 256, 0, s>>>(mvpart, mv_qstride, mv_chunks, cols, cpart,
-                                                                  cpart_qstride, cchunks, df, keys, key_qstride,
-                                                                  T, packed_b, pb_qstride);
+    finalize_kernel<<<dim3((unsigned)groups, 2, nq), 256, 0, s>>>(mvpart, mv_qstride, mv_chunks, cols, tp_out, nq,
+                                                                  (int)groups, df, keys, key_qstride, T, packed_b,
+                                                                  pb_qstride);
     return cudaGetLastError();
 }
 

@@ -104,8 +104,7 @@ struct Precomp {
     DevTables* tables = nullptr;
     uint16_t* db = nullptr;
     uint32_t* pre_a = nullptr;
-    uint32_t* pre_dp = nullptr;
-    uint32_t* pre_dm = nullptr;
+    uint8_t* pre_dt = nullptr;   // D_plus / D_minus as GEMM byte planes [l][i][g*4+a][4096]
     uint32_t* pre_df = nullptr;
     bool adopted = false;
     ~Precomp() {
@@ -125,8 +124,7 @@ static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s)
     P.tables = upload_tables(A, s);
     P.db = A.alloc<uint16_t>(R * C);
     P.pre_a = A.alloc<uint32_t>(G * kGroupStrideA);
-    P.pre_dp = A.alloc<uint32_t>(G * kGroupStrideD);
-    P.pre_dm = A.alloc<uint32_t>(G * kGroupStrideD);
+    P.pre_dt = A.alloc<uint8_t>(tp_dt_bytes(G));
     P.pre_df = A.alloc<uint32_t>(G * kGroupStrideF);
 
     DevArena tmp;
@@ -192,9 +190,11 @@ static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s)
         uint32_t* V = tmp.alloc<uint32_t>((size_t)2 * kN * kN);
         uint32_t* Tm = tmp.alloc<uint32_t>((size_t)2 * kN * kN);
         const size_t ap_gstride = (size_t)kHalf * 2 * 2 * kN;
-        const size_t wave = std::min<size_t>(G, 256);
+        const size_t wave = std::min<size_t>(G, 64);
         uint32_t* a_post = tmp.alloc<uint32_t>(wave * ap_gstride);
         uint32_t* ends = tmp.alloc<uint32_t>(wave * 2 * 2 * kN);
+        uint32_t* dp_w = tmp.alloc<uint32_t>(wave * kGroupStrideD);  // D in the reference layout, one wave
+        uint32_t* dm_w = tmp.alloc<uint32_t>(wave * kGroupStrideD);
         for (size_t w0 = 0; w0 < G; w0 += wave) {
             const size_t nw = std::min(wave, G - w0);
             for (size_t g = w0; g < w0 + nw; ++g) {
@@ -202,8 +202,8 @@ static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s)
                 IPB_CK(launch_col_ntt(V, P.tables, Tm, s));
                 IPB_CK(launch_embed_gather(Tm, a_post + (g - w0) * ap_gstride, s));
             }
-            IPB_CK(launch_collapse_a(a_post, ap_gstride, k5, P.tables, P.pre_dp + w0 * kGroupStrideD,
-                                     P.pre_dm + w0 * kGroupStrideD, ends, nw, s));
+            IPB_CK(launch_collapse_a(a_post, ap_gstride, k5, P.tables, dp_w, dm_w, ends, nw, s));
+            IPB_CK(launch_dt_transpose(dp_w, dm_w, w0, nw, G, P.pre_dt, s));
             IPB_CK(launch_collapse_final(ends, kn1, P.tables, P.pre_df + w0 * kGroupStrideF,
                                          P.pre_a + w0 * kGroupStrideA, nw, s));
         }
@@ -229,13 +229,14 @@ struct Server {
     uint32_t* keys = nullptr;
     uint32_t* rgsw32 = nullptr;
     uint32_t* mvpart = nullptr;
-    uint32_t* cpart = nullptr;
+    uint8_t* gt = nullptr;        // per-batch permuted-key planes (tensor pass N operand)
+    uint32_t* tp_out = nullptr;   // tensor pass result [l][i][q][g]
     uint32_t* packed_b = nullptr;
     uint64_t* resp = nullptr;
     uint8_t* planes = nullptr;   // query byte planes for the tensor-core mat-vec
     int* d_err = nullptr;        // device error word (pipeline wait timeouts)
-    size_t qstride = 0, mv_qstride = 0, cpart_qstride = 0, pb_qstride = 0, resp_qstride = 0;
-    int mv_chunks = 1, c_chunks = 1;
+    size_t qstride = 0, mv_qstride = 0, pb_qstride = 0, resp_qstride = 0;
+    int mv_chunks = 1, tp_pass = 32;
     bool use_tc = true;          // tcgen05 mat-vec (IPB_MATVEC=simt selects the CUDA-core kernel)
     int num_sms = 148;
     int tc_kchunk_rows = 0, tc_kchunks = 1;
@@ -283,13 +284,13 @@ static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_
     // <= 4096 rows per chunk keeps the staged query words (4 queries x 2
     // limbs x rows x 4 B) within 128 KB of shared memory.
     while (R / (size_t)S->mv_chunks > 4096) S->mv_chunks *= 2;
-    S->c_chunks = (int)std::clamp<size_t>((1184 + 2 * G - 1) / (2 * G), 2, 64);
+    S->tp_pass = (int)std::min<size_t>(max_batch, (size_t)tp_pass_queries(G));
     IPB_CK(cudaDeviceGetAttribute(&S->num_sms, cudaDevAttrMultiProcessorCount, S->device));
     if (const char* m = std::getenv("IPB_MATVEC")) S->use_tc = std::strcmp(m, "simt") != 0;
     S->tc_kchunk_rows = matvec_tc_kchunk_rows(R, C, S->num_sms);
     S->tc_kchunks = (int)(R / (size_t)S->tc_kchunk_rows);
     S->mv_qstride = (size_t)std::max(S->mv_chunks, S->tc_kchunks) * 2 * C;
-    S->cpart_qstride = G * (size_t)S->c_chunks * 2 * kN;
+
     S->pb_qstride = G * 2 * kN;
     S->resp_qstride = pp.num_cts * 4 * kN;
     DevArena& A = S->arena;
@@ -297,7 +298,8 @@ static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_
     S->keys = A.alloc<uint32_t>(max_batch * kKeyStride);
     S->rgsw32 = A.alloc<uint32_t>(max_batch * kRgswStride);
     S->mvpart = A.alloc<uint32_t>(max_batch * S->mv_qstride);
-    S->cpart = A.alloc<uint32_t>(max_batch * S->cpart_qstride);
+    S->gt = A.alloc<uint8_t>(tp_gt_bytes(S->tp_pass));
+    S->tp_out = A.alloc<uint32_t>((size_t)2 * kN * max_batch * G);
     S->packed_b = A.alloc<uint32_t>(max_batch * S->pb_qstride);
     S->resp = A.alloc<uint64_t>(max_batch * S->resp_qstride);
     S->planes = A.alloc<uint8_t>(mv_tc_planes_bytes(R, (int)max_batch));
@@ -354,13 +356,13 @@ static void run_pipeline(Server* S, size_t count) {
         S->last_mv_chunks = S->mv_chunks;
     }
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[2], st));
-    for (size_t c0 = 0; c0 < count; c0 += 8) {
-        const int n = (int)std::min<size_t>(8, count - c0);
-        IPB_CK(launch_collapse(P.pre_dp, P.pre_dm, G, S->keys + c0 * kKeyStride, kKeyStride, S->c_chunks,
-                               S->cpart + c0 * S->cpart_qstride, S->cpart_qstride, n, P.tables, st));
+    for (size_t c0 = 0; c0 < count; c0 += (size_t)S->tp_pass) {
+        const int n = (int)std::min<size_t>((size_t)S->tp_pass, count - c0);
+        IPB_CK(launch_tensor_pass(P.pre_dt, G, S->keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, S->gt,
+                                  S->tp_out, S->d_err, S->num_sms, st));
     }
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[3], st));
-    IPB_CK(launch_finalize(S->mvpart, S->mv_qstride, S->last_mv_chunks, C, S->cpart, S->cpart_qstride, S->c_chunks,
+    IPB_CK(launch_finalize(S->mvpart, S->mv_qstride, S->last_mv_chunks, C, S->tp_out,
                            P.pre_df, S->keys, kKeyStride, P.tables, S->packed_b, S->pb_qstride, G, nq, st));
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[4], st));
     IPB_CK(launch_horner(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts, S->resp,
@@ -684,8 +686,21 @@ int ipir_b200_export_precomp(const ipir_server* srv, size_t group, uint32_t* a, 
             IPB_CK(cudaSetDevice(S->device));
             const ipb::Precomp& P = *S->pre;
             if (a) IPB_CK(cudaMemcpy(a, P.pre_a + group * ipb::kGroupStrideA, ipb::kGroupStrideA * 4, cudaMemcpyDeviceToHost));
-            if (d_plus) IPB_CK(cudaMemcpy(d_plus, P.pre_dp + group * ipb::kGroupStrideD, ipb::kGroupStrideD * 4, cudaMemcpyDeviceToHost));
-            if (d_minus) IPB_CK(cudaMemcpy(d_minus, P.pre_dm + group * ipb::kGroupStrideD, ipb::kGroupStrideD * 4, cudaMemcpyDeviceToHost));
+            if (d_plus || d_minus) {
+                ipb::DevArena tmp;
+                try {
+                    uint32_t* tp = tmp.alloc<uint32_t>(ipb::kGroupStrideD);
+                    uint32_t* tm = tmp.alloc<uint32_t>(ipb::kGroupStrideD);
+                    IPB_CK(ipb::launch_dt_export(P.pre_dt, group, S->pp.n_packed, tp, tm, 0));
+                    IPB_CK(cudaDeviceSynchronize());
+                    if (d_plus) IPB_CK(cudaMemcpy(d_plus, tp, ipb::kGroupStrideD * 4, cudaMemcpyDeviceToHost));
+                    if (d_minus) IPB_CK(cudaMemcpy(d_minus, tm, ipb::kGroupStrideD * 4, cudaMemcpyDeviceToHost));
+                } catch (...) {
+                    tmp.free_all();
+                    throw;
+                }
+                tmp.free_all();
+            }
             if (d_final) IPB_CK(cudaMemcpy(d_final, P.pre_df + group * ipb::kGroupStrideF, ipb::kGroupStrideF * 4, cudaMemcpyDeviceToHost));
             return 0;
         },
