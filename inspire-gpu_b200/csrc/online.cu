@@ -287,6 +287,135 @@ __global__ void __launch_bounds__(1024, 1) horner_kernel(const uint32_t* __restr
         *reinterpret_cast<ulonglong2*>(dst + e) = make_ulonglong2(acc[e], acc[e + 1]);
 }
 
+// ------------------------------------------------------------------ horner (cluster)
+// The same chain on a cluster of four CTAs, CTA rank r = 2p + l owning
+// polynomial p (0 = a, 1 = b) in limb l.  Each CTA has two NTT groups:
+// group 0 holds the accumulator and runs the inverse NTT; both groups then
+// decompose (CRT needs the partner limb's coefficients, received through
+// distributed shared memory) and transform one gadget digit each; each
+// digit is multiplied by the RGSW rows of its polynomial (held in registers
+// for the whole chain), the contribution to the other polynomial is stored
+// into that CTA's shared memory, and group 0 sums.  Two cluster barriers per
+// step; the four SMs share the NTT work and only two NTTs sit on the
+// critical path.  Shared buffers alternate with the step parity.
+constexpr size_t kHornerClSmem =
+    2 * kN * sizeof(uint2) + (2 * 2 * kN + 2 * 2 * kN + 2 * 4 * kN) * sizeof(uint32_t);
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t map_peer(const void* local, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(r)
+                 : "r"((uint32_t)__cvta_generic_to_shared(local)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_peer4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    asm volatile("st.shared::cluster.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
+                 : "memory");
+}
+__device__ __forceinline__ void st_peer(uint32_t addr, uint32_t v) {
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
+    horner_cl_kernel(const uint32_t* __restrict__ pre_a, const uint32_t* __restrict__ packed_b, size_t pb_qstride,
+                     const uint32_t* __restrict__ rgsw32, const DevTables* __restrict__ T, size_t groups,
+                     size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint2* twf = reinterpret_cast<uint2*>(smem);
+    uint2* twi = twf + kN;
+    uint32_t* nbuf = reinterpret_cast<uint32_t*>(twi + kN);   // [2 groups][2][N]
+    uint32_t* xc = nbuf + 2 * 2 * kN;                         // [parity][own | partner limb][N]
+    uint32_t* cin = xc + 2 * 2 * kN;                          // [parity][local j0 | local j1 | peer j0 | peer j1][N]
+    const uint32_t rank = cluster_rank();
+    const int p = (int)(rank >> 1), l = (int)(rank & 1);
+    const int ct = blockIdx.x >> 2, b = blockIdx.y;
+    const int gp = threadIdx.x >> 8;
+    const uint32_t t = threadIdx.x & 255;
+    const int bar = 1 + gp;
+    const LimbTables& L = T->limb[l];
+    const uint32_t q = L.q;
+    for (int i = threadIdx.x; i < kN; i += 512) { twf[i] = L.fwd[i]; twi[i] = L.inv[i]; }
+    const uint32_t rank_limb = (uint32_t)((p << 1) | (1 - l));   // same poly, other limb
+    const uint32_t rank_poly = (uint32_t)(((1 - p) << 1) | l);   // other poly, same limb
+    const size_t start = (size_t)ct * d_act;
+    const size_t len = (start + d_act <= groups) ? d_act : groups - start;
+    const uint32_t* pbq = packed_b + (size_t)b * pb_qstride;
+    auto src_of = [&](size_t i) -> const uint32_t* {
+        return p ? pbq + (i * 2 + l) * kN : pre_a + (i * 2 + l) * kN;
+    };
+    // RGSW rows of this poly for digit gp: to own output (p' = p) and to the other (p' = 1 - p)
+    const uint32_t* rg = rgsw32 + (size_t)b * (4 * kDeff * 2 * kN);
+    uint32_t r_self[8], r_oth[8];
+    ld8(rg + (size_t)(((2 * p + p) * kDeff + gp) * 2 + l) * kN + 8 * t, r_self);
+    ld8(rg + (size_t)(((2 * p + (1 - p)) * kDeff + gp) * 2 + l) * kN + 8 * t, r_oth);
+    uint32_t acc[8];
+    if (gp == 0) ld8(src_of(start + len - 1) + 8 * t, acc);
+    cluster_sync_all();  // every CTA of the cluster is running before any remote access
+    int par = 0;
+    for (long i = (long)len - 2; i >= 0; --i, par ^= 1) {
+        uint32_t* xown = xc + (par * 2 + 0) * kN;
+        uint32_t* xpart = xc + (par * 2 + 1) * kN;
+        uint32_t* cp = cin + (size_t)par * 4 * kN;
+        uint32_t pk[8];
+        if (gp == 0) {
+            ld8(src_of(start + (size_t)i) + 8 * t, pk);
+            ntt_inv(acc, nbuf, twi, q, L.inv_n, L.inv_n_p, t, bar);
+            const uint32_t peer = map_peer(xpart, rank_limb);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                xown[t + 256 * e] = acc[e];
+                st_peer(peer + 4 * (t + 256 * e), acc[e]);
+            }
+        }
+        cluster_sync_all();
+        uint32_t d[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const uint32_t own = xown[t + 256 * e], oth = xpart[t + 256 * e];
+            int64_t s1, s2;
+            decomp2(l ? oth : own, l ? own : oth, *T, s1, s2);
+            d[e] = signed_res(gp ? s2 : s1, q);
+        }
+        ntt_fwd(d, nbuf + gp * 2 * kN, twf, q, t, bar);
+        uint32_t es[8], eo[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            es[e] = mod_u64((uint64_t)d[e] * r_self[e], L.cr, q);
+            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], L.cr, q);
+        }
+        st8(cp + (size_t)gp * kN + 8 * t, es);
+        const uint32_t peer = map_peer(cp + (size_t)(2 + gp) * kN + 8 * t, rank_poly);
+        st_peer4(peer, eo[0], eo[1], eo[2], eo[3]);
+        st_peer4(peer + 16, eo[4], eo[5], eo[6], eo[7]);
+        cluster_sync_all();
+        if (gp == 0) {
+            uint32_t v0[8], v1[8], w0[8], w1[8];
+            ld8(cp + 8 * t, v0);
+            ld8(cp + kN + 8 * t, v1);
+            ld8(cp + 2 * kN + 8 * t, w0);
+            ld8(cp + 3 * kN + 8 * t, w1);
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                acc[e] = add_mod(add_mod(add_mod(v0[e], v1[e], q), add_mod(w0[e], w1[e], q), q), pk[e], q);
+        }
+    }
+    if (gp == 0) {
+        uint64_t* dst = resp + (size_t)b * resp_qstride + ((size_t)ct * 4 + p * 2 + l) * kN + 8 * t;
+#pragma unroll
+        for (int e = 0; e < 8; e += 2)
+            *reinterpret_cast<ulonglong2*>(dst + e) = make_ulonglong2(acc[e], acc[e + 1]);
+    }
+    cluster_sync_all();  // no CTA leaves while a peer may still write into its shared memory
+}
+
 // ------------------------------------------------------------------ primitives
 __global__ void __launch_bounds__(1024) ntt_batch_kernel(uint32_t* polys, size_t n, int limb_run, bool inverse,
                                                          const DevTables* __restrict__ T) {
@@ -385,6 +514,19 @@ cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_
     if (e) return e;
     horner_kernel<<<dim3((unsigned)num_cts, nq), 1024, kHornerSmem, s>>>(pre_a, packed_b, pb_qstride, rgsw32, T,
                                                                           groups, d_act, resp, resp_qstride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
+                                  const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
+                                  size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(horner_cl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kHornerClSmem);
+    if (e) return e;
+    horner_cl_kernel<<<dim3((unsigned)(4 * num_cts), nq), 512, kHornerClSmem, s>>>(pre_a, packed_b, pb_qstride,
+                                                                                   rgsw32, T, groups, d_act, resp,
+                                                                                   resp_qstride);
     return cudaGetLastError();
 }
 

@@ -238,6 +238,7 @@ struct Server {
     size_t qstride = 0, mv_qstride = 0, pb_qstride = 0, resp_qstride = 0;
     int mv_chunks = 1, tp_pass = 32;
     bool use_tc = true;          // tcgen05 mat-vec (IPB_MATVEC=simt selects the CUDA-core kernel)
+    bool horner_cluster = true;  // 4-CTA cluster per chain (IPB_HORNER=cta selects one CTA per chain)
     int num_sms = 148;
     int tc_kchunk_rows = 0, tc_kchunks = 1;
     int last_mv_chunks = 1;
@@ -287,6 +288,7 @@ static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_
     S->tp_pass = (int)std::min<size_t>(max_batch, (size_t)tp_pass_queries(G));
     IPB_CK(cudaDeviceGetAttribute(&S->num_sms, cudaDevAttrMultiProcessorCount, S->device));
     if (const char* m = std::getenv("IPB_MATVEC")) S->use_tc = std::strcmp(m, "simt") != 0;
+    if (const char* h = std::getenv("IPB_HORNER")) S->horner_cluster = std::strcmp(h, "cta") != 0;
     S->tc_kchunk_rows = matvec_tc_kchunk_rows(R, C, S->num_sms);
     S->tc_kchunks = (int)(R / (size_t)S->tc_kchunk_rows);
     S->mv_qstride = (size_t)std::max(S->mv_chunks, S->tc_kchunks) * 2 * C;
@@ -365,8 +367,12 @@ static void run_pipeline(Server* S, size_t count) {
     IPB_CK(launch_finalize(S->mvpart, S->mv_qstride, S->last_mv_chunks, C, S->tp_out,
                            P.pre_df, S->keys, kKeyStride, P.tables, S->packed_b, S->pb_qstride, G, nq, st));
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[4], st));
-    IPB_CK(launch_horner(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts, S->resp,
-                         S->resp_qstride, nq, st));
+    if (S->horner_cluster)
+        IPB_CK(launch_horner_cluster(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts,
+                                     S->resp, S->resp_qstride, nq, st));
+    else
+        IPB_CK(launch_horner(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts, S->resp,
+                             S->resp_qstride, nq, st));
     if (S->timing) IPB_CK(cudaEventRecord(S->ev[5], st));
 }
 

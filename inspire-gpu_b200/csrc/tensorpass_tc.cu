@@ -153,9 +153,10 @@ struct TpParams {
     int nq;                // queries in this pass
     int npad;              // N = roundup16(4 nq)
     int G;                 // groups
-    int mti;               // M tiles (128 rows) per item
+    int mti;               // M tiles (128 rows) per item (4G >= 128)
     int n_mg;              // M-tile groups per (l, i)
-    int rows_box;          // rows per A box (min(128, 4G))
+    int spi;               // slots per item (4G < 128: several slots share one 128-row A tile)
+    int rows_box;          // rows per A box
     int stages;
     int acc_stages;
     uint32_t tmem_cols;
@@ -171,8 +172,12 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int S = P.stages;
     const uint32_t a_tile = 128 * 128;
-    const uint32_t b_bytes = (uint32_t)P.npad * 128;
-    const uint32_t stage_bytes = (uint32_t)P.mti * a_tile + b_bytes;
+    // With packed slots the MMA for slot sl reads rows sl*4G .. sl*4G + 127,
+    // up to 224 rows: the A region then spans two tiles so every read stays
+    // inside this stage.
+    const uint32_t a_region = (uint32_t)(P.spi > 1 ? 2 : P.mti) * a_tile;
+    const uint32_t b_bytes = (uint32_t)(P.npad * P.spi) * 128;
+    const uint32_t stage_bytes = a_region + b_bytes;
     const uint32_t tx_bytes = (uint32_t)P.mti * P.rows_box * 128 + b_bytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
     uint64_t* full = bars;
@@ -198,17 +203,18 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int n_items = 2 * kN * P.n_mg;
+    const int n_items = (2 * kN / P.spi) * P.n_mg;
     constexpr int ktiles = kUPad / 128;
-    const int acc_cols = P.mti * P.npad;
+    const int acc_cols = P.mti * P.spi * P.npad;
+    const int slot_rows = 4 * P.G;  // A rows of one slot
 
     if (warp == 0) {
         if (lane == 0) {
             int s = 0;
             uint32_t ph = 0;
             for (int item = blockIdx.x; item < n_items && !abort_flag; item += gridDim.x) {
-                const int li = item / P.n_mg, mg = item % P.n_mg;
-                const int rowa = li * 4 * P.G + mg * P.mti * 128;
+                const int li = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
+                const int rowa = li * slot_rows + mg * P.mti * 128;
                 const int rowb = li * P.npad;
                 for (int kt = 0; kt < ktiles; ++kt) {
                     if (!mbar_wait(&empty[s], ph ^ 1, P.err, 11)) { abort_flag = 1; break; }
@@ -216,7 +222,7 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
                     mbar_expect_tx(&full[s], tx_bytes);
                     for (int mt = 0; mt < P.mti; ++mt)
                         tma_load_2d(st + mt * a_tile, &map_a, &full[s], kt * 128, rowa + mt * 128);
-                    tma_load_2d(st + P.mti * a_tile, &map_b, &full[s], kt * 128, rowb);
+                    tma_load_2d(st + a_region, &map_b, &full[s], kt * 128, rowb);
                     if (++s == S) { s = 0; ph ^= 1; }
                 }
             }
@@ -238,14 +244,24 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
                     if (!mbar_wait(&full[s], ph, P.err, 14)) { abort_flag = 1; break; }
                     tc_fence_after();
                     const uint8_t* st = smem + (size_t)s * stage_bytes;
-                    const uint8_t* bt = st + P.mti * a_tile;
+                    const uint8_t* bt = st + a_region;
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
-                        const uint64_t b = smem_desc(bt + kk * 32, 16, 1024);
                         const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
-                        for (int mt = 0; mt < P.mti; ++mt)
-                            mma_i8(d0 + (uint32_t)(mt * P.npad), smem_desc(st + mt * a_tile + kk * 32, 16, 1024), b,
-                                   idesc, acc);
+                        if (P.spi == 1) {
+                            const uint64_t b = smem_desc(bt + kk * 32, 16, 1024);
+                            for (int mt = 0; mt < P.mti; ++mt)
+                                mma_i8(d0 + (uint32_t)(mt * P.npad), smem_desc(st + mt * a_tile + kk * 32, 16, 1024),
+                                       b, idesc, acc);
+                        } else {
+                            // slot sl's rows start at row sl*4G of the shared tile (a multiple of 8
+                            // rows, so the descriptor stays on a swizzle-atom boundary); rows past
+                            // the slot produce accumulator lanes the epilogue ignores.
+                            for (int sl = 0; sl < P.spi; ++sl)
+                                mma_i8(d0 + (uint32_t)(sl * P.npad),
+                                       smem_desc(st + sl * slot_rows * 128 + kk * 32, 16, 1024),
+                                       smem_desc(bt + sl * P.npad * 128 + kk * 32, 16, 1024), idesc, acc);
+                        }
                     }
                     mma_commit(&empty[s]);
                     if (++s == S) { s = 0; ph ^= 1; }
@@ -262,13 +278,15 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
         for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
             if (!mbar_wait(&tfull[as], aph, P.err, 15)) { abort_flag = 1; break; }
             tc_fence_after();
-            const int li = item / P.n_mg, mg = item % P.n_mg;
-            const int l = li / kN;
+            const int li0 = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
+            const int l = li0 / kN;
             const uint32_t* c = P.c[l];
-            for (int mt = 0; mt < P.mti; ++mt) {
-                const int grow = (mg * P.mti + mt) * 128 + wq * 32 + lane;  // g*4 + a
+            for (int mt = 0; mt < P.mti * P.spi; ++mt) {
+                // spi == 1: tile mt of the slot's 4G rows; spi > 1: slot li0 + mt, rows 0..4G-1
+                const int li = li0 + (P.spi > 1 ? mt : 0);
+                const int grow = (P.spi > 1 ? 0 : (mg * P.mti + mt) * 128) + wq * 32 + lane;  // g*4 + a
                 const int g = grow >> 2, a = grow & 3;
-                const bool valid = grow < 4 * P.G;
+                const bool valid = grow < slot_rows;
                 for (int q = 0; q < P.nq; ++q) {
                     uint32_t v[4];
                     tmem_ld4(tmem_base + lane_base + (uint32_t)(as * acc_cols + mt * P.npad + 4 * q), v);
@@ -376,10 +394,18 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     const int nmt = (int)std::max<size_t>(1, (4 * G + 127) / 128);
     P.mti = std::min(nmt, 4);
     P.n_mg = nmt / P.mti;
-    P.rows_box = (int)std::min<size_t>(128, 4 * G);
-    if (P.mti * npad > 512) return cudaErrorInvalidValue;
-    P.acc_stages = (2 * P.mti * npad <= 512) ? 2 : 1;
-    uint32_t need = (uint32_t)(P.acc_stages * P.mti * npad), tc = 32;
+    // Small G: pack spi slots (each 4G rows) into one 128-row A tile.  G even
+    // keeps every slot start on an 8-row (1024-byte) swizzle atom; spi a power
+    // of two divides kN, so a packed item never straddles the two limbs.
+    P.spi = 1;
+    if (4 * G < 128 && G % 2 == 0) {
+        while (2 * P.spi * 4 * (int)G <= 128) P.spi *= 2;
+        while (P.spi > 1 && (P.spi * npad > 256 || 2 * P.spi * npad > 512)) P.spi /= 2;
+    }
+    P.rows_box = (int)std::min<size_t>(128, 4 * G * (size_t)P.spi);
+    if (P.mti * P.spi * npad > 512) return cudaErrorInvalidValue;
+    P.acc_stages = (2 * P.mti * P.spi * npad <= 512) ? 2 : 1;
+    uint32_t need = (uint32_t)(P.acc_stages * P.mti * P.spi * npad), tc = 32;
     while (tc < need) tc <<= 1;
     P.tmem_cols = tc;
     P.err = err;
@@ -389,16 +415,17 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
         P.cr[l] = ~0ULL / qs[l];
         P.q[l] = qs[l];
     }
-    const size_t stage_bytes = (size_t)P.mti * 128 * 128 + (size_t)npad * 128;
+    const size_t a_region = (size_t)(P.spi > 1 ? 2 : P.mti) * 128 * 128;
+    const size_t stage_bytes = a_region + (size_t)npad * P.spi * 128;
     P.stages = (int)std::min<size_t>(8, (200 * 1024) / stage_bytes);
     if (P.stages < 2) return cudaErrorInvalidValue;
     CUtensorMap ma, mb;
     if (!make_map(&ma, Dt, (uint64_t)2 * kN * 4 * G, (uint32_t)P.rows_box)) return cudaErrorInvalidValue;
-    if (!make_map(&mb, Gt, (uint64_t)2 * kN * npad, (uint32_t)npad)) return cudaErrorInvalidValue;
+    if (!make_map(&mb, Gt, (uint64_t)2 * kN * npad, (uint32_t)(npad * P.spi))) return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
     e = cudaFuncSetAttribute(tp_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e) return e;
-    const int items = 2 * kN * P.n_mg;
+    const int items = (2 * kN / P.spi) * P.n_mg;
     tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), 256, smem, s>>>(ma, mb, P);
     return cudaGetLastError();
 }
