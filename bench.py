@@ -1,20 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 InsPIRe server on the 16 GB configuration.
+"""Benchmark of the B200 InsPIRe server.
 
-Workload (one step = one answer batch over the whole database):
+Default workload (one step = one answer batch over the whole database):
   setup(N_entries = 2^29, w = 30) -> 32768 x 262144 u16 DB (17.18 GB, 16 GiB),
   128 packing groups, 8.59 GB of precomputed tensors, one Horner chain of
-  128 ciphertexts per query.  w = 30 stands in for the configuration's w = 32,
-  which the reference's setup() rejects; it gives the same DB byte size.
-  DB values: synthetic, splitmix64(k) mod 65535.  Queries: synthetic residues
-  uniform in [0, q_l) per limb (the server's work does not depend on them).
+  128 ciphertexts per query.  w = 30 stands in for w = 32, which the
+  reference's setup() rejects; it gives the same DB byte size.  DB values:
+  synthetic, splitmix64(k) mod 65535.  Queries: synthetic residues uniform in
+  [0, q_l) per limb (the server's work does not depend on their values).
 
 Reported line (rank 0): ``value`` = served q/s at batch 32, device-resident
 inputs, max over ranks of the CUDA-event time of K steps; ``e2e`` = the same
 through ipir_answer_batch with pinned host queries/responses (H2D + kernels +
 D2H inside the timed region); plus the plain batch-1 q/s, p50/p99 latency of
-the plain path, DB-pass GB/s, the roofline of the mat-vec kernel and the
-CPU baseline (the oracle port on the host cores).
+the plain path, a batch sweep (B = 1, 8, 32, 64) with per-stage times, the
+DB-pass GB/s, the roofline of the mat-vec kernel, the kernel schedule the
+autotuner picked, and the CPU baseline (the oracle port on the host cores).
+
+``--mode serve`` drives the continuous-batching serving loop with open-loop
+Poisson arrivals over resident databases and reports p50/p95/p99 latency and
+sustained q/s per offered rate, every response checked bit-exact against
+the plain single answer of the same query.  ``--serve-config mixed``: a
+1 GB database (setup(2^25, 30)) and a 4 GB one (setup(2^22, 960)), 70/30
+split, 50/100/200/400 q/s.  ``--serve-config 16gb``: the default workload at
+1, 3 and 5 times the plain per-query rate.
 
 ``--impl reference`` times the CPU restatement of the reference's server
 path (the reference has no CPU server of its own) on a bounded sample of
@@ -23,6 +32,7 @@ the same workload.  Multi-GPU: every rank serves an independent replica.
 import argparse
 import json
 import os
+import random
 import statistics
 import subprocess
 import sys
@@ -37,6 +47,7 @@ sys.path.insert(0, os.path.join(REPO, "inspire-gpu_b200"))
 N = 2048
 Q = (94519297, 95293441)
 NSTEPS = 1023
+SWEEP = (1, 8, 32, 64)
 
 
 def parse():
@@ -45,15 +56,29 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="batch", choices=["batch", "serve"])
     ap.add_argument("--n-entries", type=int, default=1 << 29)
     ap.add_argument("--entry-bytes", type=int, default=30)
     ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-config", default="mixed", choices=["mixed", "16gb"])
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-rates", default="")
     return ap.parse_args()
 
 
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def describe(params):
+    R, C, G = params["db_rows"], params["db_cols"], params["n_packed"]
+    ne, w = params["n_entries"], params["entry_bytes"]
+    ne_s = f"2^{ne.bit_length() - 1}" if ne & (ne - 1) == 0 else str(ne)
+    return (f"setup({ne_s}, w={w}): {R} x {C} u16 DB ({R * C * 2 / 1e9:.2f} GB), {G} groups, "
+            f"{G * 2 * (2 * NSTEPS * 2 * N * 4) / 1e9:.2f} GB tensors, {params['num_cts']} ct/query")
 
 
 def synth_queries(params, count, seed, out):
@@ -72,54 +97,64 @@ def synth_queries(params, count, seed, out):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled through NVML every 5 ms
+    during the timed region (read-only queries)."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index):
+        self.cuda_index = cuda_index
+        self.sm, self.reasons, self.max_mhz = [], set(), None
+        self.err = None
+        self._stop = threading.Event()
+        self.t = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            masks = [(name, getattr(nv, attr)) for name, attr in self.REASONS]
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        self.sm.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = get_reasons(h)
+                        for name, m in masks:
+                            if r & m:
+                                self.reasons.add(name)
+                    except Exception as e:  # keep sampling; report the error
+                        self.err = str(e)
+                    self._stop.wait(0.005)
+
+            self.t = threading.Thread(target=loop, daemon=True)
+            self.t.start()
+        except Exception as e:
+            self.err = f"nvml unavailable: {e}"
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        self._stop.set()
+        if self.t is not None:
+            self.t.join(timeout=5)
+        d = {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.max_mhz,
+             "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml, 5 ms"}
+        if self.err:
+            d["error"] = self.err
+        return d
 
 
 def measured_peaks():
@@ -185,6 +220,7 @@ def cpu_sample(params, seconds_hint=15.0):
                        f"per-query {per_query:.2f} s = mat-vec {t_mv:.2f} + tensor {t_pack:.2f} + Horner {t_h:.2f}")}
 
 
+
 # ------------------------------------------------------------------ reference arm
 def run_reference(args):
     rank, _, world = dist_env()
@@ -199,11 +235,12 @@ def run_reference(args):
         vals.append(cpu_sample(params)["value"])
     last = cpu_sample(params)
     v = statistics.median(vals)
-    line = {"impl": "reference", "metric": "q/s at 16 GB DB (CPU restatement of the reference server path)",
+    line = {"impl": "reference",
+            "metric": "q/s at 16 GB DB (plain batch-1 vs served batch-32), p50/p99 latency, DB-pass GB/s",
             "value": v, "unit": "q/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64 modular",
             "data": "synthetic",
-            "config": {"workload": "setup(2^29, w=30): 32768 x 262144 u16 DB (17.18 GB), 128 groups, batch 1",
+            "config": {"workload": describe(params) + "; CPU restatement, one query at a time",
                        "model": "InsPIRe PIR server", "global_batch": 1, "seq_len": 0, "parallelism": "replicas"},
             "cpu_baseline": {"value": v, "unit": "q/s", "cores": last["cores"], "kind": last["kind"],
                              "sample": last["sample"]},
@@ -223,14 +260,21 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local_rank))
     import inspire_b200 as ib
     B = args.batch
+    sweep = [] if args.no_sweep else [b for b in SWEEP if b != B]
+    max_b = max([B] + sweep)
     params = ib.setup(args.n_entries, args.entry_bytes)
-    R, Ccols, G, ncts = params["db_rows"], params["db_cols"], params["n_packed"], params["num_cts"]
+    R, Ccols, G = params["db_rows"], params["db_cols"], params["n_packed"]
     db = ib.fill_db(R * Ccols, 0)
     seed = bytes(range(64))
     t0 = time.perf_counter()
-    srv = ib.Server(args.n_entries, args.entry_bytes, db, max_batch=max(B, 1), crs_seed=seed)
+    srv = ib.Server(args.n_entries, args.entry_bytes, db, max_batch=max_b, crs_seed=seed)
     t_pre = time.perf_counter() - t0
     del db
+    t_tune = 0.0
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        srv.autotune()
+        t_tune = time.perf_counter() - t0
     # A dedicated stream: the handle of torch's default stream is 0, which the
     # C ABI reads as "the server's own stream".
     stream = torch.cuda.Stream()
@@ -238,13 +282,13 @@ def run_ours(args):
     srv.set_stream(stream.cuda_stream)
     qn = ib.query_u64s(params)
     rn = ib.response_u64s(params)
-    qbuf_t = torch.empty((B, qn), dtype=torch.int64, pin_memory=True)
+    qbuf_t = torch.empty((max_b, qn), dtype=torch.int64, pin_memory=True)
     qbuf = qbuf_t.numpy().view(np.uint64)
-    synth_queries(params, B, 1000 + rank, qbuf)
-    obuf_t = torch.empty((B, rn), dtype=torch.int64, pin_memory=True)
+    synth_queries(params, max_b, 1000 + rank, qbuf)
+    obuf_t = torch.empty((max_b, rn), dtype=torch.int64, pin_memory=True)
     obuf = obuf_t.numpy().view(np.uint64)
-    views = (ib.IpirQueryView * B)()
-    for i in range(B):
+    views = (ib.IpirQueryView * max_b)()
+    for i in range(max_b):
         views[i] = ib.query_view_from_flat(params, qbuf[i])
 
     def barrier():
@@ -258,45 +302,53 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    def device_time(count, steps):
+    def device_time(count, steps, sampler=None):
         srv.stage_views(views, count)
         for _ in range(args.warmup):
             srv.run(count)
         barrier()
         torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        n0 = srv.launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
             srv.run(count)
         e1.record(stream)
         torch.cuda.synchronize()
+        launches = srv.launch_count() - n0
+        clocks = sampler.stop() if sampler else None
         barrier()
-        return max_over_ranks(e0.elapsed_time(e1) / steps)
+        return max_over_ranks(e0.elapsed_time(e1) / steps), launches, clocks
 
-    # stage timers (CUDA events on the launching stream) for the roofline
-    srv.enable_stage_timing(True)
-    srv.stage_views(views, 1)
-    st1 = []
-    for _ in range(max(3, args.warmup)):
-        srv.run(1)
-        srv.fetch(1, obuf[:1])
-        st1.append(srv.stage_times())
-    stB = []
-    srv.stage_views(views, B)
-    for _ in range(2):
-        srv.run(B)
-        srv.fetch(B, obuf)
-        stB.append(srv.stage_times())
-    srv.enable_stage_timing(False)
+    def stage_ms(count, reps):
+        srv.enable_stage_timing(True)
+        srv.stage_views(views, count)
+        st = []
+        for _ in range(reps):
+            srv.run(count)
+            srv.fetch(count, obuf[:count])
+            st.append(srv.stage_times())
+        srv.enable_stage_timing(False)
+        return {k: statistics.median(s[k] for s in st) for k in st[0]}
 
-    # plain batch-1 device time
-    ms1 = device_time(1, args.steps)
-    # headline: served batch B, timed region sampled for clocks
-    sampler = ClockSampler(local_rank)
-    sampler.start()
-    msB = device_time(B, args.steps)
-    clocks = sampler.stop()
+    st1 = stage_ms(1, max(3, args.warmup))
+    stB = stage_ms(B, 3)
+    ms1, _, _ = device_time(1, args.steps)
+    msB, launches, clocks = device_time(B, args.steps, ClockSampler(local_rank))
     value = world * B * 1000.0 / msB
+    sweep_out = {}
+    for b in sorted(set(sweep + [1, B])):
+        if b == B:
+            ms = msB
+        elif b == 1:
+            ms = ms1
+        else:
+            ms, _, _ = device_time(b, max(3, args.steps // 2))
+        sweep_out[str(b)] = {"ms_per_batch": ms, "q_per_s": b * 1000.0 / ms,
+                             "stage_ms": st1 if b == 1 else (stB if b == B else stage_ms(b, 2)),
+                             "schedule": srv.schedule(b)}
 
     # e2e through the C ABI with pinned host buffers (H2D + kernels + D2H)
     for _ in range(args.warmup):
@@ -319,36 +371,38 @@ def run_ours(args):
     p50 = lat[len(lat) // 2]
     p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
 
-    mv1 = statistics.median(s["matvec"] for s in st1)
+    mv1 = st1["matvec"]
     db_bytes = R * Ccols * 2
     alg_bytes = db_bytes + 2 * R * 8          # DB + one query's b vector per launch
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (mv1 * 1e-3) / 1e9
-    launches_per_step = 1 + (B + 3) // 4 + (B + 7) // 8 + 1 + 1
     tensor_bytes = G * 2 * (2 * NSTEPS * 2 * N * 4)
+    sched1 = srv.schedule(1)
 
     line = {
-        "metric": "q/s at 16 GB DB (served batch-32; plain batch-1, p50/p99 latency, DB-pass GB/s alongside)",
+        "metric": "q/s at 16 GB DB (plain batch-1 vs served batch-32), p50/p99 latency, DB-pass GB/s",
         "value": value, "unit": "q/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": msB, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32/u64 modular (exact)", "data": "synthetic",
-        "config": {"workload": "setup(2^29, w=30): 32768 x 262144 u16 DB (17.18 GB), 128 groups, "
-                               f"8.59 GB tensors, 1 ct/query; batch {B}",
+        "config": {"workload": describe(params) + f"; batch {B}",
                    "model": "InsPIRe PIR server", "global_batch": B * world, "seq_len": 0,
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (17 GB DB per step)"},
+                   "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 ({db_bytes / 1e9:.1f} GB DB read per step)"},
         "plain_b1": {"q_per_s": 1000.0 / ms1, "ms": ms1, "p50_ms_e2e": p50, "p99_ms_e2e": p99},
         "served": {"batch": B, "ms_per_batch": msB, "q_per_s": value / world},
+        "batch_sweep": sweep_out,
         "db_pass_gbs": db_bytes / (mv1 * 1e-3) / 1e9,
-        "stage_ms_b1": st1[-1], "stage_ms_batch": stB[-1],
-        "preprocess_s": t_pre,
-        "roofline": {"kernel": ("mv_tc_kernel (tcgen05 int8 DB pass, batch 1)" if os.environ.get("IPB_MATVEC", "tc") != "simt" else "matvec_kernel<1,8> (DB pass, batch 1)"), "bound": "hbm",
+        "stage_ms_b1": st1, "stage_ms_batch": stB,
+        "preprocess_s": t_pre, "autotune_s": t_tune,
+        "roofline": {"kernel": ("mv_tc_kernel (tcgen05 int8 DB pass, batch 1)" if sched1["matvec_tc"]
+                                else "matvec_kernel<1,8> (CUDA-core DB pass, batch 1)"), "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": None,
                      "alg_bytes_per_launch": alg_bytes},
-        "tensor_pass_gbs_b1": tensor_bytes / (statistics.median(s["collapse"] for s in st1) * 1e-3) / 1e9,
+        "tensor_pass_gbs_b1": tensor_bytes / (st1["collapse"] * 1e-3) / 1e9,
         "e2e": {"value": e2e_qps, "unit": "q/s", "h2d_bytes_per_step": B * qn * 8,
                 "d2h_bytes_per_step": B * rn * 8},
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": launches,
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -360,10 +414,156 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ serving loop
+def run_serve(args):
+    """Open-loop Poisson load on the continuous-batching serving loop."""
+    import torch
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    import inspire_b200 as ib
+    if args.serve_config == "mixed":
+        dbs = [(1 << 25, 30, 0, bytes([7] * 64)), (1 << 22, 960, 1, bytes([9] * 64))]
+        split = [0.7, 0.3]
+        rates = [50.0, 100.0, 200.0, 400.0]
+    else:
+        dbs = [(args.n_entries, args.entry_bytes, 0, bytes(range(64)))]
+        split = [1.0]
+        rates = None   # multiples of the plain rate, below
+    servers, pools, alone, plain = [], [], [], []
+    pool_n = 32
+    for k, (ne, w, dseed, cseed) in enumerate(dbs):
+        p = ib.setup(ne, w)
+        db = ib.fill_db(p["db_rows"] * p["db_cols"], dseed)
+        srv = ib.Server(ne, w, db, max_batch=1, crs_seed=cseed)
+        del db
+        servers.append(srv)
+        qs = np.zeros((pool_n, ib.query_u64s(p)), np.uint64)
+        synth_queries(p, pool_n, 100 + k, qs)
+        pools.append(qs)
+        alone.append(np.stack([srv.answer(q) for q in qs]))
+        lat = []
+        for i in range(30):
+            t0 = time.perf_counter()
+            srv.answer(qs[i % pool_n])
+            lat.append((time.perf_counter() - t0) * 1e3)
+        lat.sort()
+        plain.append({"workload": describe(p), "p50_ms": lat[len(lat) // 2], "p99_ms": lat[-1],
+                      "q_per_s": 1e3 / statistics.mean(lat)})
+    if rates is None:
+        r1 = plain[0]["q_per_s"]
+        rates = [r1, 3 * r1, 5 * r1]
+    if args.serve_rates:
+        rates = [float(x) for x in args.serve_rates.split(",")]
+    t0 = time.perf_counter()
+    loop = ib.ServeLoop(servers, max_batch=64, lanes_per_db=2, queue_slots=512)
+    t_create = time.perf_counter() - t0
+    views = [[ib.query_view_from_flat(servers[k].params, pools[k][i]) for i in range(pool_n)]
+             for k in range(len(dbs))]
+    results = []
+    rng = random.Random(6)
+    for rate in rates:
+        s0 = loop.stats()
+        tickets = []          # (ticket, db, pool index)
+        lock = threading.Lock()
+        done = {"lat": [], "bad": 0, "n": 0, "failed": 0}
+        finished = threading.Event()
+
+        def collector():
+            outs = [np.zeros(ib.response_u64s(s.params), np.uint64) for s in servers]
+            i = 0
+            while True:
+                with lock:
+                    item = tickets[i] if i < len(tickets) else None
+                if item is None:
+                    if finished.is_set():
+                        with lock:
+                            if i >= len(tickets):
+                                return
+                        continue
+                    time.sleep(0.0002)
+                    continue
+                t, k, qi = item
+                lat = C_wait(loop, t, outs[k])
+                if lat is None:
+                    done["failed"] += 1
+                else:
+                    done["lat"].append(lat)
+                    if not np.array_equal(outs[k], alone[k][qi]):
+                        done["bad"] += 1
+                done["n"] += 1
+                i += 1
+
+        th = threading.Thread(target=collector)
+        th.start()
+        t_start = time.perf_counter()
+        t_next = t_start
+        full = 0
+        while True:
+            t_next += rng.expovariate(rate)
+            if t_next - t_start > args.serve_seconds:
+                break
+            while True:
+                d = t_next - time.perf_counter()
+                if d <= 0:
+                    break
+                time.sleep(min(d, 0.001) if d > 0.0015 else 0)
+            k = 0 if rng.random() < split[0] else 1 if len(dbs) > 1 else 0
+            qi = rng.randrange(pool_n)
+            while True:
+                rc, t = loop.submit_view(k, views[k][qi])
+                if rc != ib.SERVE_FULL:
+                    break
+                full += 1
+                time.sleep(0.0005)
+            assert rc == 0, (rc, ib.last_error())
+            with lock:
+                tickets.append((t, k, qi))
+        finished.set()
+        th.join()
+        wall = time.perf_counter() - t_start
+        s1 = loop.stats()
+        lat = sorted(done["lat"])
+
+        def pct(p):
+            return lat[min(len(lat) - 1, int(round(p * (len(lat) - 1))))] if lat else None
+
+        nb = s1["batches"] - s0["batches"]
+        results.append({"offered_q_per_s": rate, "sustained_q_per_s": done["n"] / wall,
+                        "requests": done["n"], "p50_ms": pct(0.50), "p95_ms": pct(0.95), "p99_ms": pct(0.99),
+                        "max_ms": lat[-1] if lat else None, "mismatches": done["bad"], "failed": done["failed"],
+                        "batches": nb, "mean_batch": (s1["batched_queries"] - s0["batched_queries"]) / max(1, nb),
+                        "queue_full_retries": full})
+    infos = [loop.db_info(k) for k in range(len(dbs))]
+    loop.close()
+    for s in servers:
+        s.close()
+    line = {"metric": "serving loop: p50/p95/p99 latency and sustained q/s under open-loop Poisson arrivals",
+            "mode": "serve", "config": {"workload": args.serve_config, "databases": [p["workload"] for p in plain],
+                                        "split": split, "seconds_per_rate": args.serve_seconds,
+                                        "max_batch": 64, "lanes_per_db": 2},
+            "n_gpus": 1, "unit": "ms", "data": "synthetic queries (pool of 32 per database)",
+            "plain": plain, "rates": results, "create_s": t_create,
+            "lanes": [{"lanes": i["lanes"], "max_batch": i["max_batch"]} for i in infos],
+            "bit_exact_vs_alone": all(r["mismatches"] == 0 and r["failed"] == 0 for r in results)}
+    print(json.dumps(line), flush=True)
+
+
+def C_wait(loop, ticket, out):
+    import inspire_b200 as ib
+    try:
+        return loop.wait(ticket, out=out, timeout=120.0)
+    except ib.InspireError:
+        return None
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.mode == "serve":
+        rank, _, _ = dist_env()
+        if rank == 0:
+            run_serve(args)
     else:
         run_ours(args)
 

@@ -9,7 +9,9 @@
  *
  * Part 2 holds additive entry points (prefix ipir_b200_) that the reference
  * does not have: explicit streams, a device-resident staged pipeline, stage
- * timers, precomp export, and the GPU primitives for parity checks.
+ * timers, precomp export, schedule autotuning, and the GPU primitives for
+ * parity checks.  Part 3 (prefix ipir_serve_) is the continuous-batching
+ * serving loop.
  *
  * Values are residues mod the two 27-bit primes q0 = 94519297 and
  * q1 = 95293441 carried in u64 (u32 for GPU-side primitives).  One server
@@ -174,6 +176,93 @@ int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t cols, const
 /* Synthetic database for benchmarks and tests: out[k] = splitmix64(seed ^ k)
  * mod 65535 for k < count, filled on all host threads. */
 int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed);
+
+/* Kernel schedule for one batch size: mat-vec on the tensor cores
+ * (matvec_tc = 1) or the CUDA cores (0); queries per tensor-pass GEMM
+ * (tp_pass); Horner on a 4-CTA cluster per chain (horner_cluster = 1) or one
+ * CTA per chain (0).  Every schedule gives the same responses. */
+typedef struct {
+    int matvec_tc;
+    int tp_pass;
+    int horner_cluster;
+} ipir_serve_schedule;
+
+/* Time the candidate schedules on this handle for batch sizes 1, 2, 4, ...
+ * up to max_batch and keep the fastest for later calls (a second or so for
+ * a 16 GB database).  No counterpart in the reference. */
+int ipir_b200_autotune(ipir_server* srv);
+/* The schedule the handle uses for `count` queries. */
+int ipir_b200_get_schedule(const ipir_server* srv, size_t count, ipir_serve_schedule* out);
+/* Kernels launched by the handle's answer pipeline since create. */
+int ipir_b200_launch_count(const ipir_server* srv, unsigned long long* out);
+
+/* ===================================================== part 3: serving loop
+ *
+ * Continuous batching over one or more resident databases: server handles
+ * of any geometry, each created by ipir_server_create.  No counterpart in
+ * the reference, whose batch entry point answers one caller-formed batch
+ * per blocking call (src/capi.h:84-89).
+ *
+ * ipir_serve_submit copies one query for one database into a pinned request
+ * slot and returns a ticket at once.  A worker thread admits waiting
+ * requests, oldest first and up to max_batch at a time, into any free lane
+ * of their database (per-batch device buffers with their own stream): a
+ * request that arrives while a batch runs joins the next batch as soon as a
+ * lane is free, and lanes of one database and of different databases run
+ * concurrently.  A lane batch replays the CUDA graph captured for its batch
+ * size at create.  All device and pinned memory is allocated at create,
+ * with lanes sized to the HBM budget; submit, poll and wait allocate
+ * nothing.  Each response is bit-identical to ipir_answer_batch on the same
+ * query, whatever else shares its batch.
+ *
+ * The database handles must outlive the serving loop; while it runs, do not
+ * autotune them.  The loop never touches a handle's own buffers or stream,
+ * so a handle's blocking entry points stay usable from one other thread. */
+typedef struct ipir_serve ipir_serve;
+
+/* Zero fields take the defaults. */
+typedef struct {
+    size_t max_batch;        /* queries per lane batch (default 64) */
+    size_t lanes_per_db;     /* concurrent batches per database (default 2) */
+    size_t queue_slots;      /* pinned request slots (default 256) */
+    size_t hbm_budget_bytes; /* device bytes for all lanes (default: free memory less 2 GiB);
+                                over budget, max_batch halves, then lanes_per_db drops */
+    int disable_graphs;      /* 1: launch the kernels directly instead of graph replays */
+    int disable_autotune;    /* 1: default schedule instead of timing candidates at create */
+} ipir_serve_config;
+
+typedef struct {
+    uint64_t submitted;
+    uint64_t completed;
+    uint64_t failed;
+    uint64_t batches;
+    uint64_t batched_queries;
+    uint64_t max_batch_seen;
+    size_t queued;     /* admitted to no lane yet */
+    size_t free_slots; /* request slots free */
+} ipir_serve_counters;
+
+/* NULL on error (text in ipir_b200_last_error).  cfg may be NULL. */
+ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_serve_config* cfg);
+/* 0 queued (*ticket set), 1 null argument or bad db index, 3 null view
+ * field, 4 the loop failed earlier (text in ipir_b200_last_error), 6 every
+ * request slot is in use (collect tickets, then retry). */
+int ipir_serve_submit(ipir_serve* sv, size_t db, const ipir_query_view* query, uint64_t* ticket);
+/* Collect a ticket: 0 done (num_cts*4*ring_n u64 written to out_resp if not
+ * NULL, *latency_ms = submit to response on the host), 1 still pending,
+ * 2 unknown or already collected ticket, 4 failed.  Every ticket must be
+ * collected once: that frees its request slot. */
+int ipir_serve_poll(ipir_serve* sv, uint64_t ticket, uint64_t* out_resp, double* latency_ms);
+/* Same, blocking up to timeout_s; 5 when it is still pending then. */
+int ipir_serve_wait(ipir_serve* sv, uint64_t ticket, double timeout_s, uint64_t* out_resp, double* latency_ms);
+int ipir_serve_stats(ipir_serve* sv, ipir_serve_counters* out);
+/* Lanes, batch limit and schedule table (entries 1..min(sched_len-1,
+ * max_batch) of sched) the loop chose for database db. */
+int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_batch, ipir_serve_schedule* sched,
+                       size_t sched_len);
+/* Waits for the batches on the device, fails requests not yet admitted,
+ * frees everything. */
+void ipir_serve_destroy(ipir_serve* sv);
 
 #ifdef __cplusplus
 }

@@ -3,6 +3,9 @@
 #include "host_util.h"
 
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <utility>
 #include <stdexcept>
 
 namespace ipb {
@@ -166,6 +169,25 @@ int setup_geometry(size_t n_entries, size_t w, size_t db_rows, Params* out, cons
     }
     *out = pp;
     return 0;
+}
+
+cudaError_t allow_max_dynamic_smem(const void* kernel) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({kernel, dev})) return cudaSuccess;
+    int optin = 0;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+    cudaFuncAttributes fa{};
+    if ((e = cudaFuncGetAttributes(&fa, kernel))) return e;
+    if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - (int)fa.sharedSizeBytes)))
+        return e;
+    done.insert({kernel, dev});
+    return cudaSuccess;
 }
 
 }  // namespace ipb

@@ -3,6 +3,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "ipb_common.cuh"
 
 namespace ipb {
@@ -32,5 +34,15 @@ void build_tables(DevTables& T);
 int setup_geometry(size_t n_entries, size_t w, size_t db_rows, Params* out, const char** why);
 // Sets the calling thread's text for ipir_b200_last_error().
 void set_last_error(const char* msg);
+
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum (less the kernel's static shared memory), once per kernel and
+// device.  The limit is then the same for every later launch and for every
+// captured graph, whatever size one launch asks for.
+cudaError_t allow_max_dynamic_smem(const void* kernel);
+template <class K>
+inline cudaError_t allow_max_smem(K* kernel) {
+    return allow_max_dynamic_smem(reinterpret_cast<const void*>(kernel));
+}
 
 }  // namespace ipb

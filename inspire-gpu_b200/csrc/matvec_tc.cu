@@ -21,6 +21,7 @@
 #include <cuda.h>
 
 #include "ipb_common.cuh"
+#include "host_util.h"
 #include "ipb_launch.h"
 #include "tc_ptx.cuh"
 
@@ -323,7 +324,7 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     P.stages = (int)std::min<size_t>(8, budget / stage_bytes);
     if (P.stages < 2) return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
-    cudaError_t e = cudaFuncSetAttribute(mv_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_max_smem(mv_tc_kernel);
     if (e) return e;
     const int items = P.n_mtiles * P.n_kchunks;
     const int grid = std::min(items, std::max(1, num_sms));

@@ -10,6 +10,7 @@
 //             ExtProd chain (INTT, decomp, NTT, MAC) in shared memory
 // All arithmetic is exact mod q_l, so every output equals the reference's.
 #include "ipb_common.cuh"
+#include "host_util.h"
 #include "ipb_launch.h"
 
 namespace ipb {
@@ -477,17 +478,17 @@ cudaError_t launch_matvec(const uint16_t* db, size_t rows, size_t cols, int chun
     cudaError_t e;
     if (bt == 1) {
         auto k = matvec_kernel<1, 8>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        if ((e = allow_max_smem(k))) return e;
         k<<<dim3((unsigned)(cols / 2048), chunks), 256, smem, s>>>(db, rows, cols, rpc, qraw, qstride, T, part,
                                                                    part_qstride, nq);
     } else if (bt == 2) {
         auto k = matvec_kernel<2, 4>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        if ((e = allow_max_smem(k))) return e;
         k<<<dim3((unsigned)(cols / 1024), chunks), 256, smem, s>>>(db, rows, cols, rpc, qraw, qstride, T, part,
                                                                    part_qstride, nq);
     } else {
         auto k = matvec_kernel<4, 4>;
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        if ((e = allow_max_smem(k))) return e;
         k<<<dim3((unsigned)(cols / 1024), chunks), 256, smem, s>>>(db, rows, cols, rpc, qraw, qstride, T, part,
                                                                    part_qstride, nq);
     }
@@ -509,8 +510,7 @@ cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_
                           const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                           size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(horner_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kHornerSmem);
+    cudaError_t e = allow_max_smem(horner_kernel);
     if (e) return e;
     horner_kernel<<<dim3((unsigned)num_cts, nq), 1024, kHornerSmem, s>>>(pre_a, packed_b, pb_qstride, rgsw32, T,
                                                                           groups, d_act, resp, resp_qstride);
@@ -521,8 +521,7 @@ cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_
                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                                   size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(horner_cl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kHornerClSmem);
+    cudaError_t e = allow_max_smem(horner_cl_kernel);
     if (e) return e;
     horner_cl_kernel<<<dim3((unsigned)(4 * num_cts), nq), 512, kHornerClSmem, s>>>(pre_a, packed_b, pb_qstride,
                                                                                    rgsw32, T, groups, d_act, resp,
@@ -534,7 +533,7 @@ cudaError_t launch_ntt_batch(uint32_t* polys, size_t n, int limb_run, bool inver
                              cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const size_t smem = 4 * 2 * kN * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute(ntt_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_max_smem(ntt_batch_kernel);
     if (e) return e;
     ntt_batch_kernel<<<(unsigned)((n + 3) / 4), 1024, smem, s>>>(polys, n, limb_run, inverse, T);
     return cudaGetLastError();

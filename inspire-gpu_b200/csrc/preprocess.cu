@@ -20,6 +20,7 @@
 //                 direction), the KSK permutations computed in registers.
 //   collapse_final  CollapseOne -> D_final and the packed a.
 #include "ipb_common.cuh"
+#include "host_util.h"
 #include "ipb_launch.h"
 
 namespace ipb {
@@ -352,7 +353,7 @@ cudaError_t launch_encode_pass(const uint16_t* src, uint16_t* dst, size_t nrows,
     if (nl < 1 || nl > 4 || (d_act >> nl) == 0) return cudaErrorInvalidValue;
     const size_t num_cts = (cols / kN) / d_act;
     const size_t smem = (size_t)2 * (1 << nl) * kN * sizeof(uint16_t);
-    cudaError_t e = cudaFuncSetAttribute(encode_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_max_smem(encode_pass_kernel);
     if (e) return e;
     dim3 grid((unsigned)nrows, (unsigned)(num_cts * (d_act >> nl)));
     encode_pass_kernel<<<grid, 256, smem, s>>>(src, dst, cols, d_act, logd, l0, nl, first, last, d_inv);
@@ -361,7 +362,7 @@ cudaError_t launch_encode_pass(const uint16_t* src, uint16_t* dst, size_t nrows,
 
 cudaError_t launch_a_side(const uint16_t* db, size_t rows, size_t cols, size_t g, const uint32_t* crs,
                           const DevTables* T, uint32_t* V, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(a_side_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kASideSmem);
+    cudaError_t e = allow_max_smem(a_side_kernel);
     if (e) return e;
     a_side_kernel<<<kN / 8, 1024, kASideSmem, s>>>(db, rows, cols, g, crs, T, V);
     return cudaGetLastError();
@@ -369,7 +370,7 @@ cudaError_t launch_a_side(const uint16_t* db, size_t rows, size_t cols, size_t g
 
 cudaError_t launch_col_ntt(const uint32_t* V, const DevTables* T, uint32_t* Tout, cudaStream_t s) {
     const size_t smem = 4 * 2 * kN * sizeof(uint32_t);
-    cudaError_t e = cudaFuncSetAttribute(col_ntt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_max_smem(col_ntt_kernel);
     if (e) return e;
     col_ntt_kernel<<<dim3(kN / 4, 2), 1024, smem, s>>>(V, T, Tout);
     return cudaGetLastError();
@@ -383,8 +384,7 @@ cudaError_t launch_embed_gather(const uint32_t* Tin, uint32_t* a_post, cudaStrea
 cudaError_t launch_collapse_a(const uint32_t* a_post, size_t ap_gstride, const uint32_t* k5, const DevTables* T,
                               uint32_t* dp, uint32_t* dm, uint32_t* ends, size_t ngroups, cudaStream_t s) {
     if (ngroups == 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(collapse_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kCollapseASmem);
+    cudaError_t e = allow_max_smem(collapse_a_kernel);
     if (e) return e;
     collapse_a_kernel<<<dim3((unsigned)ngroups, 2), 512, kCollapseASmem, s>>>(a_post, ap_gstride, k5, T, dp, dm, ends);
     return cudaGetLastError();

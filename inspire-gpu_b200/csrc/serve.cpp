@@ -1,0 +1,526 @@
+// serve.cpp -- continuous-batching serving loop over resident databases
+// (the ipir_serve_* entry points).  The reference has no counterpart: its
+// batch entry point answers one caller-formed batch per blocking call
+// (src/gpu_protocol.cu:1414-1535, src/capi.h:84-89).
+//
+// Requests enter pinned request slots (submit copies the query there and
+// returns a ticket).  One worker thread owns every device call: for each
+// database it admits waiting requests, oldest first and at most max_batch
+// at a time, into any free lane -- a set of per-batch device buffers with
+// its own stream -- so requests that arrive while a batch runs form the next
+// batch at once instead of waiting for the previous one to finish, and the
+// lanes of one database and of different databases overlap on the device.
+// A lane batch is: one H2D copy per query, one replay of the CUDA graph
+// captured for that batch size, one D2H copy per response straight into its
+// request slot, the error word, and a host function that tells the worker.
+// Everything is allocated at create; the request path allocates nothing.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "inspire_b200.h"
+#include "server_internal.h"
+
+namespace ipb {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+enum SlotState : int { kFree = 0, kFilling, kQueued, kRunning, kDone, kFailed, kCollecting };
+
+struct ReqSlot {
+    uint64_t ticket = 0;
+    int state = kFree;
+    size_t db = 0;
+    uint64_t* q = nullptr;     // pinned flat query (the database's qstride words)
+    uint64_t* resp = nullptr;  // pinned response
+    Clock::time_point t_submit, t_done;
+};
+
+struct Engine;
+
+struct LaneRun {
+    Lane lane;
+    cudaStream_t st = nullptr;
+    std::vector<cudaGraphExec_t> graphs;  // [batch size], index 0 unused
+    bool busy = false;
+    std::vector<uint32_t> slots;
+    int* h_err = nullptr;  // pinned device-error word of the last batch
+    std::atomic<int> done{0};
+    Engine* eng = nullptr;
+};
+
+struct DbState {
+    Server* S = nullptr;
+    size_t max_batch = 0;
+    std::vector<Sched> sched;
+    std::vector<std::unique_ptr<LaneRun>> lanes;
+    std::deque<uint32_t> pending;
+    uint64_t batches = 0, queries = 0;
+};
+
+struct Engine {
+    std::vector<std::unique_ptr<DbState>> dbs;
+    size_t q_words = 0, r_words = 0;  // per request slot
+    std::vector<ReqSlot> slots;
+    std::vector<uint32_t> free_slots;
+    uint64_t* pinned_q = nullptr;
+    uint64_t* pinned_r = nullptr;
+    int* pinned_err = nullptr;
+    bool use_graphs = true;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread worker;
+    bool stop = false;
+    bool failed = false;
+    std::string fail_text;
+    uint64_t next_seq = 1;
+    uint64_t submitted = 0, completed = 0, n_failed = 0, batches = 0, batched = 0, max_seen = 0;
+
+    ~Engine();
+    void run();
+    void issue(DbState& d, LaneRun& r);
+    void finish(DbState& d, LaneRun& r);
+    void fail_all_locked(const std::string& why);
+};
+
+void CUDART_CB on_lane_done(void* p) {
+    // Runs on a CUDA callback thread: no CUDA calls, no engine lock.
+    auto* r = static_cast<LaneRun*>(p);
+    r->done.store(1, std::memory_order_release);
+    r->eng->cv_work.notify_one();
+}
+
+void Engine::issue(DbState& d, LaneRun& r) {
+    const Server& S = *d.S;
+    Lane& L = r.lane;
+    const size_t n = r.slots.size();
+    IPB_CK(cudaSetDevice(S.device));
+    for (size_t i = 0; i < n; ++i) stage_query_flat(S, L, i, slots[r.slots[i]].q, r.st);
+    if (use_graphs)
+        IPB_CK(cudaGraphLaunch(r.graphs[n], r.st));
+    else
+        run_pipeline(S, L, d.sched[n], n, r.st, nullptr);
+    const size_t rb = S.resp_qstride * 8;
+    for (size_t i = 0; i < n; ++i)
+        IPB_CK(cudaMemcpyAsync(slots[r.slots[i]].resp, L.resp + i * S.resp_qstride, rb, cudaMemcpyDeviceToHost,
+                               r.st));
+    IPB_CK(cudaMemcpyAsync(r.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost, r.st));
+    IPB_CK(cudaMemsetAsync(L.d_err, 0, sizeof(int), r.st));
+    IPB_CK(cudaLaunchHostFunc(r.st, on_lane_done, &r));
+}
+
+// Called with the lock held, after the lane's host function ran.
+void Engine::finish(DbState& d, LaneRun& r) {
+    const int err = *r.h_err;
+    const auto now = Clock::now();
+    for (uint32_t s : r.slots) {
+        slots[s].state = err ? kFailed : kDone;
+        slots[s].t_done = now;
+    }
+    if (err) {
+        n_failed += r.slots.size();
+        fail_text = "device pipeline wait timed out (code " + std::to_string(err) + ")";
+    } else {
+        completed += r.slots.size();
+    }
+    ++d.batches;
+    d.queries += r.slots.size();
+    ++batches;
+    batched += r.slots.size();
+    max_seen = std::max<uint64_t>(max_seen, r.slots.size());
+    r.slots.clear();
+    r.busy = false;
+    r.done.store(0, std::memory_order_relaxed);
+    cv_done.notify_all();
+}
+
+void Engine::fail_all_locked(const std::string& why) {
+    failed = true;
+    fail_text = why;
+    for (auto& d : dbs) {
+        for (uint32_t s : d->pending) slots[s].state = kFailed;
+        n_failed += d->pending.size();
+        d->pending.clear();
+    }
+    cv_done.notify_all();
+}
+
+void Engine::run() {
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        bool any_busy = false;
+        for (auto& dp : dbs)
+            for (auto& r : dp->lanes)
+                if (r->busy) {
+                    if (r->done.load(std::memory_order_acquire))
+                        finish(*dp, *r);
+                    else
+                        any_busy = true;
+                }
+        if (stop && !any_busy) break;
+        if (!stop && !failed) {
+            for (auto& dp : dbs) {
+                DbState& d = *dp;
+                for (auto& r : d.lanes) {
+                    if (d.pending.empty()) break;
+                    if (r->busy) continue;
+                    const size_t n = std::min(d.max_batch, d.pending.size());
+                    for (size_t i = 0; i < n; ++i) {
+                        const uint32_t s = d.pending.front();
+                        d.pending.pop_front();
+                        slots[s].state = kRunning;
+                        r->slots.push_back(s);
+                    }
+                    r->busy = true;
+                    any_busy = true;
+                    lk.unlock();
+                    std::string err;
+                    try {
+                        issue(d, *r);
+                    } catch (const std::exception& e) {
+                        err = e.what();
+                    }
+                    lk.lock();
+                    if (!err.empty()) {
+                        // The lane's stream may hold part of the batch: wait for
+                        // it outside the lock, then fail everything.
+                        lk.unlock();
+                        cudaStreamSynchronize(r->st);
+                        lk.lock();
+                        for (uint32_t s : r->slots) slots[s].state = kFailed;
+                        n_failed += r->slots.size();
+                        r->slots.clear();
+                        r->busy = false;
+                        fail_all_locked(err);
+                    }
+                }
+            }
+        }
+        if (stop) {
+            for (auto& d : dbs) {
+                for (uint32_t s : d->pending) slots[s].state = kFailed;
+                n_failed += d->pending.size();
+                d->pending.clear();
+            }
+            cv_done.notify_all();
+        }
+        if (any_busy) {
+            cv_work.wait_for(lk, std::chrono::microseconds(50));
+        } else {
+            bool work = false;
+            for (auto& d : dbs) work |= !d->pending.empty();
+            if (!work && !stop) cv_work.wait_for(lk, std::chrono::milliseconds(20));
+        }
+    }
+}
+
+Engine::~Engine() {
+    for (auto& dp : dbs) {
+        DbState& d = *dp;
+        cudaSetDevice(d.S->device);
+        for (auto& r : d.lanes) {
+            if (r->st) cudaStreamSynchronize(r->st);
+            for (auto g : r->graphs)
+                if (g) cudaGraphExecDestroy(g);
+            if (r->st) cudaStreamDestroy(r->st);
+            r->lane.arena.free_all();
+        }
+    }
+    if (pinned_q) cudaFreeHost(pinned_q);
+    if (pinned_r) cudaFreeHost(pinned_r);
+    if (pinned_err) cudaFreeHost(pinned_err);
+}
+
+void capture_graphs(DbState& d, LaneRun& r) {
+    const Server& S = *d.S;
+    r.graphs.assign(d.max_batch + 1, nullptr);
+    for (size_t c = 1; c <= d.max_batch; ++c) {
+        // An eager run first: kernel attributes are set outside the capture.
+        run_pipeline(S, r.lane, d.sched[c], c, r.st, nullptr);
+        IPB_CK(cudaStreamBeginCapture(r.st, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t g = nullptr;
+        try {
+            run_pipeline(S, r.lane, d.sched[c], c, r.st, nullptr);
+        } catch (...) {
+            cudaStreamEndCapture(r.st, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        IPB_CK(cudaStreamEndCapture(r.st, &g));
+        cudaGraphExec_t ge = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        IPB_CK(e);
+        r.graphs[c] = ge;
+    }
+    IPB_CK(cudaStreamSynchronize(r.st));
+}
+
+}  // namespace
+}  // namespace ipb
+
+struct ipir_serve {
+    ipb::Engine* e;
+};
+
+namespace {
+template <class F>
+int serve_guarded(F&& f, int fail_code) {
+    try {
+        return f();
+    } catch (const std::exception& e) {
+        ipb::set_last_error(e.what());
+    } catch (...) {
+        ipb::set_last_error("unknown error");
+    }
+    return fail_code;
+}
+}  // namespace
+
+extern "C" {
+
+ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_serve_config* cfg_in) {
+    if (!dbs || n_dbs == 0) {
+        ipb::set_last_error("ipir_serve_create: no databases");
+        return nullptr;
+    }
+    ipir_serve_config cfg{};
+    if (cfg_in) cfg = *cfg_in;
+    if (!cfg.max_batch) cfg.max_batch = 64;
+    if (!cfg.lanes_per_db) cfg.lanes_per_db = 2;
+    if (!cfg.queue_slots) cfg.queue_slots = 256;
+    ipir_serve* out = nullptr;
+    serve_guarded(
+        [&]() -> int {
+            auto E = std::make_unique<ipb::Engine>();
+            E->use_graphs = cfg.disable_graphs == 0;
+            for (size_t i = 0; i < n_dbs; ++i) {
+                if (!dbs[i] || !dbs[i]->s) throw std::invalid_argument("ipir_serve_create: null database handle");
+                auto d = std::make_unique<ipb::DbState>();
+                d->S = dbs[i]->s;
+                E->dbs.push_back(std::move(d));
+            }
+            // Size lanes by the HBM budget: halve the batch, then the lane
+            // count, until every database's lanes fit.
+            IPB_CK(cudaSetDevice(E->dbs[0]->S->device));
+            size_t budget = cfg.hbm_budget_bytes;
+            if (!budget) {
+                size_t fr = 0, tot = 0;
+                IPB_CK(cudaMemGetInfo(&fr, &tot));
+                const size_t reserve = (size_t)2 << 30;
+                budget = fr > reserve ? fr - reserve : 0;
+            }
+            size_t mb = cfg.max_batch, lanes = cfg.lanes_per_db;
+            auto need = [&](size_t b, size_t l) {
+                size_t t = 0;
+                for (auto& d : E->dbs) t += l * ipb::lane_bytes(*d->S, b, ipb::lane_gt_pass(*d->S, b));
+                return t;
+            };
+            while (need(mb, lanes) > budget) {
+                if (mb > 1) mb /= 2;
+                else if (lanes > 1) --lanes;
+                else throw std::runtime_error("ipir_serve_create: one lane per database exceeds the HBM budget");
+            }
+            size_t q_words = 0, r_words = 0;
+            for (auto& dp : E->dbs) {
+                ipb::DbState& d = *dp;
+                d.max_batch = mb;
+                q_words = std::max(q_words, d.S->qstride);
+                r_words = std::max(r_words, d.S->resp_qstride);
+                for (size_t k = 0; k < lanes; ++k) {
+                    auto r = std::make_unique<ipb::LaneRun>();
+                    r->eng = E.get();
+                    IPB_CK(cudaSetDevice(d.S->device));
+                    IPB_CK(cudaStreamCreateWithFlags(&r->st, cudaStreamNonBlocking));
+                    ipb::alloc_lane(*d.S, r->lane, mb, ipb::lane_gt_pass(*d.S, mb));
+                    d.lanes.push_back(std::move(r));
+                }
+                d.sched = !cfg.disable_autotune ? ipb::autotune(*d.S, d.lanes[0]->lane, d.lanes[0]->st)
+                                       : ipb::default_sched(*d.S, mb, d.lanes[0]->lane.gt_pass);
+                if (E->use_graphs)
+                    for (auto& r : d.lanes) ipb::capture_graphs(d, *r);
+            }
+            E->q_words = q_words;
+            E->r_words = r_words;
+            const size_t Q = cfg.queue_slots;
+            IPB_CK(cudaMallocHost(&E->pinned_q, Q * q_words * 8));
+            IPB_CK(cudaMallocHost(&E->pinned_r, Q * r_words * 8));
+            size_t n_lanes = 0;
+            for (auto& d : E->dbs) n_lanes += d->lanes.size();
+            IPB_CK(cudaMallocHost(&E->pinned_err, n_lanes * sizeof(int)));
+            size_t li = 0;
+            for (auto& d : E->dbs)
+                for (auto& r : d->lanes) {
+                    r->h_err = E->pinned_err + li++;
+                    *r->h_err = 0;
+                }
+            E->slots.resize(Q);
+            for (size_t s = 0; s < Q; ++s) {
+                E->slots[s].q = E->pinned_q + s * q_words;
+                E->slots[s].resp = E->pinned_r + s * r_words;
+                E->free_slots.push_back((uint32_t)(Q - 1 - s));
+            }
+            ipb::Engine* raw = E.get();
+            E->worker = std::thread([raw] {
+                cudaSetDevice(raw->dbs[0]->S->device);
+                raw->run();
+            });
+            out = new ipir_serve{E.release()};
+            return 0;
+        },
+        1);
+    return out;
+}
+
+int ipir_serve_submit(ipir_serve* sv, size_t db, const ipir_query_view* q, uint64_t* ticket) {
+    if (!sv || !q || !ticket) return 1;
+    ipb::Engine& E = *sv->e;
+    if (db >= E.dbs.size()) return 1;
+    if (!q->lwe_b_limb0 || !q->lwe_b_limb1 || !q->ksk5_b || !q->kskneg1_b || !q->rgsw) return 3;
+    uint32_t s;
+    {
+        std::lock_guard<std::mutex> lk(E.mu);
+        if (E.failed) {
+            ipb::set_last_error(E.fail_text.c_str());
+            return 4;
+        }
+        if (E.free_slots.empty()) return 6;
+        s = E.free_slots.back();
+        E.free_slots.pop_back();
+        ipb::ReqSlot& r = E.slots[s];
+        r.state = ipb::kFilling;
+        r.db = db;
+        r.ticket = E.next_seq++ * E.slots.size() + s;
+        *ticket = r.ticket;
+    }
+    const ipb::Server& S = *E.dbs[db]->S;
+    const size_t R = S.pp.db_rows, B = ipb::kBlk;
+    uint64_t* d = E.slots[s].q;
+    std::memcpy(d, q->lwe_b_limb0, R * 8);
+    std::memcpy(d + R, q->lwe_b_limb1, R * 8);
+    std::memcpy(d + 2 * R, q->ksk5_b, B * 8);
+    std::memcpy(d + 2 * R + B, q->kskneg1_b, B * 8);
+    std::memcpy(d + 2 * R + 2 * B, q->rgsw, 4 * B * 8);
+    {
+        std::lock_guard<std::mutex> lk(E.mu);
+        ipb::ReqSlot& r = E.slots[s];
+        r.t_submit = ipb::Clock::now();
+        if (E.failed) {
+            r.state = ipb::kFailed;
+            ++E.n_failed;
+        } else {
+            r.state = ipb::kQueued;
+            E.dbs[db]->pending.push_back(s);
+            ++E.submitted;
+        }
+    }
+    E.cv_work.notify_one();
+    return 0;
+}
+
+namespace {
+// Collects a finished slot: 0 done, 1 pending, 2 unknown ticket, 4 failed.
+int collect(ipb::Engine& E, std::unique_lock<std::mutex>& lk, uint64_t ticket, uint64_t* out, double* lat) {
+    const size_t s = (size_t)(ticket % E.slots.size());
+    ipb::ReqSlot& r = E.slots[s];
+    if (r.ticket != ticket || r.state == ipb::kFree || r.state == ipb::kCollecting) return 2;
+    if (r.state == ipb::kFailed) {
+        ipb::set_last_error(E.fail_text.empty() ? "request failed" : E.fail_text.c_str());
+        r.state = ipb::kFree;
+        E.free_slots.push_back((uint32_t)s);
+        return 4;
+    }
+    if (r.state != ipb::kDone) return 1;
+    if (lat) *lat = std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
+    r.state = ipb::kCollecting;
+    const size_t words = E.dbs[r.db]->S->resp_qstride;
+    lk.unlock();
+    if (out) std::memcpy(out, r.resp, words * 8);
+    lk.lock();
+    r.state = ipb::kFree;
+    E.free_slots.push_back((uint32_t)s);
+    return 0;
+}
+}  // namespace
+
+int ipir_serve_poll(ipir_serve* sv, uint64_t ticket, uint64_t* out_resp, double* latency_ms) {
+    if (!sv) return 1;
+    std::unique_lock<std::mutex> lk(sv->e->mu);
+    return collect(*sv->e, lk, ticket, out_resp, latency_ms);
+}
+
+int ipir_serve_wait(ipir_serve* sv, uint64_t ticket, double timeout_s, uint64_t* out_resp, double* latency_ms) {
+    if (!sv) return 1;
+    ipb::Engine& E = *sv->e;
+    const auto deadline = ipb::Clock::now() + std::chrono::duration_cast<ipb::Clock::duration>(
+                                                  std::chrono::duration<double>(std::max(0.0, timeout_s)));
+    std::unique_lock<std::mutex> lk(E.mu);
+    for (;;) {
+        const int rc = collect(E, lk, ticket, out_resp, latency_ms);
+        if (rc != 1) return rc;
+        if (E.cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
+            const int rc2 = collect(E, lk, ticket, out_resp, latency_ms);
+            return rc2 == 1 ? 5 : rc2;
+        }
+    }
+}
+
+int ipir_serve_stats(ipir_serve* sv, ipir_serve_counters* out) {
+    if (!sv || !out) return 1;
+    ipb::Engine& E = *sv->e;
+    std::lock_guard<std::mutex> lk(E.mu);
+    out->submitted = E.submitted;
+    out->completed = E.completed;
+    out->failed = E.n_failed;
+    out->batches = E.batches;
+    out->batched_queries = E.batched;
+    out->max_batch_seen = E.max_seen;
+    size_t q = 0;
+    for (auto& d : E.dbs) q += d->pending.size();
+    out->queued = q;
+    out->free_slots = E.free_slots.size();
+    return 0;
+}
+
+int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_batch, ipir_serve_schedule* sched,
+                       size_t sched_len) {
+    if (!sv) return 1;
+    ipb::Engine& E = *sv->e;
+    if (db >= E.dbs.size()) return 1;
+    const ipb::DbState& d = *E.dbs[db];
+    if (lanes) *lanes = d.lanes.size();
+    if (max_batch) *max_batch = d.max_batch;
+    if (sched)
+        for (size_t c = 1; c < sched_len && c <= d.max_batch; ++c) {
+            sched[c].matvec_tc = d.sched[c].matvec_tc;
+            sched[c].tp_pass = d.sched[c].tp_pass;
+            sched[c].horner_cluster = d.sched[c].horner_cluster;
+        }
+    return 0;
+}
+
+void ipir_serve_destroy(ipir_serve* sv) {
+    if (!sv) return;
+    ipb::Engine* E = sv->e;
+    {
+        std::lock_guard<std::mutex> lk(E->mu);
+        E->stop = true;
+    }
+    E->cv_work.notify_all();
+    if (E->worker.joinable()) E->worker.join();
+    delete E;
+    delete sv;
+}
+
+}  // extern "C"

@@ -1,5 +1,6 @@
 // server.cpp -- host orchestration of the B200 InsPIRe server: preprocess,
-// server context, answer pipeline, caps, and the C / C++ entry points.
+// server context, answer pipeline, schedule autotuner, caps, and the C / C++
+// entry points.
 //
 // Reference counterparts: src/gpu_protocol.cu (GpuServerCtx, gpu_preprocess,
 // gpu_setup_server, answer_one, gpu_answer_batch, caps, free) and
@@ -17,19 +18,25 @@
 #include <thread>
 #include <vector>
 
-#include "host_util.h"
 #include "inspire_b200.h"
 #include "inspire_b200.hpp"
-#include "ipb_launch.h"
+#include "server_internal.h"
 
 namespace ipb {
 
 namespace {
 thread_local std::string g_last_error;
 
-struct CudaFailure : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
+uint32_t inv_mod_p(uint32_t d) {  // d^-1 mod 65535 (d a power of two)
+    int64_t old_r = d, r = kP, old_s = 1, s = 0;
+    while (r) {
+        int64_t qq = old_r / r, t = r;
+        r = old_r - qq * r; old_r = t;
+        t = s; s = old_s - qq * s; old_s = t;
+    }
+    return (uint32_t)((old_s % (int64_t)kP + kP) % kP);
+}
+}  // namespace
 
 [[noreturn]] void cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
     char buf[512];
@@ -37,31 +44,8 @@ struct CudaFailure : std::runtime_error {
                   what);
     throw CudaFailure(buf);
 }
-#define IPB_CK(call)                                                      \
-    do {                                                                  \
-        cudaError_t e_ = (call);                                          \
-        if (e_ != cudaSuccess) ::ipb::cuda_fail(e_, #call, __FILE__, __LINE__);  \
-    } while (0)
 
-// Device allocation list freed together.
-struct DevArena {
-    std::vector<void*> ptrs;
-    size_t bytes = 0;
-    template <class T>
-    T* alloc(size_t count) {
-        void* p = nullptr;
-        const size_t b = count * sizeof(T);
-        IPB_CK(cudaMalloc(&p, b ? b : 16));
-        ptrs.push_back(p);
-        bytes += b;
-        return static_cast<T*>(p);
-    }
-    void free_all() {
-        for (void* p : ptrs) cudaFree(p);
-        ptrs.clear();
-        bytes = 0;
-    }
-};
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
 const DevTables& host_tables() {
     static DevTables T;
@@ -75,45 +59,6 @@ DevTables* upload_tables(DevArena& A, cudaStream_t s) {
     IPB_CK(cudaMemcpyAsync(d, &host_tables(), sizeof(DevTables), cudaMemcpyHostToDevice, s));
     return d;
 }
-
-uint32_t inv_mod_p(uint32_t d) {  // d^-1 mod 65535 (d a power of two)
-    int64_t old_r = d, r = kP, old_s = 1, s = 0;
-    while (r) {
-        int64_t qq = old_r / r, t = r;
-        r = old_r - qq * r; old_r = t;
-        t = s; s = old_s - qq * s; old_s = t;
-    }
-    return (uint32_t)((old_s % (int64_t)kP + kP) % kP);
-}
-
-constexpr size_t kGroupStrideD = (size_t)2 * kSteps * kDeff * kN;  // u32 per group, D_plus / D_minus
-constexpr size_t kGroupStrideF = (size_t)2 * kDeff * kN;
-constexpr size_t kGroupStrideA = (size_t)2 * kN;
-constexpr size_t kBlk = (size_t)kDeff * 2 * kN;                    // one KSK / RGSW part
-constexpr size_t kKeyStride = 4 * kDeff * kN;                      // keys per query (u32)
-constexpr size_t kRgswStride = 4 * kBlk;                           // rgsw32 per query (u32)
-}  // namespace
-
-void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
-
-// --------------------------------------------------------------- precomp state
-struct Precomp {
-    Params pp{};
-    int device = 0;
-    DevArena arena;  // owns everything below
-    DevTables* tables = nullptr;
-    uint16_t* db = nullptr;
-    uint32_t* pre_a = nullptr;
-    uint8_t* pre_dt = nullptr;   // D_plus / D_minus as GEMM byte planes [l][i][g*4+a][4096]
-    uint32_t* pre_df = nullptr;
-    bool adopted = false;
-    ~Precomp() {
-        if (!adopted) {
-            cudaSetDevice(device);
-            arena.free_all();
-        }
-    }
-};
 
 // gpu_preprocess (reference src/gpu_protocol.cu:535-817) on one stream.
 static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s) {
@@ -217,55 +162,54 @@ static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s)
 }
 
 // --------------------------------------------------------------- server
-struct Server {
-    Params pp{};
-    int device = 0;
-    size_t max_batch = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    std::shared_ptr<Precomp> pre;
-    DevArena arena;
-    uint64_t* qraw = nullptr;
-    uint32_t* keys = nullptr;
-    uint32_t* rgsw32 = nullptr;
-    uint32_t* mvpart = nullptr;
-    uint8_t* gt = nullptr;        // per-batch permuted-key planes (tensor pass N operand)
-    uint32_t* tp_out = nullptr;   // tensor pass result [l][i][q][g]
-    uint32_t* packed_b = nullptr;
-    uint64_t* resp = nullptr;
-    uint8_t* planes = nullptr;   // query byte planes for the tensor-core mat-vec
-    int* d_err = nullptr;        // device error word (pipeline wait timeouts)
-    size_t qstride = 0, mv_qstride = 0, pb_qstride = 0, resp_qstride = 0;
-    int mv_chunks = 1, tp_pass = 32;
-    bool use_tc = true;          // tcgen05 mat-vec (IPB_MATVEC=simt selects the CUDA-core kernel)
-    bool horner_cluster = true;  // 4-CTA cluster per chain (IPB_HORNER=cta selects one CTA per chain)
-    int num_sms = 148;
-    int tc_kchunk_rows = 0, tc_kchunks = 1;
-    int last_mv_chunks = 1;
-    size_t staged = 0;
-    bool timing = false;
-    cudaEvent_t ev[6] = {};
-    float stage_ms[5] = {};
-    size_t resident_bytes = 0;
-
-    ~Server() {
-        cudaSetDevice(device);
-        if (stream) cudaStreamSynchronize(stream);
-        for (auto& e : ev)
-            if (e) cudaEventDestroy(e);
-        arena.free_all();
-        if (pre) {
-            pre->adopted = false;  // Precomp frees the DB and tensors
-            pre.reset();
-        }
-        if (own_stream) cudaStreamDestroy(own_stream);
+Server::~Server() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    lane.arena.free_all();
+    if (pre) {
+        pre->adopted = false;  // Precomp frees the DB and tensors
+        pre.reset();
     }
-};
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
 
 static int pick_pow2_chunks(size_t target, size_t maxv) {
     size_t c = 1;
     while (c < target && c * 2 <= maxv) c *= 2;
     return (int)c;
+}
+
+size_t lane_bytes(const Server& S, size_t cap, int gt_pass) {
+    const size_t R = S.pp.db_rows, G = S.pp.n_packed;
+    return cap * S.qstride * 8 + cap * kKeyStride * 4 + cap * kRgswStride * 4 + cap * S.mv_qstride * 4 +
+           tp_gt_bytes(gt_pass) + (size_t)2 * kN * cap * G * 4 + cap * S.pb_qstride * 4 + cap * S.resp_qstride * 8 +
+           mv_tc_planes_bytes(R, (int)cap) + sizeof(int);
+}
+
+void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
+    const size_t R = S.pp.db_rows, G = S.pp.n_packed;
+    DevArena& A = L.arena;
+    L.cap = cap;
+    L.gt_pass = gt_pass;
+    L.qraw = A.alloc<uint64_t>(cap * S.qstride);
+    L.keys = A.alloc<uint32_t>(cap * kKeyStride);
+    L.rgsw32 = A.alloc<uint32_t>(cap * kRgswStride);
+    L.mvpart = A.alloc<uint32_t>(cap * S.mv_qstride);
+    L.gt = A.alloc<uint8_t>(tp_gt_bytes(gt_pass));
+    L.tp_out = A.alloc<uint32_t>((size_t)2 * kN * cap * G);
+    L.packed_b = A.alloc<uint32_t>(cap * S.pb_qstride);
+    L.resp = A.alloc<uint64_t>(cap * S.resp_qstride);
+    L.planes = A.alloc<uint8_t>(mv_tc_planes_bytes(R, (int)cap));
+    L.d_err = A.alloc<int>(1);
+    // Defined contents before any pipeline run (the autotuner runs on them).
+    IPB_CK(cudaMemset(L.qraw, 0, cap * S.qstride * 8));
+    IPB_CK(cudaMemset(L.planes, 0, mv_tc_planes_bytes(R, (int)cap)));
+    IPB_CK(cudaMemset(L.d_err, 0, sizeof(int)));
+    // The lanes run on non-blocking streams, which do not wait for the
+    // legacy stream the memsets above went to.
+    IPB_CK(cudaDeviceSynchronize());
 }
 
 static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_t max_batch) {
@@ -285,41 +229,31 @@ static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_
     // <= 4096 rows per chunk keeps the staged query words (4 queries x 2
     // limbs x rows x 4 B) within 128 KB of shared memory.
     while (R / (size_t)S->mv_chunks > 4096) S->mv_chunks *= 2;
-    S->tp_pass = (int)std::min<size_t>(max_batch, (size_t)tp_pass_queries(G));
     IPB_CK(cudaDeviceGetAttribute(&S->num_sms, cudaDevAttrMultiProcessorCount, S->device));
-    if (const char* m = std::getenv("IPB_MATVEC")) S->use_tc = std::strcmp(m, "simt") != 0;
-    if (const char* h = std::getenv("IPB_HORNER")) S->horner_cluster = std::strcmp(h, "cta") != 0;
     S->tc_kchunk_rows = matvec_tc_kchunk_rows(R, C, S->num_sms);
     S->tc_kchunks = (int)(R / (size_t)S->tc_kchunk_rows);
     S->mv_qstride = (size_t)std::max(S->mv_chunks, S->tc_kchunks) * 2 * C;
-
     S->pb_qstride = G * 2 * kN;
     S->resp_qstride = pp.num_cts * 4 * kN;
-    DevArena& A = S->arena;
-    S->qraw = A.alloc<uint64_t>(max_batch * S->qstride);
-    S->keys = A.alloc<uint32_t>(max_batch * kKeyStride);
-    S->rgsw32 = A.alloc<uint32_t>(max_batch * kRgswStride);
-    S->mvpart = A.alloc<uint32_t>(max_batch * S->mv_qstride);
-    S->gt = A.alloc<uint8_t>(tp_gt_bytes(S->tp_pass));
-    S->tp_out = A.alloc<uint32_t>((size_t)2 * kN * max_batch * G);
-    S->packed_b = A.alloc<uint32_t>(max_batch * S->pb_qstride);
-    S->resp = A.alloc<uint64_t>(max_batch * S->resp_qstride);
-    S->planes = A.alloc<uint8_t>(mv_tc_planes_bytes(R, (int)max_batch));
-    IPB_CK(cudaMemset(S->planes, 0, mv_tc_planes_bytes(R, (int)max_batch)));
-    S->d_err = A.alloc<int>(1);
-    IPB_CK(cudaMemset(S->d_err, 0, sizeof(int)));
+    const int gt_pass = lane_gt_pass(*S, max_batch);
+    S->sched = default_sched(*S, max_batch, gt_pass);
+    alloc_lane(*S, S->lane, max_batch, gt_pass);
     for (auto& e : S->ev) IPB_CK(cudaEventCreate(&e));
     pre->adopted = true;
-    S->resident_bytes = pre->arena.bytes + A.bytes;
+    S->resident_bytes = pre->arena.bytes + S->lane.arena.bytes;
     S->pre = std::move(pre);
     return S.release();
+}
+
+void stage_query_flat(const Server& S, Lane& L, size_t i, const uint64_t* flat, cudaStream_t st) {
+    IPB_CK(cudaMemcpyAsync(L.qraw + i * S.qstride, flat, S.qstride * 8, cudaMemcpyHostToDevice, st));
 }
 
 static void stage_queries(Server* S, const ipir_query_view* qs, size_t count) {
     IPB_CK(cudaSetDevice(S->device));
     const size_t R = S->pp.db_rows;
     for (size_t i = 0; i < count; ++i) {
-        uint64_t* d = S->qraw + i * S->qstride;
+        uint64_t* d = S->lane.qraw + i * S->qstride;
         const ipir_query_view& v = qs[i];
         IPB_CK(cudaMemcpyAsync(d, v.lwe_b_limb0, R * 8, cudaMemcpyHostToDevice, S->stream));
         IPB_CK(cudaMemcpyAsync(d + R, v.lwe_b_limb1, R * 8, cudaMemcpyHostToDevice, S->stream));
@@ -330,70 +264,169 @@ static void stage_queries(Server* S, const ipir_query_view* qs, size_t count) {
     S->staged = count;
 }
 
-static void run_pipeline(Server* S, size_t count) {
-    IPB_CK(cudaSetDevice(S->device));
-    const Params& pp = S->pp;
-    const Precomp& P = *S->pre;
+const Sched& sched_for(const Server& S, size_t c) { return S.sched[std::min(c, S.sched.size() - 1)]; }
+
+int lane_gt_pass(const Server& S, size_t cap) {
+    return (int)std::min<size_t>(cap, (size_t)tp_pass_queries(S.pp.n_packed));
+}
+
+std::vector<Sched> default_sched(const Server&, size_t cap, int gt_pass) {
+    Sched def;
+    def.tp_pass = gt_pass;
+    if (const char* m = std::getenv("IPB_MATVEC")) def.matvec_tc = std::strcmp(m, "simt") != 0;
+    if (const char* h = std::getenv("IPB_HORNER")) def.horner_cluster = std::strcmp(h, "cta") != 0;
+    return std::vector<Sched>(cap + 1, def);
+}
+
+int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev) {
+    if (count == 0) return 0;
+    if (count > L.cap || sc.tp_pass < 1 || sc.tp_pass > L.gt_pass)
+        throw std::invalid_argument("run_pipeline: batch exceeds the lane or its tensor-pass buffer");
+    const Params& pp = S.pp;
+    const Precomp& P = *S.pre;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
     const size_t d_act = std::min(pp.D, G);
-    cudaStream_t st = S->stream;
     const int nq = (int)count;
-    if (S->timing) IPB_CK(cudaEventRecord(S->ev[0], st));
-    IPB_CK(launch_qprep(S->qraw, S->qstride, R, P.tables, S->keys, S->rgsw32, nq, st));
-    if (S->timing) IPB_CK(cudaEventRecord(S->ev[1], st));
-    if (S->use_tc) {
-        IPB_CK(launch_qplanes(S->qraw, S->qstride, R, P.tables, S->planes, nq, st));
+    int launches = 0;
+    if (ev) IPB_CK(cudaEventRecord(ev[0], st));
+    IPB_CK(launch_qprep(L.qraw, S.qstride, R, P.tables, L.keys, L.rgsw32, nq, st));
+    ++launches;
+    if (ev) IPB_CK(cudaEventRecord(ev[1], st));
+    int mv_parts;
+    if (sc.matvec_tc) {
+        IPB_CK(launch_qplanes(L.qraw, S.qstride, R, P.tables, L.planes, nq, st));
+        ++launches;
         for (size_t c0 = 0; c0 < count; c0 += 32) {
             const int n = (int)std::min<size_t>(32, count - c0);
-            IPB_CK(launch_matvec_tc(P.db, R, C, S->planes + 8 * c0 * R, n, P.tables, S->mvpart + c0 * S->mv_qstride,
-                                    S->mv_qstride, S->d_err, S->num_sms, S->tc_kchunk_rows, st));
+            IPB_CK(launch_matvec_tc(P.db, R, C, L.planes + 8 * c0 * R, n, P.tables, L.mvpart + c0 * S.mv_qstride,
+                                    S.mv_qstride, L.d_err, S.num_sms, S.tc_kchunk_rows, st));
+            ++launches;
         }
-        S->last_mv_chunks = S->tc_kchunks;
+        mv_parts = S.tc_kchunks;
     } else {
         for (size_t c0 = 0; c0 < count; c0 += 4) {
             const int n = (int)std::min<size_t>(4, count - c0);
-            IPB_CK(launch_matvec(P.db, R, C, S->mv_chunks, S->qraw + c0 * S->qstride, S->qstride, P.tables,
-                                 S->mvpart + c0 * S->mv_qstride, S->mv_qstride, n, st));
+            IPB_CK(launch_matvec(P.db, R, C, S.mv_chunks, L.qraw + c0 * S.qstride, S.qstride, P.tables,
+                                 L.mvpart + c0 * S.mv_qstride, S.mv_qstride, n, st));
+            ++launches;
         }
-        S->last_mv_chunks = S->mv_chunks;
+        mv_parts = S.mv_chunks;
     }
-    if (S->timing) IPB_CK(cudaEventRecord(S->ev[2], st));
-    for (size_t c0 = 0; c0 < count; c0 += (size_t)S->tp_pass) {
-        const int n = (int)std::min<size_t>((size_t)S->tp_pass, count - c0);
-        IPB_CK(launch_tensor_pass(P.pre_dt, G, S->keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, S->gt,
-                                  S->tp_out, S->d_err, S->num_sms, st));
+    if (ev) IPB_CK(cudaEventRecord(ev[2], st));
+    for (size_t c0 = 0; c0 < count; c0 += (size_t)sc.tp_pass) {
+        const int n = (int)std::min<size_t>((size_t)sc.tp_pass, count - c0);
+        IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.gt, L.tp_out,
+                                  L.d_err, S.num_sms, st));
+        launches += 2;  // permuted-key planes + GEMM
     }
-    if (S->timing) IPB_CK(cudaEventRecord(S->ev[3], st));
-    IPB_CK(launch_finalize(S->mvpart, S->mv_qstride, S->last_mv_chunks, C, S->tp_out,
-                           P.pre_df, S->keys, kKeyStride, P.tables, S->packed_b, S->pb_qstride, G, nq, st));
-    if (S->timing) IPB_CK(cudaEventRecord(S->ev[4], st));
-    if (S->horner_cluster)
-        IPB_CK(launch_horner_cluster(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts,
-                                     S->resp, S->resp_qstride, nq, st));
+    if (ev) IPB_CK(cudaEventRecord(ev[3], st));
+    IPB_CK(launch_finalize(L.mvpart, S.mv_qstride, mv_parts, C, L.tp_out, P.pre_df, L.keys, kKeyStride, P.tables,
+                           L.packed_b, S.pb_qstride, G, nq, st));
+    ++launches;
+    if (ev) IPB_CK(cudaEventRecord(ev[4], st));
+    if (sc.horner_cluster)
+        IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts,
+                                     L.resp, S.resp_qstride, nq, st));
     else
-        IPB_CK(launch_horner(P.pre_a, S->packed_b, S->pb_qstride, S->rgsw32, P.tables, G, d_act, pp.num_cts, S->resp,
-                             S->resp_qstride, nq, st));
-    if (S->timing) IPB_CK(cudaEventRecord(S->ev[5], st));
+        IPB_CK(launch_horner(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts, L.resp,
+                             S.resp_qstride, nq, st));
+    ++launches;
+    if (ev) IPB_CK(cudaEventRecord(ev[5], st));
+    return launches;
+}
+
+static void run_pipeline(Server* S, size_t count) {
+    IPB_CK(cudaSetDevice(S->device));
+    S->launches += (unsigned long long)run_pipeline(*S, S->lane, sched_for(*S, count), count, S->stream,
+                                                    S->timing ? S->ev : nullptr);
 }
 
 // A kernel whose pipeline wait ran out of iterations leaves a code in the
 // device error word; report it (the responses are then not valid).
-static void check_device_error(Server* S) {
+static void check_device_error(Lane& L) {
     int e = 0;
-    IPB_CK(cudaMemcpy(&e, S->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    IPB_CK(cudaMemcpy(&e, L.d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
-        IPB_CK(cudaMemset(S->d_err, 0, sizeof(int)));
+        IPB_CK(cudaMemset(L.d_err, 0, sizeof(int)));
         throw std::runtime_error("device pipeline wait timed out (code " + std::to_string(e) + ")");
     }
 }
 
 static void fetch(Server* S, size_t count, uint64_t* out) {
     IPB_CK(cudaSetDevice(S->device));
-    IPB_CK(cudaMemcpyAsync(out, S->resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, S->stream));
+    IPB_CK(cudaMemcpyAsync(out, S->lane.resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, S->stream));
     IPB_CK(cudaStreamSynchronize(S->stream));
-    check_device_error(S);
+    check_device_error(S->lane);
     if (S->timing)
         for (int i = 0; i < 5; ++i) IPB_CK(cudaEventElapsedTime(&S->stage_ms[i], S->ev[i], S->ev[i + 1]));
+}
+
+// ------------------------------------------------------------ schedule autotuner
+// For batch sizes 1, 2, 4, ... up to the lane's capacity (and the capacity
+// itself) time every candidate schedule end to end on the device -- mat-vec
+// kernel (tcgen05 / CUDA-core; the CUDA-core kernel streams the DB once per
+// 4 queries, so it is tried up to 8), queries per tensor-pass GEMM (the Gt
+// capacity and its half: fewer queries per pass re-read the tensors but
+// double-buffer the accumulators), Horner kernel (cluster / single CTA) --
+// and keep the fastest.  Sizes between two measured ones use the smaller's.
+std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
+    IPB_CK(cudaSetDevice(S.device));
+    std::vector<size_t> sizes;
+    for (size_t b = 1; b <= L.cap; b *= 2) sizes.push_back(b);
+    if (sizes.back() != L.cap) sizes.push_back(L.cap);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    IPB_CK(cudaEventCreate(&e0));
+    IPB_CK(cudaEventCreate(&e1));
+    std::vector<std::pair<size_t, Sched>> best;
+    try {
+        for (size_t b : sizes) {
+            std::vector<Sched> cands;
+            std::vector<int> passes{(int)std::min<size_t>(b, (size_t)L.gt_pass)};
+            if (passes[0] >= 16) passes.push_back(passes[0] / 2);
+            for (int mv : {1, 0}) {
+                if (!mv && b > 8) continue;
+                for (int p : passes)
+                    for (int h : {1, 0}) cands.push_back(Sched{mv, p, h});
+            }
+            float best_ms = 1e30f;
+            Sched pick = cands[0];
+            for (const Sched& c : cands) {
+                run_pipeline(S, L, c, b, st, nullptr);  // warm
+                float ms = 1e30f;
+                for (int r = 0; r < 2; ++r) {
+                    IPB_CK(cudaEventRecord(e0, st));
+                    run_pipeline(S, L, c, b, st, nullptr);
+                    IPB_CK(cudaEventRecord(e1, st));
+                    IPB_CK(cudaEventSynchronize(e1));
+                    float t = 0;
+                    IPB_CK(cudaEventElapsedTime(&t, e0, e1));
+                    ms = std::min(ms, t);
+                }
+                if (ms < best_ms * 0.98f) {  // keep the earlier (default-ordered) choice on near ties
+                    best_ms = ms;
+                    pick = c;
+                }
+            }
+            best.emplace_back(b, pick);
+        }
+        IPB_CK(cudaStreamSynchronize(st));
+        check_device_error(L);
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::vector<Sched> table(L.cap + 1);
+    for (size_t c = 1; c <= L.cap; ++c) {
+        const Sched* s = &best[0].second;
+        for (auto& kv : best)
+            if (kv.first <= c) s = &kv.second;
+        table[c] = *s;
+    }
+    table[0] = table[1];
+    return table;
 }
 
 static int validate_batch(const Server* S, const ipir_query_view* qs, size_t count, const void* out) {
@@ -531,9 +564,6 @@ void gpu_free_server(GpuServerCtx* ctx) {
 }  // namespace inspire_b200
 
 // ======================================================================= C ABI
-struct ipir_server {
-    ipb::Server* s;
-};
 
 namespace {
 template <class F>
@@ -679,6 +709,35 @@ int ipir_b200_enable_stage_timing(ipir_server* srv, int on) {
 int ipir_b200_stage_times(const ipir_server* srv, float* ms_out, size_t n) {
     if (!srv || !ms_out) return 1;
     for (size_t i = 0; i < n && i < 5; ++i) ms_out[i] = srv->s->stage_ms[i];
+    return 0;
+}
+
+int ipir_b200_autotune(ipir_server* srv) {
+    if (!srv) return 1;
+    return guarded(
+        [&]() -> int {
+            ipb::Server* S = srv->s;
+            IPB_CK(cudaSetDevice(S->device));
+            S->sched = ipb::autotune(*S, S->lane, S->stream);
+            S->tuned = true;
+            return 0;
+        },
+        4);
+}
+
+int ipir_b200_get_schedule(const ipir_server* srv, size_t count, ipir_serve_schedule* out) {
+    if (!srv || !out) return 1;
+    if (count == 0 || count > srv->s->max_batch) return 2;
+    const ipb::Sched& sc = ipb::sched_for(*srv->s, count);
+    out->matvec_tc = sc.matvec_tc;
+    out->tp_pass = sc.tp_pass;
+    out->horner_cluster = sc.horner_cluster;
+    return 0;
+}
+
+int ipir_b200_launch_count(const ipir_server* srv, unsigned long long* out) {
+    if (!srv || !out) return 1;
+    *out = srv->s->launches;
     return 0;
 }
 

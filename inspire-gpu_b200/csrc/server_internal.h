@@ -1,0 +1,157 @@
+// server_internal.h -- server state shared by the per-handle entry points
+// (server.cpp) and the serving loop (serve.cpp).  Not installed.
+//
+// A Server is one resident database: its preprocess output (Precomp), its
+// derived geometry, one Lane of per-batch device scratch for the plain
+// blocking entry points, and a schedule table (which mat-vec kernel, how
+// many queries per tensor-pass GEMM, which Horner kernel) per batch size.
+// The serving loop adds more Lanes over the same Precomp.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "host_util.h"
+#include "ipb_launch.h"
+
+namespace ipb {
+
+struct CudaFailure : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+[[noreturn]] void cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define IPB_CK(call)                                                            \
+    do {                                                                        \
+        cudaError_t e_ = (call);                                                \
+        if (e_ != cudaSuccess) ::ipb::cuda_fail(e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+// Device allocations freed together.
+struct DevArena {
+    std::vector<void*> ptrs;
+    size_t bytes = 0;
+    template <class T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        const size_t b = count * sizeof(T);
+        IPB_CK(cudaMalloc(&p, b ? b : 16));
+        ptrs.push_back(p);
+        bytes += b;
+        return static_cast<T*>(p);
+    }
+    void free_all() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+        bytes = 0;
+    }
+};
+
+constexpr size_t kGroupStrideD = (size_t)2 * kSteps * kDeff * kN;  // u32 per group, D_plus / D_minus
+constexpr size_t kGroupStrideF = (size_t)2 * kDeff * kN;
+constexpr size_t kGroupStrideA = (size_t)2 * kN;
+constexpr size_t kBlk = (size_t)kDeff * 2 * kN;                    // one KSK / RGSW part
+constexpr size_t kKeyStride = 4 * kDeff * kN;                      // keys per query (u32)
+constexpr size_t kRgswStride = 4 * kBlk;                           // rgsw32 per query (u32)
+
+const DevTables& host_tables();
+DevTables* upload_tables(DevArena& A, cudaStream_t s);
+
+// Output of gpu_preprocess: the encoded DB and the precomputed tensors.
+struct Precomp {
+    Params pp{};
+    int device = 0;
+    DevArena arena;  // owns everything below
+    DevTables* tables = nullptr;
+    uint16_t* db = nullptr;
+    uint32_t* pre_a = nullptr;
+    uint8_t* pre_dt = nullptr;  // D_plus / D_minus as GEMM byte planes [l][i][g*4+a][4096]
+    uint32_t* pre_df = nullptr;
+    bool adopted = false;
+    ~Precomp() {
+        if (!adopted) {
+            cudaSetDevice(device);
+            arena.free_all();
+        }
+    }
+};
+
+// Kernel choices for one batch size.
+struct Sched {
+    int matvec_tc = 1;       // 1: tcgen05 int8 mat-vec, 0: CUDA-core mat-vec
+    int tp_pass = 32;        // queries per tensor-pass GEMM (<= the lane's Gt capacity)
+    int horner_cluster = 1;  // 1: 4-CTA cluster per chain, 0: one CTA per chain
+};
+
+// Per-batch device scratch for up to `cap` queries.
+struct Lane {
+    DevArena arena;
+    size_t cap = 0;
+    int gt_pass = 0;  // queries per tensor pass the Gt buffer holds
+    uint64_t* qraw = nullptr;
+    uint32_t* keys = nullptr;
+    uint32_t* rgsw32 = nullptr;
+    uint32_t* mvpart = nullptr;
+    uint8_t* gt = nullptr;       // per-pass permuted-key planes (tensor-pass N operand)
+    uint32_t* tp_out = nullptr;  // tensor-pass result [l][i][q][g]
+    uint32_t* packed_b = nullptr;
+    uint64_t* resp = nullptr;
+    uint8_t* planes = nullptr;   // query byte planes for the tensor-core mat-vec
+    int* d_err = nullptr;        // device error word (pipeline wait timeouts)
+    ~Lane() { arena.free_all(); }
+};
+
+struct Server {
+    Params pp{};
+    int device = 0;
+    size_t max_batch = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::shared_ptr<Precomp> pre;
+    Lane lane;
+    // geometry derived at setup
+    size_t qstride = 0, mv_qstride = 0, pb_qstride = 0, resp_qstride = 0;
+    int mv_chunks = 1;
+    int num_sms = 148;
+    int tc_kchunk_rows = 0, tc_kchunks = 1;
+    // sched[c] for batch size c (index 0 unused); env overrides applied at setup
+    std::vector<Sched> sched;
+    bool tuned = false;
+    size_t staged = 0;
+    bool timing = false;
+    cudaEvent_t ev[6] = {};
+    float stage_ms[5] = {};
+    size_t resident_bytes = 0;
+    unsigned long long launches = 0;  // kernels launched through this handle's pipeline
+
+    ~Server();
+};
+
+// Bytes of a lane of `cap` queries whose Gt holds `gt_pass` queries.
+size_t lane_bytes(const Server& S, size_t cap, int gt_pass);
+void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass);
+// Enqueues the answer pipeline for `count` staged queries of lane L on
+// stream st; returns the number of kernels launched.  ev (6 events) or null.
+int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev);
+// H2D of one flat query into query slot i of lane L.
+void stage_query_flat(const Server& S, Lane& L, size_t i, const uint64_t* flat, cudaStream_t st);
+// Schedule table (index = batch size, 0 unused) for a lane of `cap` queries
+// whose Gt holds gt_pass: the handle's defaults (env overrides included).
+std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass);
+// Measures candidate schedules per batch size on lane L; returns the table.
+std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st);
+// Sched for batch size c of the handle's own table.
+const Sched& sched_for(const Server& S, size_t c);
+// Queries per tensor-pass GEMM a lane of `cap` queries provisions Gt for.
+int lane_gt_pass(const Server& S, size_t cap);
+
+}  // namespace ipb
+
+// The C ABI handle (opaque in the public header).
+struct ipir_server {
+    ipb::Server* s;
+};

@@ -24,6 +24,7 @@
 #include <algorithm>
 
 #include "ipb_common.cuh"
+#include "host_util.h"
 #include "ipb_launch.h"
 #include "tc_ptx.cuh"
 
@@ -423,7 +424,7 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     if (!make_map(&ma, Dt, (uint64_t)2 * kN * 4 * G, (uint32_t)P.rows_box)) return cudaErrorInvalidValue;
     if (!make_map(&mb, Gt, (uint64_t)2 * kN * npad, (uint32_t)(npad * P.spi))) return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
-    e = cudaFuncSetAttribute(tp_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_max_smem(tp_tc_kernel);
     if (e) return e;
     const int items = (2 * kN / P.spi) * P.n_mg;
     tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), 256, smem, s>>>(ma, mb, P);

@@ -92,13 +92,47 @@ _L.ipir_b200_matvec.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, 
 _L.ipir_b200_matvec_noalloc.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t,
                                         C.c_void_p, C.c_void_p]
 
+
+class IpirSchedule(C.Structure):
+    _fields_ = [("matvec_tc", C.c_int), ("tp_pass", C.c_int), ("horner_cluster", C.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class IpirServeConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_size_t), ("lanes_per_db", C.c_size_t), ("queue_slots", C.c_size_t),
+                ("hbm_budget_bytes", C.c_size_t), ("disable_graphs", C.c_int), ("disable_autotune", C.c_int)]
+
+
+class IpirServeCounters(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("batches", C.c_uint64), ("batched_queries", C.c_uint64), ("max_batch_seen", C.c_uint64),
+                ("queued", C.c_size_t), ("free_slots", C.c_size_t)]
+
+
+_L.ipir_b200_autotune.argtypes = [C.c_void_p]
+_L.ipir_b200_get_schedule.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirSchedule)]
+_L.ipir_b200_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
+_L.ipir_serve_create.restype = C.c_void_p
+_L.ipir_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, C.POINTER(IpirServeConfig)]
+_L.ipir_serve_submit.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirQueryView), C.POINTER(C.c_uint64)]
+_L.ipir_serve_poll.argtypes = [C.c_void_p, C.c_uint64, u64p, C.POINTER(C.c_double)]
+_L.ipir_serve_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_double, u64p, C.POINTER(C.c_double)]
+_L.ipir_serve_stats.argtypes = [C.c_void_p, C.POINTER(IpirServeCounters)]
+_L.ipir_serve_db_info.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                  C.POINTER(IpirSchedule), C.c_size_t]
+_L.ipir_serve_destroy.argtypes = [C.c_void_p]
+
 EXPORTED = [
     "ipir_server_create", "ipir_server_caps", "ipir_answer_batch", "ipir_server_destroy",
     "ipir_b200_last_error", "ipir_b200_setup", "ipir_b200_set_stream", "ipir_b200_stage_queries",
     "ipir_b200_run", "ipir_b200_fetch_responses", "ipir_b200_sync", "ipir_b200_enable_stage_timing",
     "ipir_b200_stage_times", "ipir_b200_export_precomp", "ipir_b200_export_db", "ipir_b200_ntt",
     "ipir_b200_decomp", "ipir_b200_shake256", "ipir_b200_expand_seed", "ipir_b200_fill_db",
-    "ipir_b200_matvec", "ipir_b200_matvec_noalloc",
+    "ipir_b200_matvec", "ipir_b200_matvec_noalloc", "ipir_b200_autotune", "ipir_b200_get_schedule",
+    "ipir_b200_launch_count", "ipir_serve_create", "ipir_serve_submit", "ipir_serve_poll", "ipir_serve_wait",
+    "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_destroy",
 ]
 
 
@@ -278,9 +312,107 @@ class Server:
             raise InspireError(f"export_db rc={rc}: {last_error()}")
         return out
 
+    # schedules ---------------------------------------------------------
+    def autotune(self):
+        """Time the candidate kernel schedules per batch size; later calls use the fastest."""
+        self._check()
+        if _L.ipir_b200_autotune(self._h):
+            raise InspireError(f"autotune: {last_error()}")
+
+    def schedule(self, count):
+        self._check()
+        s = IpirSchedule()
+        rc = _L.ipir_b200_get_schedule(self._h, count, C.byref(s))
+        if rc:
+            raise InspireError(f"get_schedule rc={rc}")
+        return s.as_dict()
+
+    def launch_count(self):
+        """Kernels launched by this handle's answer pipeline so far."""
+        v = C.c_ulonglong()
+        _L.ipir_b200_launch_count(self._h, C.byref(v))
+        return v.value
+
     def close(self):
         if self._h:
             _L.ipir_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ serving loop
+SERVE_DONE, SERVE_PENDING, SERVE_UNKNOWN, SERVE_FAILED, SERVE_TIMEOUT, SERVE_FULL = 0, 1, 2, 4, 5, 6
+
+
+class ServeLoop:
+    """Continuous-batching serving loop over resident databases (the
+    ipir_serve_* entry points): submit() returns a ticket at once; poll() /
+    wait() collect the response and its submit-to-response latency."""
+
+    def __init__(self, servers, max_batch=0, lanes_per_db=0, queue_slots=0, hbm_budget_bytes=0,
+                 graphs=True, autotune=True):
+        self.servers = list(servers)
+        hs = (C.c_void_p * len(self.servers))(*[s._h for s in self.servers])
+        cfg = IpirServeConfig(max_batch, lanes_per_db, queue_slots, hbm_budget_bytes,
+                              0 if graphs else 1, 0 if autotune else 1)
+        h = _L.ipir_serve_create(hs, len(self.servers), C.byref(cfg))
+        if not h:
+            raise InspireError(f"ipir_serve_create failed: {last_error()}")
+        self._h = h
+
+    def submit_view(self, db, view):
+        """Returns (rc, ticket); rc 6 means every request slot is in use."""
+        t = C.c_uint64()
+        rc = _L.ipir_serve_submit(self._h, db, C.byref(view), C.byref(t))
+        return rc, t.value
+
+    def submit(self, db, flat_query):
+        v = query_view_from_flat(self.servers[db].params, flat_query)
+        rc, t = self.submit_view(db, v)
+        if rc:
+            raise InspireError(f"submit rc={rc}: {last_error() if rc == 4 else ''}")
+        return t
+
+    def poll(self, ticket, out=None):
+        """(rc, latency_ms); rc SERVE_DONE writes the response into out (if given)."""
+        lat = C.c_double()
+        rc = _L.ipir_serve_poll(self._h, ticket, _ptr(out, u64p) if out is not None else None, C.byref(lat))
+        return rc, lat.value
+
+    def wait(self, ticket, out=None, timeout=60.0):
+        lat = C.c_double()
+        rc = _L.ipir_serve_wait(self._h, ticket, timeout, _ptr(out, u64p) if out is not None else None,
+                                C.byref(lat))
+        if rc:
+            raise InspireError(f"wait rc={rc}: {last_error() if rc == 4 else ''}")
+        return lat.value
+
+    def stats(self):
+        c = IpirServeCounters()
+        _L.ipir_serve_stats(self._h, C.byref(c))
+        return {f: getattr(c, f) for f, _ in c._fields_}
+
+    def db_info(self, db):
+        lanes, mb = C.c_size_t(), C.c_size_t()
+        tab = (IpirSchedule * 65)()
+        _L.ipir_serve_db_info(self._h, db, C.byref(lanes), C.byref(mb), tab, 65)
+        return {"lanes": lanes.value, "max_batch": mb.value,
+                "schedule": {c: tab[c].as_dict() for c in range(1, min(64, mb.value) + 1)}}
+
+    def close(self):
+        if self._h:
+            _L.ipir_serve_destroy(self._h)
             self._h = None
 
     def __enter__(self):

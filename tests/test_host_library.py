@@ -84,3 +84,23 @@ def test_server_create_rejects_bad_args_without_gpu_work():
     import inspire_b200 as ib
     with pytest.raises(ib.InspireError):
         ib.Server(1 << 25, 32, np.zeros(16, np.uint16))   # geometry rejected before any device call
+
+
+def test_serve_entry_points_reject_null_without_gpu_work():
+    import ctypes as C
+    import inspire_b200 as ib
+    L = ib.library_handle()
+    assert not L.ipir_serve_create(None, 0, None)
+    assert "no databases" in ib.last_error()
+    t = C.c_uint64()
+    assert L.ipir_serve_submit(None, 0, None, C.byref(t)) == 1
+    assert L.ipir_serve_poll(None, 1, None, None) == 1
+    assert L.ipir_serve_wait(None, 1, 0.0, None, None) == 1
+    assert L.ipir_serve_stats(None, None) == 1
+    assert L.ipir_serve_db_info(None, 0, None, None, None, 0) == 1
+    L.ipir_serve_destroy(None)
+    s = ib.IpirSchedule()
+    assert L.ipir_b200_get_schedule(None, 1, C.byref(s)) == 1
+    assert L.ipir_b200_autotune(None) == 1
+    v = C.c_ulonglong()
+    assert L.ipir_b200_launch_count(None, C.byref(v)) == 1
