@@ -465,7 +465,8 @@ def run_serve(args):
         s0 = loop.stats()
         tickets = []          # (ticket, db, pool index)
         lock = threading.Lock()
-        done = {"lat": [], "bad": 0, "n": 0, "failed": 0}
+        done = {"lat": [], "queue": [], "slow": [], "bad": 0, "n": 0, "failed": 0}
+        t_start = time.perf_counter()
         finished = threading.Event()
 
         def collector():
@@ -482,12 +483,15 @@ def run_serve(args):
                         continue
                     time.sleep(0.0002)
                     continue
-                t, k, qi = item
-                lat = C_wait(loop, t, outs[k])
-                if lat is None:
+                t, k, qi, t_arr = item
+                lq = C_wait(loop, t, outs[k])
+                if lq is None:
                     done["failed"] += 1
                 else:
-                    done["lat"].append(lat)
+                    done["lat"].append(lq[0])
+                    done["queue"].append(lq[1])
+                    if lq[0] > 10.0:
+                        done["slow"].append((round(t_arr - t_start, 3), round(lq[0], 2), round(lq[1], 2), k))
                     if not np.array_equal(outs[k], alone[k][qi]):
                         done["bad"] += 1
                 done["n"] += 1
@@ -495,9 +499,9 @@ def run_serve(args):
 
         th = threading.Thread(target=collector)
         th.start()
-        t_start = time.perf_counter()
         t_next = t_start
         full = 0
+        late = 0.0
         while True:
             t_next += rng.expovariate(rate)
             if t_next - t_start > args.serve_seconds:
@@ -516,8 +520,9 @@ def run_serve(args):
                 full += 1
                 time.sleep(0.0005)
             assert rc == 0, (rc, ib.last_error())
+            late = max(late, time.perf_counter() - t_next)
             with lock:
-                tickets.append((t, k, qi))
+                tickets.append((t, k, qi, t_next))
         finished.set()
         th.join()
         wall = time.perf_counter() - t_start
@@ -527,12 +532,27 @@ def run_serve(args):
         def pct(p):
             return lat[min(len(lat) - 1, int(round(p * (len(lat) - 1))))] if lat else None
 
+        qs = sorted(done["queue"])
+
+        def qpct(p):
+            return qs[min(len(qs) - 1, int(round(p * (len(qs) - 1))))] if qs else None
+
+        tr = [r for r in loop.trace() if r["t_issue_s"] >= t_start]
+        slow_batches = sorted(([round(r["t_issue_s"] - t_start, 3), round(r["issue_ms"], 2), round(r["device_ms"], 2),
+                                round(r["notice_ms"], 3), r["db"], r["lane"], r["count"]]
+                               for r in tr if r["device_ms"] > 5.0 or r["issue_ms"] > 2.0), key=lambda x: x[0])
+        dev = sorted(r["device_ms"] for r in tr)
         nb = s1["batches"] - s0["batches"]
         results.append({"offered_q_per_s": rate, "sustained_q_per_s": done["n"] / wall,
                         "requests": done["n"], "p50_ms": pct(0.50), "p95_ms": pct(0.95), "p99_ms": pct(0.99),
                         "max_ms": lat[-1] if lat else None, "mismatches": done["bad"], "failed": done["failed"],
                         "batches": nb, "mean_batch": (s1["batched_queries"] - s0["batched_queries"]) / max(1, nb),
-                        "queue_full_retries": full})
+                        "queue_full_retries": full, "queue_p50_ms": qpct(0.5), "queue_p99_ms": qpct(0.99),
+                        "slow_over_10ms": done["slow"][:20], "max_notice_ms": s1["max_notice_ms"],
+                        "batch_device_ms_p50": dev[len(dev) // 2] if dev else None,
+                        "batch_device_ms_max": dev[-1] if dev else None,
+                        "slow_batches_t_issue_dev_notice_db_lane_n": slow_batches[:20],
+                        "generator_max_late_ms": late * 1e3})
     infos = [loop.db_info(k) for k in range(len(dbs))]
     loop.close()
     for s in servers:
@@ -551,7 +571,7 @@ def run_serve(args):
 def C_wait(loop, ticket, out):
     import inspire_b200 as ib
     try:
-        return loop.wait(ticket, out=out, timeout=120.0)
+        return loop.wait(ticket, out=out, timeout=120.0, with_queue=True)
     except ib.InspireError:
         return None
 

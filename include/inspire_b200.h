@@ -238,8 +238,9 @@ typedef struct {
     uint64_t batches;
     uint64_t batched_queries;
     uint64_t max_batch_seen;
-    size_t queued;     /* admitted to no lane yet */
-    size_t free_slots; /* request slots free */
+    size_t queued;        /* admitted to no lane yet */
+    size_t free_slots;    /* request slots free */
+    double max_notice_ms; /* bound on the longest wait from a batch's end to the worker handling it */
 } ipir_serve_counters;
 
 /* NULL on error (text in ipir_b200_last_error).  cfg may be NULL. */
@@ -249,17 +250,32 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
  * request slot is in use (collect tickets, then retry). */
 int ipir_serve_submit(ipir_serve* sv, size_t db, const ipir_query_view* query, uint64_t* ticket);
 /* Collect a ticket: 0 done (num_cts*4*ring_n u64 written to out_resp if not
- * NULL, *latency_ms = submit to response on the host), 1 still pending,
- * 2 unknown or already collected ticket, 4 failed.  Every ticket must be
- * collected once: that frees its request slot. */
-int ipir_serve_poll(ipir_serve* sv, uint64_t ticket, uint64_t* out_resp, double* latency_ms);
+ * NULL; *latency_ms = submit to response on the host, *queue_ms = submit to
+ * the batch launch; either pointer may be NULL), 1 still pending, 2 unknown
+ * or already collected ticket, 4 failed.  Every ticket must be collected
+ * once: that frees its request slot. */
+int ipir_serve_poll(ipir_serve* sv, uint64_t ticket, uint64_t* out_resp, double* latency_ms, double* queue_ms);
 /* Same, blocking up to timeout_s; 5 when it is still pending then. */
-int ipir_serve_wait(ipir_serve* sv, uint64_t ticket, double timeout_s, uint64_t* out_resp, double* latency_ms);
+int ipir_serve_wait(ipir_serve* sv, uint64_t ticket, double timeout_s, uint64_t* out_resp, double* latency_ms,
+                    double* queue_ms);
 int ipir_serve_stats(ipir_serve* sv, ipir_serve_counters* out);
 /* Lanes, batch limit and schedule table (entries 1..min(sched_len-1,
  * max_batch) of sched) the loop chose for database db. */
 int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_batch, ipir_serve_schedule* sched,
                        size_t sched_len);
+/* One lane batch, for tracing. */
+typedef struct {
+    double t_issue_s;  /* steady (CLOCK_MONOTONIC) seconds when the batch was issued */
+    float issue_ms;    /* host time to enqueue copies + graph replay */
+    float device_ms;   /* device time of the batch, copies included (CUDA events) */
+    float notice_ms;   /* bound on the delay from the batch's end to the worker handling it */
+    uint16_t db, lane;
+    uint32_t count;    /* queries in the batch */
+    uint32_t failed;
+} ipir_serve_batch_record;
+/* Copies the most recent batches (up to max_records of the last 4096, oldest
+ * first) into out; returns how many. */
+size_t ipir_serve_trace(ipir_serve* sv, ipir_serve_batch_record* out, size_t max_records);
 /* Waits for the batches on the device, fails requests not yet admitted,
  * frees everything. */
 void ipir_serve_destroy(ipir_serve* sv);

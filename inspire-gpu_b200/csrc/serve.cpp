@@ -12,8 +12,10 @@
 // lanes of one database and of different databases overlap on the device.
 // A lane batch is: one H2D copy per query, one replay of the CUDA graph
 // captured for that batch size, one D2H copy per response straight into its
-// request slot, the error word, and a host function that tells the worker.
-// Everything is allocated at create; the request path allocates nothing.
+// request slot, the error word, and an event the worker polls (a host
+// function per batch was tried first: on B200 with driver 580 its callbacks
+// stalled for ~40 ms every ~2 s on an otherwise idle GPU).  Everything is
+// allocated at create; the request path allocates nothing.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,7 +46,7 @@ struct ReqSlot {
     size_t db = 0;
     uint64_t* q = nullptr;     // pinned flat query (the database's qstride words)
     uint64_t* resp = nullptr;  // pinned response
-    Clock::time_point t_submit, t_done;
+    Clock::time_point t_submit, t_issue, t_done;
 };
 
 struct Engine;
@@ -56,7 +58,9 @@ struct LaneRun {
     bool busy = false;
     std::vector<uint32_t> slots;
     int* h_err = nullptr;  // pinned device-error word of the last batch
-    std::atomic<int> done{0};
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+    int64_t t_issue0 = 0, t_issue1 = 0;  // steady-clock ns around the last issue()
+    uint16_t db_index = 0, lane_index = 0;
     Engine* eng = nullptr;
 };
 
@@ -86,6 +90,9 @@ struct Engine {
     std::string fail_text;
     uint64_t next_seq = 1;
     uint64_t submitted = 0, completed = 0, n_failed = 0, batches = 0, batched = 0, max_seen = 0;
+    double max_notice_ms = 0;  // batch end on the device -> completion handled by the worker (bound)
+    std::vector<ipir_serve_batch_record> trace;  // ring of the last batches
+    uint64_t trace_n = 0;
 
     ~Engine();
     void run();
@@ -94,18 +101,12 @@ struct Engine {
     void fail_all_locked(const std::string& why);
 };
 
-void CUDART_CB on_lane_done(void* p) {
-    // Runs on a CUDA callback thread: no CUDA calls, no engine lock.
-    auto* r = static_cast<LaneRun*>(p);
-    r->done.store(1, std::memory_order_release);
-    r->eng->cv_work.notify_one();
-}
-
 void Engine::issue(DbState& d, LaneRun& r) {
     const Server& S = *d.S;
     Lane& L = r.lane;
     const size_t n = r.slots.size();
     IPB_CK(cudaSetDevice(S.device));
+    IPB_CK(cudaEventRecord(r.ev_start, r.st));
     for (size_t i = 0; i < n; ++i) stage_query_flat(S, L, i, slots[r.slots[i]].q, r.st);
     if (use_graphs)
         IPB_CK(cudaGraphLaunch(r.graphs[n], r.st));
@@ -117,13 +118,30 @@ void Engine::issue(DbState& d, LaneRun& r) {
                                r.st));
     IPB_CK(cudaMemcpyAsync(r.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost, r.st));
     IPB_CK(cudaMemsetAsync(L.d_err, 0, sizeof(int), r.st));
-    IPB_CK(cudaLaunchHostFunc(r.st, on_lane_done, &r));
+    IPB_CK(cudaEventRecord(r.ev_end, r.st));
 }
 
-// Called with the lock held, after the lane's host function ran.
+// Called with the lock held, once the lane's end event completed.
 void Engine::finish(DbState& d, LaneRun& r) {
     const int err = *r.h_err;
     const auto now = Clock::now();
+    float dev_ms = 0.f;
+    if (cudaEventElapsedTime(&dev_ms, r.ev_start, r.ev_end) != cudaSuccess) dev_ms = -1.f;
+    // Upper bound on the delay between the batch's end and this call: wall
+    // time since the enqueue began, less the device time.
+    const double notice = std::max(0.0, (now.time_since_epoch().count() - r.t_issue0) * 1e-6 - dev_ms);
+    max_notice_ms = std::max(max_notice_ms, notice);
+    if (!trace.empty()) {
+        ipir_serve_batch_record& t = trace[trace_n++ % trace.size()];
+        t.t_issue_s = r.t_issue0 * 1e-9;
+        t.issue_ms = (float)((r.t_issue1 - r.t_issue0) * 1e-6);
+        t.device_ms = dev_ms;
+        t.notice_ms = (float)notice;
+        t.db = r.db_index;
+        t.lane = r.lane_index;
+        t.count = (uint32_t)r.slots.size();
+        t.failed = err != 0;
+    }
     for (uint32_t s : r.slots) {
         slots[s].state = err ? kFailed : kDone;
         slots[s].t_done = now;
@@ -141,7 +159,6 @@ void Engine::finish(DbState& d, LaneRun& r) {
     max_seen = std::max<uint64_t>(max_seen, r.slots.size());
     r.slots.clear();
     r.busy = false;
-    r.done.store(0, std::memory_order_relaxed);
     cv_done.notify_all();
 }
 
@@ -160,14 +177,24 @@ void Engine::run() {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         bool any_busy = false;
+        std::string poll_err;
         for (auto& dp : dbs)
             for (auto& r : dp->lanes)
                 if (r->busy) {
-                    if (r->done.load(std::memory_order_acquire))
+                    const cudaError_t q = cudaEventQuery(r->ev_end);
+                    if (q == cudaSuccess) {
                         finish(*dp, *r);
-                    else
+                    } else if (q == cudaErrorNotReady) {
                         any_busy = true;
+                    } else {
+                        for (uint32_t s : r->slots) slots[s].state = kFailed;
+                        n_failed += r->slots.size();
+                        r->slots.clear();
+                        r->busy = false;
+                        poll_err = std::string("CUDA error while waiting for a batch: ") + cudaGetErrorString(q);
+                    }
                 }
+        if (!poll_err.empty()) fail_all_locked(poll_err);
         if (stop && !any_busy) break;
         if (!stop && !failed) {
             for (auto& dp : dbs) {
@@ -176,21 +203,25 @@ void Engine::run() {
                     if (d.pending.empty()) break;
                     if (r->busy) continue;
                     const size_t n = std::min(d.max_batch, d.pending.size());
+                    const auto t_issue = Clock::now();
                     for (size_t i = 0; i < n; ++i) {
                         const uint32_t s = d.pending.front();
                         d.pending.pop_front();
                         slots[s].state = kRunning;
+                        slots[s].t_issue = t_issue;
                         r->slots.push_back(s);
                     }
                     r->busy = true;
                     any_busy = true;
                     lk.unlock();
                     std::string err;
+                    r->t_issue0 = Clock::now().time_since_epoch().count();
                     try {
                         issue(d, *r);
                     } catch (const std::exception& e) {
                         err = e.what();
                     }
+                    r->t_issue1 = Clock::now().time_since_epoch().count();
                     lk.lock();
                     if (!err.empty()) {
                         // The lane's stream may hold part of the batch: wait for
@@ -216,7 +247,7 @@ void Engine::run() {
             cv_done.notify_all();
         }
         if (any_busy) {
-            cv_work.wait_for(lk, std::chrono::microseconds(50));
+            cv_work.wait_for(lk, std::chrono::microseconds(20));
         } else {
             bool work = false;
             for (auto& d : dbs) work |= !d->pending.empty();
@@ -231,6 +262,8 @@ Engine::~Engine() {
         cudaSetDevice(d.S->device);
         for (auto& r : d.lanes) {
             if (r->st) cudaStreamSynchronize(r->st);
+            if (r->ev_start) cudaEventDestroy(r->ev_start);
+            if (r->ev_end) cudaEventDestroy(r->ev_end);
             for (auto g : r->graphs)
                 if (g) cudaGraphExecDestroy(g);
             if (r->st) cudaStreamDestroy(r->st);
@@ -341,8 +374,12 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                 for (size_t k = 0; k < lanes; ++k) {
                     auto r = std::make_unique<ipb::LaneRun>();
                     r->eng = E.get();
+                    r->db_index = (uint16_t)(&dp - &E->dbs[0]);
+                    r->lane_index = (uint16_t)k;
                     IPB_CK(cudaSetDevice(d.S->device));
                     IPB_CK(cudaStreamCreateWithFlags(&r->st, cudaStreamNonBlocking));
+                    IPB_CK(cudaEventCreate(&r->ev_start));
+                    IPB_CK(cudaEventCreate(&r->ev_end));
                     ipb::alloc_lane(*d.S, r->lane, mb, ipb::lane_gt_pass(*d.S, mb));
                     d.lanes.push_back(std::move(r));
                 }
@@ -365,6 +402,7 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                     r->h_err = E->pinned_err + li++;
                     *r->h_err = 0;
                 }
+            E->trace.resize(4096);
             E->slots.resize(Q);
             for (size_t s = 0; s < Q; ++s) {
                 E->slots[s].q = E->pinned_q + s * q_words;
@@ -431,7 +469,8 @@ int ipir_serve_submit(ipir_serve* sv, size_t db, const ipir_query_view* q, uint6
 
 namespace {
 // Collects a finished slot: 0 done, 1 pending, 2 unknown ticket, 4 failed.
-int collect(ipb::Engine& E, std::unique_lock<std::mutex>& lk, uint64_t ticket, uint64_t* out, double* lat) {
+int collect(ipb::Engine& E, std::unique_lock<std::mutex>& lk, uint64_t ticket, uint64_t* out, double* lat,
+            double* queue) {
     const size_t s = (size_t)(ticket % E.slots.size());
     ipb::ReqSlot& r = E.slots[s];
     if (r.ticket != ticket || r.state == ipb::kFree || r.state == ipb::kCollecting) return 2;
@@ -443,6 +482,7 @@ int collect(ipb::Engine& E, std::unique_lock<std::mutex>& lk, uint64_t ticket, u
     }
     if (r.state != ipb::kDone) return 1;
     if (lat) *lat = std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
+    if (queue) *queue = std::chrono::duration<double, std::milli>(r.t_issue - r.t_submit).count();
     r.state = ipb::kCollecting;
     const size_t words = E.dbs[r.db]->S->resp_qstride;
     lk.unlock();
@@ -454,23 +494,24 @@ int collect(ipb::Engine& E, std::unique_lock<std::mutex>& lk, uint64_t ticket, u
 }
 }  // namespace
 
-int ipir_serve_poll(ipir_serve* sv, uint64_t ticket, uint64_t* out_resp, double* latency_ms) {
+int ipir_serve_poll(ipir_serve* sv, uint64_t ticket, uint64_t* out_resp, double* latency_ms, double* queue_ms) {
     if (!sv) return 1;
     std::unique_lock<std::mutex> lk(sv->e->mu);
-    return collect(*sv->e, lk, ticket, out_resp, latency_ms);
+    return collect(*sv->e, lk, ticket, out_resp, latency_ms, queue_ms);
 }
 
-int ipir_serve_wait(ipir_serve* sv, uint64_t ticket, double timeout_s, uint64_t* out_resp, double* latency_ms) {
+int ipir_serve_wait(ipir_serve* sv, uint64_t ticket, double timeout_s, uint64_t* out_resp, double* latency_ms,
+                    double* queue_ms) {
     if (!sv) return 1;
     ipb::Engine& E = *sv->e;
     const auto deadline = ipb::Clock::now() + std::chrono::duration_cast<ipb::Clock::duration>(
                                                   std::chrono::duration<double>(std::max(0.0, timeout_s)));
     std::unique_lock<std::mutex> lk(E.mu);
     for (;;) {
-        const int rc = collect(E, lk, ticket, out_resp, latency_ms);
+        const int rc = collect(E, lk, ticket, out_resp, latency_ms, queue_ms);
         if (rc != 1) return rc;
         if (E.cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
-            const int rc2 = collect(E, lk, ticket, out_resp, latency_ms);
+            const int rc2 = collect(E, lk, ticket, out_resp, latency_ms, queue_ms);
             return rc2 == 1 ? 5 : rc2;
         }
     }
@@ -490,6 +531,7 @@ int ipir_serve_stats(ipir_serve* sv, ipir_serve_counters* out) {
     for (auto& d : E.dbs) q += d->pending.size();
     out->queued = q;
     out->free_slots = E.free_slots.size();
+    out->max_notice_ms = E.max_notice_ms;
     return 0;
 }
 
@@ -508,6 +550,17 @@ int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_bat
             sched[c].horner_cluster = d.sched[c].horner_cluster;
         }
     return 0;
+}
+
+size_t ipir_serve_trace(ipir_serve* sv, ipir_serve_batch_record* out, size_t max_records) {
+    if (!sv || !out) return 0;
+    ipb::Engine& E = *sv->e;
+    std::lock_guard<std::mutex> lk(E.mu);
+    const size_t cap = E.trace.size();
+    const size_t avail = (size_t)std::min<uint64_t>(E.trace_n, cap);
+    const size_t n = std::min(avail, max_records);
+    for (size_t i = 0; i < n; ++i) out[i] = E.trace[(E.trace_n - n + i) % cap];
+    return n;
 }
 
 void ipir_serve_destroy(ipir_serve* sv) {

@@ -108,7 +108,7 @@ class IpirServeConfig(C.Structure):
 class IpirServeCounters(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("batches", C.c_uint64), ("batched_queries", C.c_uint64), ("max_batch_seen", C.c_uint64),
-                ("queued", C.c_size_t), ("free_slots", C.c_size_t)]
+                ("queued", C.c_size_t), ("free_slots", C.c_size_t), ("max_notice_ms", C.c_double)]
 
 
 _L.ipir_b200_autotune.argtypes = [C.c_void_p]
@@ -117,12 +117,23 @@ _L.ipir_b200_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
 _L.ipir_serve_create.restype = C.c_void_p
 _L.ipir_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, C.POINTER(IpirServeConfig)]
 _L.ipir_serve_submit.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirQueryView), C.POINTER(C.c_uint64)]
-_L.ipir_serve_poll.argtypes = [C.c_void_p, C.c_uint64, u64p, C.POINTER(C.c_double)]
-_L.ipir_serve_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_double, u64p, C.POINTER(C.c_double)]
+_L.ipir_serve_poll.argtypes = [C.c_void_p, C.c_uint64, u64p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+_L.ipir_serve_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_double, u64p, C.POINTER(C.c_double),
+                               C.POINTER(C.c_double)]
 _L.ipir_serve_stats.argtypes = [C.c_void_p, C.POINTER(IpirServeCounters)]
 _L.ipir_serve_db_info.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                   C.POINTER(IpirSchedule), C.c_size_t]
 _L.ipir_serve_destroy.argtypes = [C.c_void_p]
+
+
+class IpirServeBatchRecord(C.Structure):
+    _fields_ = [("t_issue_s", C.c_double), ("issue_ms", C.c_float), ("device_ms", C.c_float),
+                ("notice_ms", C.c_float), ("db", C.c_uint16), ("lane", C.c_uint16), ("count", C.c_uint32),
+                ("failed", C.c_uint32)]
+
+
+_L.ipir_serve_trace.restype = C.c_size_t
+_L.ipir_serve_trace.argtypes = [C.c_void_p, C.POINTER(IpirServeBatchRecord), C.c_size_t]
 
 EXPORTED = [
     "ipir_server_create", "ipir_server_caps", "ipir_answer_batch", "ipir_server_destroy",
@@ -132,7 +143,7 @@ EXPORTED = [
     "ipir_b200_decomp", "ipir_b200_shake256", "ipir_b200_expand_seed", "ipir_b200_fill_db",
     "ipir_b200_matvec", "ipir_b200_matvec_noalloc", "ipir_b200_autotune", "ipir_b200_get_schedule",
     "ipir_b200_launch_count", "ipir_serve_create", "ipir_serve_submit", "ipir_serve_poll", "ipir_serve_wait",
-    "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_destroy",
+    "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy",
 ]
 
 
@@ -387,21 +398,28 @@ class ServeLoop:
     def poll(self, ticket, out=None):
         """(rc, latency_ms); rc SERVE_DONE writes the response into out (if given)."""
         lat = C.c_double()
-        rc = _L.ipir_serve_poll(self._h, ticket, _ptr(out, u64p) if out is not None else None, C.byref(lat))
+        rc = _L.ipir_serve_poll(self._h, ticket, _ptr(out, u64p) if out is not None else None, C.byref(lat), None)
         return rc, lat.value
 
-    def wait(self, ticket, out=None, timeout=60.0):
-        lat = C.c_double()
+    def wait(self, ticket, out=None, timeout=60.0, with_queue=False):
+        """Latency in ms (submit to response); with_queue: (latency, submit-to-launch)."""
+        lat, qms = C.c_double(), C.c_double()
         rc = _L.ipir_serve_wait(self._h, ticket, timeout, _ptr(out, u64p) if out is not None else None,
-                                C.byref(lat))
+                                C.byref(lat), C.byref(qms))
         if rc:
             raise InspireError(f"wait rc={rc}: {last_error() if rc == 4 else ''}")
-        return lat.value
+        return (lat.value, qms.value) if with_queue else lat.value
 
     def stats(self):
         c = IpirServeCounters()
         _L.ipir_serve_stats(self._h, C.byref(c))
         return {f: getattr(c, f) for f, _ in c._fields_}
+
+    def trace(self, max_records=4096):
+        """The most recent lane batches, oldest first (dicts of ipir_serve_batch_record)."""
+        buf = (IpirServeBatchRecord * max_records)()
+        n = _L.ipir_serve_trace(self._h, buf, max_records)
+        return [{f: getattr(buf[i], f) for f, _ in IpirServeBatchRecord._fields_} for i in range(n)]
 
     def db_info(self, db):
         lanes, mb = C.c_size_t(), C.c_size_t()

@@ -94,8 +94,8 @@ def test_serve_entry_points_reject_null_without_gpu_work():
     assert "no databases" in ib.last_error()
     t = C.c_uint64()
     assert L.ipir_serve_submit(None, 0, None, C.byref(t)) == 1
-    assert L.ipir_serve_poll(None, 1, None, None) == 1
-    assert L.ipir_serve_wait(None, 1, 0.0, None, None) == 1
+    assert L.ipir_serve_poll(None, 1, None, None, None) == 1
+    assert L.ipir_serve_wait(None, 1, 0.0, None, None, None) == 1
     assert L.ipir_serve_stats(None, None) == 1
     assert L.ipir_serve_db_info(None, 0, None, None, None, 0) == 1
     L.ipir_serve_destroy(None)
