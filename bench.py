@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--serve-config", default="mixed", choices=["mixed", "16gb"])
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-rates", default="")
+    ap.add_argument("--serve-lanes", type=int, default=2)
+    ap.add_argument("--serve-max-batch", type=int, default=64)
+    ap.add_argument("--serve-overlap", action="store_true",
+                    help="admit batches while the previous DB pass of their database still runs")
     return ap.parse_args()
 
 
@@ -455,7 +459,8 @@ def run_serve(args):
     if args.serve_rates:
         rates = [float(x) for x in args.serve_rates.split(",")]
     t0 = time.perf_counter()
-    loop = ib.ServeLoop(servers, max_batch=64, lanes_per_db=2, queue_slots=512)
+    loop = ib.ServeLoop(servers, max_batch=args.serve_max_batch, lanes_per_db=args.serve_lanes, queue_slots=512,
+                        overlap_db_passes=args.serve_overlap)
     t_create = time.perf_counter() - t0
     views = [[ib.query_view_from_flat(servers[k].params, pools[k][i]) for i in range(pool_n)]
              for k in range(len(dbs))]
@@ -560,7 +565,8 @@ def run_serve(args):
     line = {"metric": "serving loop: p50/p95/p99 latency and sustained q/s under open-loop Poisson arrivals",
             "mode": "serve", "config": {"workload": args.serve_config, "databases": [p["workload"] for p in plain],
                                         "split": split, "seconds_per_rate": args.serve_seconds,
-                                        "max_batch": 64, "lanes_per_db": 2},
+                                        "max_batch": args.serve_max_batch, "lanes_per_db": args.serve_lanes,
+                                        "overlap_db_passes": args.serve_overlap},
             "n_gpus": 1, "unit": "ms", "data": "synthetic queries (pool of 32 per database)",
             "plain": plain, "rates": results, "create_s": t_create,
             "lanes": [{"lanes": i["lanes"], "max_batch": i["max_batch"]} for i in infos],

@@ -206,11 +206,12 @@ int ipir_b200_launch_count(const ipir_server* srv, unsigned long long* out);
  * ipir_serve_submit copies one query for one database into a pinned request
  * slot and returns a ticket at once.  A worker thread admits waiting
  * requests, oldest first and up to max_batch at a time, into any free lane
- * of their database (per-batch device buffers with their own stream): a
- * request that arrives while a batch runs joins the next batch as soon as a
- * lane is free, and lanes of one database and of different databases run
- * concurrently.  A lane batch replays the CUDA graph captured for its batch
- * size at create.  All device and pinned memory is allocated at create,
+ * of their database (per-batch device buffers with their own stream).  A
+ * database's next batch starts as soon as its previous batch has finished
+ * streaming the database and precomputed tensors, overlapping that batch's
+ * Horner chains; requests that arrive meanwhile join it.  Lanes of
+ * different databases run concurrently.  A lane batch replays the CUDA
+ * graphs captured for its batch size at create.  All device and pinned memory is allocated at create,
  * with lanes sized to the HBM budget; submit, poll and wait allocate
  * nothing.  Each response is bit-identical to ipir_answer_batch on the same
  * query, whatever else shares its batch.
@@ -229,6 +230,9 @@ typedef struct {
                                 over budget, max_batch halves, then lanes_per_db drops */
     int disable_graphs;      /* 1: launch the kernels directly instead of graph replays */
     int disable_autotune;    /* 1: default schedule instead of timing candidates at create */
+    int overlap_db_passes;   /* 1: admit a batch on any free lane at once, even while the previous
+                                batch of its database still streams the DB (default 0: wait for
+                                that pass to end, overlapping only its Horner chains) */
 } ipir_serve_config;
 
 typedef struct {

@@ -32,9 +32,11 @@ size_t mv_tc_planes_bytes(size_t rows, int max_queries);
 int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms);
 cudaError_t launch_qplanes(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
                            uint8_t* planes, int nq, cudaStream_t s);
+// tiles: a device counter the launch zeroes and the kernel's CTAs draw work
+// items from (one per concurrently running launch).
 cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const uint8_t* planes, int nq,
-                             const DevTables* T, uint32_t* part, size_t part_qstride, int* err, int num_sms,
-                             int kchunk_rows, cudaStream_t s);
+                             const DevTables* T, uint32_t* part, size_t part_qstride, int* err, unsigned* tiles,
+                             int num_sms, int kchunk_rows, cudaStream_t s);
 
 // out[q][limb][cols] = sum over chunks of part[q][chunk][limb][cols] mod q.
 cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, int chunks, size_t cols,
@@ -50,8 +52,8 @@ cudaError_t launch_dt_transpose(const uint32_t* dp, const uint32_t* dm, size_t g
                                 cudaStream_t s);
 cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp, uint32_t* dm, cudaStream_t s);
 cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
-                               int nq_total, int q0, uint8_t* Gt, uint32_t* tp_out, int* err, int num_sms,
-                               cudaStream_t s);
+                               int nq_total, int q0, uint8_t* Gt, uint32_t* tp_out, int* err, unsigned* tiles,
+                               int num_sms, cudaStream_t s);
 
 // packed_b[q][g][limb][N] = NTT(sum_y mvpart) - tp_out - Dfinal (.) Kn1.
 cudaError_t launch_finalize(const uint32_t* mvpart, size_t mv_qstride, int mv_chunks, size_t cols,

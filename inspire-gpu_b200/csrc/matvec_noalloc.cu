@@ -13,7 +13,8 @@
 // another allocator or pool it must not bypass, or code running where a
 // cudaMalloc would implicitly synchronise the device.  Its scratch (NTT
 // tables, the device error word, the query byte planes) lives in the
-// file-scope array below, sized for at most kNoAllocMaxRows DB rows and
+// file-scope array below (NTT tables, error word and work-item counter, query
+// byte planes), sized for at most kNoAllocMaxRows DB rows and
 // kNoAllocMaxQueries queries per call; every GPU that loads this library
 // holds the array until the process exits.
 
@@ -82,12 +83,13 @@ extern "C" int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const DevTables* T = reinterpret_cast<const DevTables*>(base + kNoAllocTablesOff);
     int* err = reinterpret_cast<int*>(base + kNoAllocErrOff);
+    unsigned* tiles = reinterpret_cast<unsigned*>(base + kNoAllocErrOff + 128);  // same 256-byte slot
     uint8_t* planes = base + kNoAllocPlanesOff;
     e = cudaMemsetAsync(err, 0, sizeof(int), s);  // the array keeps the last call's contents
     if (e == cudaSuccess) e = launch_qplanes(queries, 2 * rows, rows, T, planes, (int)count, s);
     // rows <= 32768: one exact K-chunk, so the kernel writes the result directly.
     if (e == cudaSuccess)
-        e = launch_matvec_tc(db, rows, cols, planes, (int)count, T, out, 2 * cols, err, sms, (int)rows, s);
+        e = launch_matvec_tc(db, rows, cols, planes, (int)count, T, out, 2 * cols, err, tiles, sms, (int)rows, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     int h_err = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);

@@ -18,6 +18,13 @@
 // thread issues the MMAs, warps 4..7 drain TMEM (tcgen05.ld) and write
 // partial sums.  Stages are recycled through mbarriers; every wait is
 // bounded and reports a timeout through *err instead of hanging.
+//
+// Work items (m'-tile, K-chunk) are handed out dynamically: the producer
+// thread takes the next item from a per-launch atomic counter (zeroed by the
+// launcher) and publishes it to the MMA thread and the epilogue through a
+// ring of kRing shared slots; -1 ends the sequence.  SMs that other kernels
+// hold when this one starts (the previous batch's Horner, another lane)
+// simply take fewer items instead of delaying the whole pass.
 #include <cuda.h>
 
 #include "ipb_common.cuh"
@@ -33,6 +40,7 @@ using namespace tc;
 constexpr int kKT = 128;          // DB rows per pipeline stage (bytes of K)
 constexpr int kMT = 256;          // m' rows per tile (two M = 128 MMAs)
 constexpr int kKChunk = 32768;    // rows per exact s32 accumulation
+constexpr int kRing = 8;          // published work items in flight
 struct TcParams {
     uint32_t* part;        // [q][chunk][limb][cols]
     size_t part_qstride;
@@ -46,6 +54,7 @@ struct TcParams {
     int acc_stages;
     uint32_t tmem_cols;
     int* err;
+    unsigned* tiles;       // work-item counter, zero at launch
     const DevTables* T;
 };
 
@@ -64,12 +73,15 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
     uint64_t* tempty = bars + 2 * S + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 4);
     __shared__ volatile int abort_flag;
+    __shared__ volatile int item_ring[kRing];
+    __shared__ uint64_t ifull[kRing], iempty[kRing];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128); }
+        for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 128); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -89,7 +101,18 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
         if (lane == 0) {
             int s = 0;
             uint32_t ph = 0;
-            for (int item = blockIdx.x; item < n_items && !abort_flag; item += gridDim.x) {
+            for (int it = 0;; ++it) {
+                const int r = it % kRing;
+                int item = -1;
+                if (!abort_flag && mbar_wait(&iempty[r], ((uint32_t)(it / kRing) & 1) ^ 1, P.err, 6)) {
+                    const unsigned t = atomicAdd(P.tiles, 1u);
+                    if (t < (unsigned)n_items) item = (int)t;
+                } else {
+                    abort_flag = 1;
+                }
+                item_ring[r] = item;
+                mbar_arrive(&ifull[r]);
+                if (item < 0) break;
                 const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
                 const int m0 = mt * kMT;
                 for (int kt = 0; kt < ktiles; ++kt) {
@@ -115,7 +138,12 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
             const uint32_t idesc = idesc_i8(P.npad);
             int s = 0, as = 0;
             uint32_t ph = 0, aph = 0;
-            for (int item = blockIdx.x; item < n_items && !abort_flag; item += gridDim.x) {
+            for (int it = 0;; ++it) {
+                const int r = it % kRing;
+                if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 7)) { abort_flag = 1; break; }
+                const int item = item_ring[r];
+                mbar_arrive(&iempty[r]);
+                if (item < 0 || abort_flag) break;
                 if (!mbar_wait(&tempty[as], aph ^ 1, P.err, 3)) { abort_flag = 1; break; }
                 tc_fence_after();
                 const uint32_t d0 = tmem_base + (uint32_t)(as * 2 * P.npad);
@@ -149,7 +177,12 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
         int as = 0;
         uint32_t aph = 0;
         const uint64_t cr0 = P.T->limb[0].cr, cr1 = P.T->limb[1].cr;
-        for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        for (int it = 0;; ++it) {
+            const int r = it % kRing;
+            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 8)) { abort_flag = 1; break; }
+            const int item = item_ring[r];
+            mbar_arrive(&iempty[r]);
+            if (item < 0) break;
             if (!mbar_wait(&tfull[as], aph, P.err, 5)) { abort_flag = 1; break; }
             tc_fence_after();
             const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
@@ -273,10 +306,10 @@ int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms) {
 }
 
 cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const uint8_t* planes, int nq,
-                             const DevTables* T, uint32_t* part, size_t part_qstride, int* err, int num_sms,
-                             int kchunk_rows, cudaStream_t s) {
+                             const DevTables* T, uint32_t* part, size_t part_qstride, int* err, unsigned* tiles,
+                             int num_sms, int kchunk_rows, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    if (nq > 32 || rows % kKT || cols % 128) return cudaErrorInvalidValue;
+    if (nq > 32 || rows % kKT || cols % 128 || !tiles) return cudaErrorInvalidValue;
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
     const int npad = ((8 * nq + 15) / 16) * 16;
@@ -318,6 +351,7 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     while (tc < need) tc <<= 1;
     P.tmem_cols = tc;
     P.err = err;
+    P.tiles = tiles;
     P.T = T;
     const size_t stage_bytes = 2 * (size_t)kKT * 128 + (size_t)npad * 128;
     const size_t budget = 200 * 1024;
@@ -328,6 +362,7 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     if (e) return e;
     const int items = P.n_mtiles * P.n_kchunks;
     const int grid = std::min(items, std::max(1, num_sms));
+    if ((e = cudaMemsetAsync(tiles, 0, sizeof(unsigned), s))) return e;
     mv_tc_kernel<<<grid, 256, smem, s>>>(ma, mb, P);
     return cudaGetLastError();
 }

@@ -6,13 +6,18 @@
 // Requests enter pinned request slots (submit copies the query there and
 // returns a ticket).  One worker thread owns every device call: for each
 // database it admits waiting requests, oldest first and at most max_batch
-// at a time, into any free lane -- a set of per-batch device buffers with
-// its own stream -- so requests that arrive while a batch runs form the next
-// batch at once instead of waiting for the previous one to finish, and the
-// lanes of one database and of different databases overlap on the device.
-// A lane batch is: one H2D copy per query, one replay of the CUDA graph
-// captured for that batch size, one D2H copy per response straight into its
-// request slot, the error word, and an event the worker polls (a host
+// at a time, into a free lane -- a set of per-batch device buffers with its
+// own stream.  A batch has two phases: the DB-bound one (mat-vec and tensor
+// pass stream the whole database and the precomputed tensors) and the
+// latency-bound Horner chains.  A database's next batch is admitted as soon
+// as its previous batch has left the DB-bound phase, so the next DB pass
+// overlaps only the previous batch's Horner (two DB passes at once would
+// just share the memory bandwidth), and requests that arrive meanwhile
+// still join it.  Lanes of different databases run concurrently.
+// A lane batch is: one H2D copy per query, one replay of each phase's CUDA
+// graph captured for that batch size (an event between them), one D2H copy
+// per response straight into its request slot, the error word, and an
+// event the worker polls (a host
 // function per batch was tried first: on B200 with driver 580 its callbacks
 // stalled for ~40 ms every ~2 s on an otherwise idle GPU).  Everything is
 // allocated at create; the request path allocates nothing.
@@ -54,11 +59,11 @@ struct Engine;
 struct LaneRun {
     Lane lane;
     cudaStream_t st = nullptr;
-    std::vector<cudaGraphExec_t> graphs;  // [batch size], index 0 unused
+    std::vector<cudaGraphExec_t> graphs_db, graphs_horner;  // [batch size], index 0 unused
     bool busy = false;
     std::vector<uint32_t> slots;
     int* h_err = nullptr;  // pinned device-error word of the last batch
-    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_db = nullptr, ev_end = nullptr;
     int64_t t_issue0 = 0, t_issue1 = 0;  // steady-clock ns around the last issue()
     uint16_t db_index = 0, lane_index = 0;
     Engine* eng = nullptr;
@@ -70,6 +75,7 @@ struct DbState {
     std::vector<Sched> sched;
     std::vector<std::unique_ptr<LaneRun>> lanes;
     std::deque<uint32_t> pending;
+    int last_lane = -1;  // lane of the most recently issued batch
     uint64_t batches = 0, queries = 0;
 };
 
@@ -82,6 +88,7 @@ struct Engine {
     uint64_t* pinned_r = nullptr;
     int* pinned_err = nullptr;
     bool use_graphs = true;
+    bool overlap_db = false;  // admit without waiting for the previous DB phase
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::thread worker;
@@ -109,9 +116,14 @@ void Engine::issue(DbState& d, LaneRun& r) {
     IPB_CK(cudaEventRecord(r.ev_start, r.st));
     for (size_t i = 0; i < n; ++i) stage_query_flat(S, L, i, slots[r.slots[i]].q, r.st);
     if (use_graphs)
-        IPB_CK(cudaGraphLaunch(r.graphs[n], r.st));
+        IPB_CK(cudaGraphLaunch(r.graphs_db[n], r.st));
     else
-        run_pipeline(S, L, d.sched[n], n, r.st, nullptr);
+        run_pipeline(S, L, d.sched[n], n, r.st, nullptr, kPhaseDb);
+    IPB_CK(cudaEventRecord(r.ev_db, r.st));
+    if (use_graphs)
+        IPB_CK(cudaGraphLaunch(r.graphs_horner[n], r.st));
+    else
+        run_pipeline(S, L, d.sched[n], n, r.st, nullptr, kPhaseHorner);
     const size_t rb = S.resp_qstride * 8;
     for (size_t i = 0; i < n; ++i)
         IPB_CK(cudaMemcpyAsync(slots[r.slots[i]].resp, L.resp + i * S.resp_qstride, rb, cudaMemcpyDeviceToHost,
@@ -199,7 +211,13 @@ void Engine::run() {
         if (!stop && !failed) {
             for (auto& dp : dbs) {
                 DbState& d = *dp;
-                for (auto& r : d.lanes) {
+                if (d.pending.empty()) continue;
+                if (!overlap_db && d.last_lane >= 0 && d.lanes[d.last_lane]->busy) {
+                    const cudaError_t q = cudaEventQuery(d.lanes[d.last_lane]->ev_db);
+                    if (q == cudaErrorNotReady) continue;  // previous DB pass still running
+                }
+                for (size_t li = 0; li < d.lanes.size(); ++li) {
+                    auto& r = d.lanes[li];
                     if (d.pending.empty()) break;
                     if (r->busy) continue;
                     const size_t n = std::min(d.max_batch, d.pending.size());
@@ -213,6 +231,7 @@ void Engine::run() {
                     }
                     r->busy = true;
                     any_busy = true;
+                    d.last_lane = (int)li;
                     lk.unlock();
                     std::string err;
                     r->t_issue0 = Clock::now().time_since_epoch().count();
@@ -235,6 +254,7 @@ void Engine::run() {
                         r->busy = false;
                         fail_all_locked(err);
                     }
+                    if (!overlap_db) break;  // one DB pass at a time per database
                 }
             }
         }
@@ -263,8 +283,11 @@ Engine::~Engine() {
         for (auto& r : d.lanes) {
             if (r->st) cudaStreamSynchronize(r->st);
             if (r->ev_start) cudaEventDestroy(r->ev_start);
+            if (r->ev_db) cudaEventDestroy(r->ev_db);
             if (r->ev_end) cudaEventDestroy(r->ev_end);
-            for (auto g : r->graphs)
+            for (auto g : r->graphs_db)
+                if (g) cudaGraphExecDestroy(g);
+            for (auto g : r->graphs_horner)
                 if (g) cudaGraphExecDestroy(g);
             if (r->st) cudaStreamDestroy(r->st);
             r->lane.arena.free_all();
@@ -275,27 +298,32 @@ Engine::~Engine() {
     if (pinned_err) cudaFreeHost(pinned_err);
 }
 
+cudaGraphExec_t capture_phase(DbState& d, LaneRun& r, size_t c, int phase) {
+    cudaGraph_t g = nullptr;
+    IPB_CK(cudaStreamBeginCapture(r.st, cudaStreamCaptureModeThreadLocal));
+    try {
+        run_pipeline(*d.S, r.lane, d.sched[c], c, r.st, nullptr, phase);
+    } catch (...) {
+        cudaStreamEndCapture(r.st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    IPB_CK(cudaStreamEndCapture(r.st, &g));
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    IPB_CK(e);
+    return ge;
+}
+
 void capture_graphs(DbState& d, LaneRun& r) {
-    const Server& S = *d.S;
-    r.graphs.assign(d.max_batch + 1, nullptr);
+    r.graphs_db.assign(d.max_batch + 1, nullptr);
+    r.graphs_horner.assign(d.max_batch + 1, nullptr);
     for (size_t c = 1; c <= d.max_batch; ++c) {
         // An eager run first: kernel attributes are set outside the capture.
-        run_pipeline(S, r.lane, d.sched[c], c, r.st, nullptr);
-        IPB_CK(cudaStreamBeginCapture(r.st, cudaStreamCaptureModeThreadLocal));
-        cudaGraph_t g = nullptr;
-        try {
-            run_pipeline(S, r.lane, d.sched[c], c, r.st, nullptr);
-        } catch (...) {
-            cudaStreamEndCapture(r.st, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
-        }
-        IPB_CK(cudaStreamEndCapture(r.st, &g));
-        cudaGraphExec_t ge = nullptr;
-        const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
-        cudaGraphDestroy(g);
-        IPB_CK(e);
-        r.graphs[c] = ge;
+        run_pipeline(*d.S, r.lane, d.sched[c], c, r.st, nullptr);
+        r.graphs_db[c] = capture_phase(d, r, c, kPhaseDb);
+        r.graphs_horner[c] = capture_phase(d, r, c, kPhaseHorner);
     }
     IPB_CK(cudaStreamSynchronize(r.st));
 }
@@ -338,6 +366,7 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
         [&]() -> int {
             auto E = std::make_unique<ipb::Engine>();
             E->use_graphs = cfg.disable_graphs == 0;
+            E->overlap_db = cfg.overlap_db_passes != 0;
             for (size_t i = 0; i < n_dbs; ++i) {
                 if (!dbs[i] || !dbs[i]->s) throw std::invalid_argument("ipir_serve_create: null database handle");
                 auto d = std::make_unique<ipb::DbState>();
@@ -380,6 +409,7 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                     IPB_CK(cudaStreamCreateWithFlags(&r->st, cudaStreamNonBlocking));
                     IPB_CK(cudaEventCreate(&r->ev_start));
                     IPB_CK(cudaEventCreate(&r->ev_end));
+                    IPB_CK(cudaEventCreateWithFlags(&r->ev_db, cudaEventDisableTiming));
                     ipb::alloc_lane(*d.S, r->lane, mb, ipb::lane_gt_pass(*d.S, mb));
                     d.lanes.push_back(std::move(r));
                 }

@@ -185,7 +185,7 @@ size_t lane_bytes(const Server& S, size_t cap, int gt_pass) {
     const size_t R = S.pp.db_rows, G = S.pp.n_packed;
     return cap * S.qstride * 8 + cap * kKeyStride * 4 + cap * kRgswStride * 4 + cap * S.mv_qstride * 4 +
            tp_gt_bytes(gt_pass) + (size_t)2 * kN * cap * G * 4 + cap * S.pb_qstride * 4 + cap * S.resp_qstride * 8 +
-           mv_tc_planes_bytes(R, (int)cap) + sizeof(int);
+           mv_tc_planes_bytes(R, (int)cap) + sizeof(int) + 2 * sizeof(unsigned);
 }
 
 void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
@@ -203,6 +203,7 @@ void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
     L.resp = A.alloc<uint64_t>(cap * S.resp_qstride);
     L.planes = A.alloc<uint8_t>(mv_tc_planes_bytes(R, (int)cap));
     L.d_err = A.alloc<int>(1);
+    L.tiles = A.alloc<unsigned>(2);
     // Defined contents before any pipeline run (the autotuner runs on them).
     IPB_CK(cudaMemset(L.qraw, 0, cap * S.qstride * 8));
     IPB_CK(cudaMemset(L.planes, 0, mv_tc_planes_bytes(R, (int)cap)));
@@ -278,14 +279,12 @@ std::vector<Sched> default_sched(const Server&, size_t cap, int gt_pass) {
     return std::vector<Sched>(cap + 1, def);
 }
 
-int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev) {
-    if (count == 0) return 0;
-    if (count > L.cap || sc.tp_pass < 1 || sc.tp_pass > L.gt_pass)
-        throw std::invalid_argument("run_pipeline: batch exceeds the lane or its tensor-pass buffer");
+// Query prep, mat-vec, tensor pass, finalize: the part that streams the DB
+// and the precomputed tensors.
+static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev) {
     const Params& pp = S.pp;
     const Precomp& P = *S.pre;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
-    const size_t d_act = std::min(pp.D, G);
     const int nq = (int)count;
     int launches = 0;
     if (ev) IPB_CK(cudaEventRecord(ev[0], st));
@@ -299,7 +298,7 @@ int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaSt
         for (size_t c0 = 0; c0 < count; c0 += 32) {
             const int n = (int)std::min<size_t>(32, count - c0);
             IPB_CK(launch_matvec_tc(P.db, R, C, L.planes + 8 * c0 * R, n, P.tables, L.mvpart + c0 * S.mv_qstride,
-                                    S.mv_qstride, L.d_err, S.num_sms, S.tc_kchunk_rows, st));
+                                    S.mv_qstride, L.d_err, L.tiles, S.num_sms, S.tc_kchunk_rows, st));
             ++launches;
         }
         mv_parts = S.tc_kchunks;
@@ -316,13 +315,21 @@ int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaSt
     for (size_t c0 = 0; c0 < count; c0 += (size_t)sc.tp_pass) {
         const int n = (int)std::min<size_t>((size_t)sc.tp_pass, count - c0);
         IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.gt, L.tp_out,
-                                  L.d_err, S.num_sms, st));
+                                  L.d_err, L.tiles + 1, S.num_sms, st));
         launches += 2;  // permuted-key planes + GEMM
     }
     if (ev) IPB_CK(cudaEventRecord(ev[3], st));
     IPB_CK(launch_finalize(L.mvpart, S.mv_qstride, mv_parts, C, L.tp_out, P.pre_df, L.keys, kKeyStride, P.tables,
                            L.packed_b, S.pb_qstride, G, nq, st));
-    ++launches;
+    return launches + 1;
+}
+
+static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st,
+                            cudaEvent_t* ev) {
+    const Params& pp = S.pp;
+    const Precomp& P = *S.pre;
+    const size_t G = pp.n_packed, d_act = std::min(pp.D, G);
+    const int nq = (int)count;
     if (ev) IPB_CK(cudaEventRecord(ev[4], st));
     if (sc.horner_cluster)
         IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts,
@@ -330,8 +337,19 @@ int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaSt
     else
         IPB_CK(launch_horner(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts, L.resp,
                              S.resp_qstride, nq, st));
-    ++launches;
     if (ev) IPB_CK(cudaEventRecord(ev[5], st));
+    return 1;
+}
+
+int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
+                 int phases) {
+    if (count == 0) return 0;
+    if (count > L.cap || sc.tp_pass < 1 || sc.tp_pass > L.gt_pass)
+        throw std::invalid_argument("run_pipeline: batch exceeds the lane or its tensor-pass buffer");
+    if (phases != kPhaseAll) ev = nullptr;
+    int launches = 0;
+    if (phases & kPhaseDb) launches += run_db_phase(S, L, sc, count, st, ev);
+    if (phases & kPhaseHorner) launches += run_horner_phase(S, L, sc, count, st, ev);
     return launches;
 }
 
@@ -418,12 +436,19 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    // Sizes between two measured ones take the smaller one's kernels, with
+    // its tensor-pass split scaled to their own size (one pass, or halves),
+    // never more passes than that split.
     std::vector<Sched> table(L.cap + 1);
     for (size_t c = 1; c <= L.cap; ++c) {
-        const Sched* s = &best[0].second;
+        const std::pair<size_t, Sched>* s = &best[0];
         for (auto& kv : best)
-            if (kv.first <= c) s = &kv.second;
-        table[c] = *s;
+            if (kv.first <= c) s = &kv;
+        table[c] = s->second;
+        const int whole = (int)std::min<size_t>(s->first, (size_t)L.gt_pass);
+        const bool halves = s->second.tp_pass < whole;
+        const size_t want = halves ? (c + 1) / 2 : c;
+        table[c].tp_pass = (int)std::max<size_t>(1, std::min<size_t>(want, (size_t)L.gt_pass));
     }
     table[0] = table[1];
     return table;
@@ -836,6 +861,7 @@ struct MvScratch {
     ipb::DevArena arena;
     ipb::DevTables* T = nullptr;
     int* err = nullptr;
+    unsigned* tiles = nullptr;
     uint8_t* planes = nullptr;
     size_t planes_cap = 0;
     uint32_t* part = nullptr;
@@ -866,6 +892,7 @@ int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_
             if (!M.T) {
                 M.T = ipb::upload_tables(M.arena, 0);
                 M.err = M.arena.alloc<int>(1);
+                M.tiles = M.arena.alloc<unsigned>(1);
                 IPB_CK(cudaMemset(M.err, 0, sizeof(int)));
                 IPB_CK(cudaDeviceSynchronize());  // tables visible to any stream
             }
@@ -886,7 +913,7 @@ int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_
                 const int n = (int)std::min<size_t>(32, count - q0);
                 uint32_t* dst = chunks == 1 ? out + q0 * 2 * cols : M.part + q0 * pq;
                 IPB_CK(ipb::launch_matvec_tc(db, rows, cols, M.planes + 8 * q0 * rows, n, M.T, dst,
-                                             chunks == 1 ? 2 * cols : pq, M.err, sms, (int)kchunk, s));
+                                             chunks == 1 ? 2 * cols : pq, M.err, M.tiles, sms, (int)kchunk, s));
             }
             if (chunks > 1)
                 IPB_CK(ipb::launch_mv_chunk_reduce(M.part, pq, chunks, cols, M.T, out, 2 * cols, (int)count, s));

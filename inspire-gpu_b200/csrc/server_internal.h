@@ -102,6 +102,7 @@ struct Lane {
     uint64_t* resp = nullptr;
     uint8_t* planes = nullptr;   // query byte planes for the tensor-core mat-vec
     int* d_err = nullptr;        // device error word (pipeline wait timeouts)
+    unsigned* tiles = nullptr;   // work-item counters: [0] mat-vec, [1] tensor pass
     ~Lane() { arena.free_all(); }
 };
 
@@ -134,9 +135,14 @@ struct Server {
 // Bytes of a lane of `cap` queries whose Gt holds `gt_pass` queries.
 size_t lane_bytes(const Server& S, size_t cap, int gt_pass);
 void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass);
-// Enqueues the answer pipeline for `count` staged queries of lane L on
-// stream st; returns the number of kernels launched.  ev (6 events) or null.
-int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev);
+// Pipeline phases: the DB-bound part (query prep, mat-vec, tensor pass,
+// finalize) and the Horner chains.
+constexpr int kPhaseDb = 1, kPhaseHorner = 2, kPhaseAll = 3;
+// Enqueues the answer pipeline (the given phases) for `count` staged
+// queries of lane L on stream st; returns the number of kernels launched.
+// ev (6 stage events, used when all phases run) or null.
+int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
+                 int phases = kPhaseAll);
 // H2D of one flat query into query slot i of lane L.
 void stage_query_flat(const Server& S, Lane& L, size_t i, const uint64_t* flat, cudaStream_t st);
 // Schedule table (index = batch size, 0 unused) for a lane of `cap` queries

@@ -19,6 +19,11 @@
 // Layouts (u8): Dt[l][i][g*4 + a][u] (built once at preprocess by
 // dt_transpose_kernel), Gt[l][i][q*4 + b][u] (built per batch by
 // gen_g_kernel).  Output tp_out[l][i][q][g] (u32, reduced).
+//
+// The GEMM kernel is persistent with dynamic work items: the producer takes
+// the next item from a per-launch atomic counter and publishes it to the MMA
+// thread and the epilogue through a ring of shared slots (-1 ends it), so
+// SMs held by other kernels at launch take fewer items.
 #include <cuda.h>
 
 #include <algorithm>
@@ -34,6 +39,7 @@ namespace {
 using namespace tc;
 
 constexpr int kUPad = 4096;       // u range, 4092 used
+constexpr int kRing = 8;          // published work items in flight
 constexpr int kUsed = 2 * 2 * kSteps;
 
 __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
@@ -162,6 +168,7 @@ struct TpParams {
     int acc_stages;
     uint32_t tmem_cols;
     int* err;
+    unsigned* tiles;       // work-item counter, zero at launch
     uint32_t c[2][7];      // 256^k mod q_l
     uint64_t cr[2];
     uint32_t q[2];
@@ -187,12 +194,15 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
     uint64_t* tempty = bars + 2 * S + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 4);
     __shared__ volatile int abort_flag;
+    __shared__ volatile int item_ring[kRing];
+    __shared__ uint64_t ifull[kRing], iempty[kRing];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         abort_flag = 0;
         for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128); }
+        for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 128); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -213,7 +223,18 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
         if (lane == 0) {
             int s = 0;
             uint32_t ph = 0;
-            for (int item = blockIdx.x; item < n_items && !abort_flag; item += gridDim.x) {
+            for (int it = 0;; ++it) {
+                const int r = it % kRing;
+                int item = -1;
+                if (!abort_flag && mbar_wait(&iempty[r], ((uint32_t)(it / kRing) & 1) ^ 1, P.err, 16)) {
+                    const unsigned t = atomicAdd(P.tiles, 1u);
+                    if (t < (unsigned)n_items) item = (int)t;
+                } else {
+                    abort_flag = 1;
+                }
+                item_ring[r] = item;
+                mbar_arrive(&ifull[r]);
+                if (item < 0) break;
                 const int li = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
                 const int rowa = li * slot_rows + mg * P.mti * 128;
                 const int rowb = li * P.npad;
@@ -237,7 +258,12 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
             const uint32_t idesc = idesc_i8_kk(P.npad);
             int s = 0, as = 0;
             uint32_t ph = 0, aph = 0;
-            for (int item = blockIdx.x; item < n_items && !abort_flag; item += gridDim.x) {
+            for (int it = 0;; ++it) {
+                const int r = it % kRing;
+                if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 17)) { abort_flag = 1; break; }
+                const int item = item_ring[r];
+                mbar_arrive(&iempty[r]);
+                if (item < 0 || abort_flag) break;
                 if (!mbar_wait(&tempty[as], aph ^ 1, P.err, 13)) { abort_flag = 1; break; }
                 tc_fence_after();
                 const uint32_t d0 = tmem_base + (uint32_t)(as * acc_cols);
@@ -276,7 +302,12 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
         const uint32_t lane_base = (uint32_t)(wq * 32) << 16;
         int as = 0;
         uint32_t aph = 0;
-        for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        for (int it = 0;; ++it) {
+            const int r = it % kRing;
+            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 18)) { abort_flag = 1; break; }
+            const int item = item_ring[r];
+            mbar_arrive(&iempty[r]);
+            if (item < 0) break;
             if (!mbar_wait(&tfull[as], aph, P.err, 15)) { abort_flag = 1; break; }
             tc_fence_after();
             const int li0 = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
@@ -377,10 +408,10 @@ cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp
 }
 
 cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
-                               int nq_total, int q0, uint8_t* Gt, uint32_t* tp_out, int* err, int num_sms,
-                               cudaStream_t s) {
+                               int nq_total, int q0, uint8_t* Gt, uint32_t* tp_out, int* err, unsigned* tiles,
+                               int num_sms, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    if (nq > 32) return cudaErrorInvalidValue;
+    if (nq > 32 || !tiles) return cudaErrorInvalidValue;
     const int npad = ((4 * nq + 15) / 16) * 16;
     gen_g_kernel<<<dim3(kN / 8, nq, 2), 256, 0, s>>>(keys, key_qstride, Gt, npad);
     cudaError_t e = cudaGetLastError();
@@ -410,6 +441,7 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     while (tc < need) tc <<= 1;
     P.tmem_cols = tc;
     P.err = err;
+    P.tiles = tiles;
     const uint32_t qs[2] = {kQ0, kQ1};
     for (int l = 0; l < 2; ++l) {
         for (int k = 0; k < 7; ++k) P.c[l][k] = powmod_host(256, k, qs[l]);
@@ -427,6 +459,7 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     e = allow_max_smem(tp_tc_kernel);
     if (e) return e;
     const int items = (2 * kN / P.spi) * P.n_mg;
+    if ((e = cudaMemsetAsync(tiles, 0, sizeof(unsigned), s))) return e;
     tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), 256, smem, s>>>(ma, mb, P);
     return cudaGetLastError();
 }
