@@ -17,8 +17,9 @@
 // reduces mod q_l.  Exact, so equal to the reference.
 //
 // Layouts (u8): Dt[l][i][g*4 + a][u] (built once at preprocess by
-// dt_transpose_kernel), Gt[l][i][q*4 + b][u] (built per batch by
-// gen_g_kernel).  Output tp_out[l][i][q][g] (u32, reduced).
+// dt_transpose_kernel), Gt[l][i][q*4 + b][u] with 4 nq rows per slot, no
+// padding (built per pass by gen_g_kernel).  Output tp_out[l][i][q][g]
+// (u32, reduced).
 //
 // The GEMM kernel is persistent with dynamic work items: the producer takes
 // the next item from a per-launch atomic counter and publishes it to the MMA
@@ -110,10 +111,10 @@ __global__ void __launch_bounds__(256) dt_export_kernel(const uint8_t* __restric
 
 // ------------------------------------------------------------------ permuted keys
 // Gt[l][i][q*4 + b][u] = byte b of K5_q[l][j][perm_t(i)], t = 5^(1022-s) or
-// 2N - 5^(1022-s).  One CTA per (8 slots, query, limb); the query's key for
-// the limb sits in shared memory.
+// 2N - 5^(1022-s), rq = 4 nq rows per slot.  One CTA per (8 slots, query,
+// limb); the query's key for the limb sits in shared memory.
 __global__ void __launch_bounds__(256) gen_g_kernel(const uint32_t* __restrict__ keys, size_t key_qstride,
-                                                    uint8_t* __restrict__ Gt, int npad) {
+                                                    uint8_t* __restrict__ Gt, int rq) {
     __shared__ uint32_t k5[2][kN];
     __shared__ uint32_t tpow[kSteps];
     const int ib = blockIdx.x, q = blockIdx.y, l = blockIdx.z;
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256) gen_g_kernel(const uint32_t* __restrict__
     for (int ii = 0; ii < 8; ++ii) {
         const int i = ib * 8 + ii;
         const uint32_t odd = 2 * brev11(i) + 1;
-        uint8_t* base = Gt + ((size_t)(l * kN + i) * npad + q * 4) * kUPad;
+        uint8_t* base = Gt + ((size_t)(l * kN + i) * rq + q * 4) * kUPad;
         for (int u4 = threadIdx.x; u4 < kUPad / 4; u4 += 256) {
             uint32_t v[4];
 #pragma unroll
@@ -158,7 +159,8 @@ struct TpParams {
     int nq_total;          // queries in the batch (out stride)
     int q0;                // first query of this pass
     int nq;                // queries in this pass
-    int npad;              // N = roundup16(4 nq)
+    int rq;                // key rows per slot in Gt (4 nq)
+    int nb;                // N = key rows per item, roundup16(spi * rq)
     int G;                 // groups
     int mti;               // M tiles (128 rows) per item (4G >= 128)
     int n_mg;              // M-tile groups per (l, i)
@@ -180,11 +182,8 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int S = P.stages;
     const uint32_t a_tile = 128 * 128;
-    // With packed slots the MMA for slot sl reads rows sl*4G .. sl*4G + 127,
-    // up to 224 rows: the A region then spans two tiles so every read stays
-    // inside this stage.
-    const uint32_t a_region = (uint32_t)(P.spi > 1 ? 2 : P.mti) * a_tile;
-    const uint32_t b_bytes = (uint32_t)(P.npad * P.spi) * 128;
+    const uint32_t a_region = (uint32_t)P.mti * a_tile;
+    const uint32_t b_bytes = (uint32_t)P.nb * 128;
     const uint32_t stage_bytes = a_region + b_bytes;
     const uint32_t tx_bytes = (uint32_t)P.mti * P.rows_box * 128 + b_bytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
@@ -216,7 +215,7 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
     const uint32_t tmem_base = *tmem_slot;
     const int n_items = (2 * kN / P.spi) * P.n_mg;
     constexpr int ktiles = kUPad / 128;
-    const int acc_cols = P.mti * P.spi * P.npad;
+    const int acc_cols = P.mti * P.nb;
     const int slot_rows = 4 * P.G;  // A rows of one slot
 
     if (warp == 0) {
@@ -237,7 +236,7 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
                 if (item < 0) break;
                 const int li = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
                 const int rowa = li * slot_rows + mg * P.mti * 128;
-                const int rowb = li * P.npad;
+                const int rowb = li * P.rq;
                 for (int kt = 0; kt < ktiles; ++kt) {
                     if (!mbar_wait(&empty[s], ph ^ 1, P.err, 11)) { abort_flag = 1; break; }
                     uint8_t* st = smem + (size_t)s * stage_bytes;
@@ -255,7 +254,10 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = idesc_i8_kk(P.npad);
+            // Packed slots: one M = 128 MMA over all spi slots' rows against all
+            // their key rows (N = nb); the epilogue keeps the diagonal blocks
+            // (slot rows x the same slot's key columns).
+            const uint32_t idesc = idesc_i8_kk(P.nb);
             int s = 0, as = 0;
             uint32_t ph = 0, aph = 0;
             for (int it = 0;; ++it) {
@@ -278,16 +280,11 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
                         if (P.spi == 1) {
                             const uint64_t b = smem_desc(bt + kk * 32, 16, 1024);
                             for (int mt = 0; mt < P.mti; ++mt)
-                                mma_i8(d0 + (uint32_t)(mt * P.npad), smem_desc(st + mt * a_tile + kk * 32, 16, 1024),
+                                mma_i8(d0 + (uint32_t)(mt * P.nb), smem_desc(st + mt * a_tile + kk * 32, 16, 1024),
                                        b, idesc, acc);
                         } else {
-                            // slot sl's rows start at row sl*4G of the shared tile (a multiple of 8
-                            // rows, so the descriptor stays on a swizzle-atom boundary); rows past
-                            // the slot produce accumulator lanes the epilogue ignores.
-                            for (int sl = 0; sl < P.spi; ++sl)
-                                mma_i8(d0 + (uint32_t)(sl * P.npad),
-                                       smem_desc(st + sl * slot_rows * 128 + kk * 32, 16, 1024),
-                                       smem_desc(bt + sl * P.npad * 128 + kk * 32, 16, 1024), idesc, acc);
+                            mma_i8(d0, smem_desc(st + kk * 32, 16, 1024), smem_desc(bt + kk * 32, 16, 1024), idesc,
+                                   acc);
                         }
                     }
                     mma_commit(&empty[s]);
@@ -313,15 +310,24 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
             const int li0 = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
             const int l = li0 / kN;
             const uint32_t* c = P.c[l];
-            for (int mt = 0; mt < P.mti * P.spi; ++mt) {
-                // spi == 1: tile mt of the slot's 4G rows; spi > 1: slot li0 + mt, rows 0..4G-1
+            // spi == 1: TMEM block mt (columns mt * nb) holds M-tile mt of the
+            // slot's 4G rows.  spi > 1: lane row = sl * 4G + g*4 + a, and slot
+            // sl's keys are columns sl * rq ..; the loop runs over the slots
+            // this warp's 32 lanes touch (warp-uniform bounds for tcgen05.ld).
+            const int row = wq * 32 + lane;
+            const int nblk = P.spi > 1 ? min(P.spi - 1, (wq * 32 + 31) / slot_rows) - (wq * 32) / slot_rows + 1
+                                       : P.mti;
+            const int blk0 = P.spi > 1 ? (wq * 32) / slot_rows : 0;
+            for (int bi = 0; bi < nblk; ++bi) {
+                const int mt = blk0 + bi;
                 const int li = li0 + (P.spi > 1 ? mt : 0);
-                const int grow = (P.spi > 1 ? 0 : (mg * P.mti + mt) * 128) + wq * 32 + lane;  // g*4 + a
+                const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;  // g*4 + a
                 const int g = grow >> 2, a = grow & 3;
-                const bool valid = grow < slot_rows;
+                const bool valid = grow >= 0 && grow < slot_rows;
                 for (int q = 0; q < P.nq; ++q) {
                     uint32_t v[4];
-                    tmem_ld4(tmem_base + lane_base + (uint32_t)(as * acc_cols + mt * P.npad + 4 * q), v);
+                    const int col = (P.spi > 1 ? mt * P.rq : mt * P.nb) + 4 * q;
+                    tmem_ld4(tmem_base + lane_base + (uint32_t)(as * acc_cols + col), v);
                     uint64_t part = (uint64_t)c[a] * v[0] + (uint64_t)c[a + 1] * v[1] + (uint64_t)c[a + 2] * v[2] +
                                     (uint64_t)c[a + 3] * v[3];
                     part += __shfl_down_sync(0xffffffffu, part, 1);
@@ -384,7 +390,7 @@ uint32_t powmod_host(uint64_t b, uint64_t e, uint64_t q) {
 }  // namespace
 
 size_t tp_dt_bytes(size_t groups) { return (size_t)2 * kN * 4 * groups * kUPad; }
-size_t tp_gt_bytes(int max_pass) { return (size_t)2 * kN * (size_t)(((4 * max_pass + 15) / 16) * 16) * kUPad; }
+size_t tp_gt_bytes(int max_pass) { return (size_t)2 * kN * 4 * (size_t)max_pass * kUPad; }
 
 int tp_pass_queries(size_t groups) {
     // queries per GEMM pass so that the accumulators fit TMEM (512 columns)
@@ -412,8 +418,8 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
                                int num_sms, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
     if (nq > 32 || !tiles) return cudaErrorInvalidValue;
-    const int npad = ((4 * nq + 15) / 16) * 16;
-    gen_g_kernel<<<dim3(kN / 8, nq, 2), 256, 0, s>>>(keys, key_qstride, Gt, npad);
+    const int rq = 4 * nq;
+    gen_g_kernel<<<dim3(kN / 8, nq, 2), 256, 0, s>>>(keys, key_qstride, Gt, rq);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
     TpParams P{};
@@ -421,7 +427,7 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     P.nq_total = nq_total;
     P.q0 = q0;
     P.nq = nq;
-    P.npad = npad;
+    P.rq = rq;
     P.G = (int)G;
     const int nmt = (int)std::max<size_t>(1, (4 * G + 127) / 128);
     P.mti = std::min(nmt, 4);
@@ -429,15 +435,17 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     // Small G: pack spi slots (each 4G rows) into one 128-row A tile.  G even
     // keeps every slot start on an 8-row (1024-byte) swizzle atom; spi a power
     // of two divides kN, so a packed item never straddles the two limbs.
+    auto nb_of = [&](int sp) { return ((sp * rq + 15) / 16) * 16; };
     P.spi = 1;
     if (4 * G < 128 && G % 2 == 0) {
         while (2 * P.spi * 4 * (int)G <= 128) P.spi *= 2;
-        while (P.spi > 1 && (P.spi * npad > 256 || 2 * P.spi * npad > 512)) P.spi /= 2;
+        while (P.spi > 1 && (nb_of(P.spi) > 256 || 2 * nb_of(P.spi) > 512)) P.spi /= 2;
     }
+    P.nb = nb_of(P.spi);
     P.rows_box = (int)std::min<size_t>(128, 4 * G * (size_t)P.spi);
-    if (P.mti * P.spi * npad > 512) return cudaErrorInvalidValue;
-    P.acc_stages = (2 * P.mti * P.spi * npad <= 512) ? 2 : 1;
-    uint32_t need = (uint32_t)(P.acc_stages * P.mti * P.spi * npad), tc = 32;
+    if (P.mti * P.nb > 512) return cudaErrorInvalidValue;
+    P.acc_stages = (2 * P.mti * P.nb <= 512) ? 2 : 1;
+    uint32_t need = (uint32_t)(P.acc_stages * P.mti * P.nb), tc = 32;
     while (tc < need) tc <<= 1;
     P.tmem_cols = tc;
     P.err = err;
@@ -448,13 +456,14 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
         P.cr[l] = ~0ULL / qs[l];
         P.q[l] = qs[l];
     }
-    const size_t a_region = (size_t)(P.spi > 1 ? 2 : P.mti) * 128 * 128;
-    const size_t stage_bytes = a_region + (size_t)npad * P.spi * 128;
+    const size_t a_region = (size_t)P.mti * 128 * 128;
+    const size_t stage_bytes = a_region + (size_t)P.nb * 128;
     P.stages = (int)std::min<size_t>(8, (200 * 1024) / stage_bytes);
     if (P.stages < 2) return cudaErrorInvalidValue;
     CUtensorMap ma, mb;
     if (!make_map(&ma, Dt, (uint64_t)2 * kN * 4 * G, (uint32_t)P.rows_box)) return cudaErrorInvalidValue;
-    if (!make_map(&mb, Gt, (uint64_t)2 * kN * npad, (uint32_t)(npad * P.spi))) return cudaErrorInvalidValue;
+    // Box rows past the last slot's keys read zeros (TMA out-of-range fill).
+    if (!make_map(&mb, Gt, (uint64_t)2 * kN * rq, (uint32_t)P.nb)) return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
     e = allow_max_smem(tp_tc_kernel);
     if (e) return e;
