@@ -314,6 +314,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         if sampler:
             sampler.start()
+            torch.cuda.nvtx.range_push("timed")   # the headline region, for ncu --nvtx-include timed/
         n0 = srv.launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -321,6 +322,8 @@ def run_ours(args):
             srv.run(count)
         e1.record(stream)
         torch.cuda.synchronize()
+        if sampler:
+            torch.cuda.nvtx.range_pop()
         launches = srv.launch_count() - n0
         clocks = sampler.stop() if sampler else None
         barrier()
