@@ -43,16 +43,17 @@ cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, in
                                    const DevTables* T, uint32_t* out, size_t out_qstride, int nq, cudaStream_t s);
 
 // Tensor pass on tcgen05 (tensorpass_tc.cu).  Dt: re-laid-out D tensors
-// [l][i][g*4 + a][4096] u8; Gt: per-batch permuted-key planes; tp_out:
-// [l][i][q][g] u32 for the nq_total queries of the batch.
+// [l][i][g*4 + a][4096] u8; keyt: per-pass key table scratch
+// (tp_keyt_bytes); tp_out: [l][i][q][g] u32 for the nq_total queries of
+// the batch.
 size_t tp_dt_bytes(size_t groups);
-size_t tp_gt_bytes(int max_pass);
+size_t tp_keyt_bytes(int max_pass);
 int tp_pass_queries(size_t groups);
 cudaError_t launch_dt_transpose(const uint32_t* dp, const uint32_t* dm, size_t g0, size_t nw, size_t G, uint8_t* Dt,
                                 cudaStream_t s);
 cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp, uint32_t* dm, cudaStream_t s);
 cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
-                               int nq_total, int q0, uint8_t* Gt, uint32_t* tp_out, int* err, unsigned* tiles,
+                               int nq_total, int q0, uint32_t* keyt, uint32_t* tp_out, int* err, unsigned* tiles,
                                int num_sms, cudaStream_t s);
 
 // packed_b[q][g][limb][N] = NTT(sum_y mvpart) - tp_out - Dfinal (.) Kn1.

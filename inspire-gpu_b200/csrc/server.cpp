@@ -184,7 +184,7 @@ static int pick_pow2_chunks(size_t target, size_t maxv) {
 size_t lane_bytes(const Server& S, size_t cap, int gt_pass) {
     const size_t R = S.pp.db_rows, G = S.pp.n_packed;
     return cap * S.qstride * 8 + cap * kKeyStride * 4 + cap * kRgswStride * 4 + cap * S.mv_qstride * 4 +
-           tp_gt_bytes(gt_pass) + (size_t)2 * kN * cap * G * 4 + cap * S.pb_qstride * 4 + cap * S.resp_qstride * 8 +
+           tp_keyt_bytes(gt_pass) + (size_t)2 * kN * cap * G * 4 + cap * S.pb_qstride * 4 + cap * S.resp_qstride * 8 +
            mv_tc_planes_bytes(R, (int)cap) + sizeof(int) + 2 * sizeof(unsigned);
 }
 
@@ -197,7 +197,7 @@ void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
     L.keys = A.alloc<uint32_t>(cap * kKeyStride);
     L.rgsw32 = A.alloc<uint32_t>(cap * kRgswStride);
     L.mvpart = A.alloc<uint32_t>(cap * S.mv_qstride);
-    L.gt = A.alloc<uint8_t>(tp_gt_bytes(gt_pass));
+    L.keyt = A.alloc<uint32_t>(tp_keyt_bytes(gt_pass) / 4);
     L.tp_out = A.alloc<uint32_t>((size_t)2 * kN * cap * G);
     L.packed_b = A.alloc<uint32_t>(cap * S.pb_qstride);
     L.resp = A.alloc<uint64_t>(cap * S.resp_qstride);
@@ -314,9 +314,9 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
     if (ev) IPB_CK(cudaEventRecord(ev[2], st));
     for (size_t c0 = 0; c0 < count; c0 += (size_t)sc.tp_pass) {
         const int n = (int)std::min<size_t>((size_t)sc.tp_pass, count - c0);
-        IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.gt, L.tp_out,
-                                  L.d_err, L.tiles + 1, S.num_sms, st));
-        launches += 2;  // permuted-key planes + GEMM
+        IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.keyt,
+                                  L.tp_out, L.d_err, L.tiles + 1, S.num_sms, st));
+        launches += 2;  // key table + GEMM
     }
     if (ev) IPB_CK(cudaEventRecord(ev[3], st));
     IPB_CK(launch_finalize(L.mvpart, S.mv_qstride, mv_parts, C, L.tp_out, P.pre_df, L.keys, kKeyStride, P.tables,

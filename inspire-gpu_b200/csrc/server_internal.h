@@ -91,12 +91,12 @@ struct Sched {
 struct Lane {
     DevArena arena;
     size_t cap = 0;
-    int gt_pass = 0;  // queries per tensor pass the Gt buffer holds
+    int gt_pass = 0;  // queries per tensor pass the key-table buffer holds
     uint64_t* qraw = nullptr;
     uint32_t* keys = nullptr;
     uint32_t* rgsw32 = nullptr;
     uint32_t* mvpart = nullptr;
-    uint8_t* gt = nullptr;       // per-pass permuted-key planes (tensor-pass N operand)
+    uint32_t* keyt = nullptr;    // per-pass key table the tensor-pass GEMM gathers its N operand from
     uint32_t* tp_out = nullptr;  // tensor-pass result [l][i][q][g]
     uint32_t* packed_b = nullptr;
     uint64_t* resp = nullptr;

@@ -16,15 +16,22 @@
 // epilogue forms sum_{a,b} (256^(a+b) mod q_l) * P[g*4+a][q*4+b] < 2^59 and
 // reduces mod q_l.  Exact, so equal to the reference.
 //
-// Layouts (u8): Dt[l][i][g*4 + a][u] (built once at preprocess by
-// dt_transpose_kernel), Gt[l][i][q*4 + b][u] with 4 nq rows per slot, no
-// padding (built per pass by gen_g_kernel).  Output tp_out[l][i][q][g]
-// (u32, reduced).
+// Layouts: Dt[l][i][g*4 + a][u] u8 (built once at preprocess by
+// dt_transpose_kernel) is the A operand, loaded by TMA.  The B operand, the
+// byte planes Gq[l][i][q*4 + b][u], is never stored: per pass keyt_kernel
+// writes the compact key table Kt[l][j][p][q] (u32, queries innermost,
+// <= 1 MB, stays in L2) and the GEMM's key warps gather from it straight
+// into each stage's swizzled B tile.  Output tp_out[l][i][q][g] (u32,
+// reduced).
 //
 // The GEMM kernel is persistent with dynamic work items: the producer takes
 // the next item from a per-launch atomic counter and publishes it to the MMA
-// thread and the epilogue through a ring of shared slots (-1 ends it), so
-// SMs held by other kernels at launch take fewer items.
+// thread, the key warps and the epilogue through a ring of shared slots
+// (-1 ends it), so SMs held by other kernels at launch take fewer items.
+// Warp roles (768 threads): 0 TMA producer (one thread), 1 TMEM allocation
+// and MMA issue (one thread), 4..7 epilogue, 8..23 key planes in four
+// groups of 128 threads, group g filling the K tiles kt = g mod 4, so four
+// stages' gathers are in flight at once.
 #include <cuda.h>
 
 #include <algorithm>
@@ -41,6 +48,10 @@ using namespace tc;
 
 constexpr int kUPad = 4096;       // u range, 4092 used
 constexpr int kRing = 8;          // published work items in flight
+constexpr int kKeyGroups = 4;
+constexpr int kKeyGroup = 128;    // threads per key group
+constexpr int kKeyThreads = kKeyGroups * kKeyGroup;  // warps 8..23
+constexpr int kTpThreads = 256 + kKeyThreads;
 constexpr int kUsed = 2 * 2 * kSteps;
 
 __device__ __forceinline__ uint32_t pow5_mod2n(uint32_t e) {
@@ -109,48 +120,31 @@ __global__ void __launch_bounds__(256) dt_export_kernel(const uint8_t* __restric
     (dir ? dm : dp)[((size_t)(l * kSteps + s) * kDeff + j) * kN + i] = v;
 }
 
-// ------------------------------------------------------------------ permuted keys
-// Gt[l][i][q*4 + b][u] = byte b of K5_q[l][j][perm_t(i)], t = 5^(1022-s) or
-// 2N - 5^(1022-s), rq = 4 nq rows per slot.  One CTA per (8 slots, query,
-// limb); the query's key for the limb sits in shared memory.
-__global__ void __launch_bounds__(256) gen_g_kernel(const uint32_t* __restrict__ keys, size_t key_qstride,
-                                                    uint8_t* __restrict__ Gt, int rq) {
-    __shared__ uint32_t k5[2][kN];
-    __shared__ uint32_t tpow[kSteps];
-    const int ib = blockIdx.x, q = blockIdx.y, l = blockIdx.z;
-    const uint32_t* kp = keys + (size_t)q * key_qstride + (size_t)(l * kDeff) * kN;  // key 0 = ksk5, [j][N]
-    for (int t = threadIdx.x; t < 2 * kN; t += 256) k5[t / kN][t % kN] = kp[t];
-    for (int s = threadIdx.x; s < kSteps; s += 256) tpow[s] = pow5_mod2n(kHalf - 2 - s);
-    __syncthreads();
-    for (int ii = 0; ii < 8; ++ii) {
-        const int i = ib * 8 + ii;
-        const uint32_t odd = 2 * brev11(i) + 1;
-        uint8_t* base = Gt + ((size_t)(l * kN + i) * rq + q * 4) * kUPad;
-        for (int u4 = threadIdx.x; u4 < kUPad / 4; u4 += 256) {
-            uint32_t v[4];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int w = 2 * u4 + h;
-                if (w < 2 * kSteps) {
-                    const int dir = w >= kSteps;
-                    const int s = w - dir * kSteps;
-                    uint32_t t = tpow[s];
-                    if (dir) t = (2 * kN - t) & (2 * kN - 1);
-                    const uint32_t p = perm_from_odd(t, odd);
-                    v[2 * h] = k5[0][p];
-                    v[2 * h + 1] = k5[1][p];
-                } else {
-                    v[2 * h] = v[2 * h + 1] = 0;
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                const uint32_t word = ((v[0] >> (8 * b)) & 0xFFu) | (((v[1] >> (8 * b)) & 0xFFu) << 8) |
-                                      (((v[2] >> (8 * b)) & 0xFFu) << 16) | (((v[3] >> (8 * b)) & 0xFFu) << 24);
-                *reinterpret_cast<uint32_t*>(base + (size_t)b * kUPad + 4 * u4) = word;
-            }
-        }
-    }
+// ------------------------------------------------------------------ key table
+// Kt[l][j][p][qq] = K5_q[l][j][p] (key 0 of query qq of the pass, NTT form)
+// for qq < nq, zero for nq <= qq < W, W = 8 ceil(nq / 8): the W values of one
+// position fill whole 32-byte sectors.
+__global__ void __launch_bounds__(256) keyt_kernel(const uint32_t* __restrict__ keys, size_t key_qstride, int nq,
+                                                   int W, uint32_t* __restrict__ Kt) {
+    const size_t idx = (size_t)blockIdx.x * 256 + threadIdx.x;  // over ((l*kDeff + j)*kN + p)*W + qq
+    if (idx >= (size_t)2 * kDeff * kN * W) return;
+    const int qq = (int)(idx % (size_t)W);
+    const size_t ljp = idx / (size_t)W;
+    uint32_t v = 0;
+    if (qq < nq) v = keys[(size_t)qq * key_qstride + ljp];  // keys[q][key 0][l][j][p]
+    Kt[idx] = v;
+}
+
+// One 32-byte sector (8 queries' key words) in a single 256-bit load.
+__device__ __forceinline__ void ld_sector(const uint32_t* p, uint32_t (&v)[8]) {
+    asm volatile("ld.global.nc.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "l"(p));
+}
+// 32-bit store into a K-major SWIZZLE_128B tile (1024-byte aligned base):
+// row r's 16-byte chunk c sits at chunk c ^ (r & 7).
+__device__ __forceinline__ void st_sw128(uint8_t* tile, uint32_t row, uint32_t col, uint32_t w) {
+    *reinterpret_cast<uint32_t*>(tile + row * 128 + ((((col >> 4) ^ (row & 7)) & 7) << 4) + (col & 15)) = w;
 }
 
 // ------------------------------------------------------------------ GEMM
@@ -159,8 +153,10 @@ struct TpParams {
     int nq_total;          // queries in the batch (out stride)
     int q0;                // first query of this pass
     int nq;                // queries in this pass
-    int rq;                // key rows per slot in Gt (4 nq)
+    int rq;                // key rows per slot in the B tile (4 nq)
     int nb;                // N = key rows per item, roundup16(spi * rq)
+    int w8;                // 8-query groups per key-table position
+    const uint32_t* keyt;  // Kt[l][j][p][8 * w8], 32-byte aligned rows
     int G;                 // groups
     int mti;               // M tiles (128 rows) per item (4G >= 128)
     int n_mg;              // M-tile groups per (l, i)
@@ -176,8 +172,7 @@ struct TpParams {
     uint32_t q[2];
 };
 
-__global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ CUtensorMap map_a,
-                                                       const __grid_constant__ CUtensorMap map_b, TpParams P) {
+__global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_constant__ CUtensorMap map_a, TpParams P) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int S = P.stages;
@@ -185,7 +180,7 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
     const uint32_t a_region = (uint32_t)P.mti * a_tile;
     const uint32_t b_bytes = (uint32_t)P.nb * 128;
     const uint32_t stage_bytes = a_region + b_bytes;
-    const uint32_t tx_bytes = (uint32_t)P.mti * P.rows_box * 128 + b_bytes;
+    const uint32_t tx_bytes = (uint32_t)P.mti * P.rows_box * 128;  // A only; B is written by the key warps
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
     uint64_t* full = bars;
     uint64_t* empty = bars + S;
@@ -195,13 +190,26 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
     __shared__ volatile int abort_flag;
     __shared__ volatile int item_ring[kRing];
     __shared__ uint64_t ifull[kRing], iempty[kRing];
+    // tw[w] for w = dir * 1023 + s: t = 5^(1022 - s), or 2N - t when dir = 1;
+    // the two w of a 4-u group are one aligned 64-bit read.
+    __shared__ __align__(8) uint32_t tw[2 * kSteps + 2];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int w = threadIdx.x; w < 2 * kSteps + 2; w += blockDim.x) {
+        uint32_t t = 0;
+        if (w < 2 * kSteps) {
+            const int dir = w >= kSteps;
+            t = pow5_mod2n(kHalf - 2 - (w - dir * kSteps));
+            if (dir) t = (2 * kN - t) & (2 * kN - 1);
+        }
+        tw[w] = t;
+    }
     if (threadIdx.x == 0) {
         abort_flag = 0;
-        for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        // full: the producer's expect_tx arrival (A bytes) + the key group of the stage
+        for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1 + kKeyGroup); mbar_init(&empty[s], 1); }
         for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128); }
-        for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 128); }
+        for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 128 + kKeyThreads); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -236,14 +244,12 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
                 if (item < 0) break;
                 const int li = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
                 const int rowa = li * slot_rows + mg * P.mti * 128;
-                const int rowb = li * P.rq;
                 for (int kt = 0; kt < ktiles; ++kt) {
                     if (!mbar_wait(&empty[s], ph ^ 1, P.err, 11)) { abort_flag = 1; break; }
                     uint8_t* st = smem + (size_t)s * stage_bytes;
                     mbar_expect_tx(&full[s], tx_bytes);
                     for (int mt = 0; mt < P.mti; ++mt)
                         tma_load_2d(st + mt * a_tile, &map_a, &full[s], kt * 128, rowa + mt * 128);
-                    tma_load_2d(st + a_region, &map_b, &full[s], kt * 128, rowb);
                     if (++s == S) { s = 0; ph ^= 1; }
                 }
             }
@@ -292,6 +298,81 @@ __global__ void __launch_bounds__(256, 1) tp_tc_kernel(const __grid_constant__ C
                 }
                 mma_commit(&tfull[as]);
                 if (++as == P.acc_stages) { as = 0; aph ^= 1; }
+            }
+        }
+    } else if (warp >= 8) {
+        // ---------------- key planes: the B tile of every stage, gathered from
+        // the key table.  Unit = (slot sl, 8-query group q8, 4 consecutive u
+        // = steps w0, w0+1 x digits j = 0, 1): both digits of a step share the
+        // permuted position, so 2 permutations and 4 sector loads; bytes are
+        // regrouped into one 32-bit word per (query, byte plane) covering the
+        // 4 u.  Lanes take consecutive u groups, so a warp's stores hit 32
+        // distinct banks.  The stage of K tile kt of the n-th item is
+        // n * ktiles + kt in the producer's sequence (slot and phase follow).
+        //
+        // Groups take K tiles round robin, so a group can run ahead of the MMA
+        // by its stride of stages; an mbarrier parity wait tells the awaited
+        // phase apart from one two phases older only if the group's stride
+        // is <= the stage count.  So at most min(kKeyGroups, S) groups fill
+        // stages; the others only follow the item ring.
+        const int kid = (warp - 8) * 32 + lane;
+        const int grp = kid / kKeyGroup, gk = kid % kKeyGroup;
+        const int ngrp = S < kKeyGroups ? S : kKeyGroups;
+        const int units = P.spi * P.w8 * 32;
+        const int W = 8 * P.w8;
+        int base = 0;  // stages issued before this item
+        for (int it = 0;; ++it, base += ktiles) {
+            const int r = it % kRing;
+            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 19)) { abort_flag = 1; break; }
+            const int item = item_ring[r];
+            mbar_arrive(&iempty[r]);
+            if (item < 0) break;
+            const int li0 = (item / P.n_mg) * P.spi;
+            const int l = li0 / kN;
+            const uint32_t* kl = P.keyt + (size_t)l * kDeff * kN * W;  // [j][p][W]
+            for (int kt = grp; grp < ngrp && kt < ktiles; kt += ngrp) {
+                const int seq = base + kt, s = seq % S;
+                const uint32_t ph = (uint32_t)(seq / S) & 1;
+                if (!mbar_wait(&empty[s], ph ^ 1, P.err, 20)) { abort_flag = 1; break; }
+                uint8_t* bt = smem + (size_t)s * stage_bytes + a_region;
+                for (int unit = gk; unit < units; unit += kKeyGroup) {
+                    const int u4 = unit & 31, sq = unit >> 5;
+                    const int sl = sq / P.w8, q8 = sq - sl * P.w8;
+                    const uint32_t odd = 2 * brev11((uint32_t)((li0 + sl) & (kN - 1))) + 1;
+                    const int w0 = kt * 64 + u4 * 2;  // even: w0 and w0 + 1 both < 2046 or both not
+                    uint32_t v[4][8];
+                    if (w0 < 2 * kSteps) {
+                        const uint2 tt = *reinterpret_cast<const uint2*>(&tw[w0]);
+                        const uint32_t p0 = perm_from_odd(tt.x, odd), p1 = perm_from_odd(tt.y, odd);
+                        ld_sector(kl + (size_t)p0 * W + 8 * q8, v[0]);          // w0, j = 0
+                        ld_sector(kl + ((size_t)kN + p0) * W + 8 * q8, v[1]);   // w0, j = 1
+                        ld_sector(kl + (size_t)p1 * W + 8 * q8, v[2]);          // w0 + 1, j = 0
+                        ld_sector(kl + ((size_t)kN + p1) * W + 8 * q8, v[3]);   // w0 + 1, j = 1
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) v[e][c] = 0;
+                    }
+                    const uint32_t col = (uint32_t)u4 * 4;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const int q = q8 * 8 + c;
+                        if (q >= P.nq) break;
+                        const uint32_t lo01 = __byte_perm(v[0][c], v[1][c], 0x5140);
+                        const uint32_t lo23 = __byte_perm(v[2][c], v[3][c], 0x5140);
+                        const uint32_t hi01 = __byte_perm(v[0][c], v[1][c], 0x7362);
+                        const uint32_t hi23 = __byte_perm(v[2][c], v[3][c], 0x7362);
+                        const uint32_t row0 = (uint32_t)(sl * P.rq + q * 4);
+                        st_sw128(bt, row0 + 0, col, __byte_perm(lo01, lo23, 0x5410));  // byte 0 of u..u+3
+                        st_sw128(bt, row0 + 1, col, __byte_perm(lo01, lo23, 0x7632));  // byte 1
+                        st_sw128(bt, row0 + 2, col, __byte_perm(hi01, hi23, 0x5410));  // byte 2
+                        st_sw128(bt, row0 + 3, col, __byte_perm(hi01, hi23, 0x7632));  // byte 3
+                    }
+                }
+                // generic-proxy stores -> visible to the tensor core's async proxy
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(&full[s]);
             }
         }
     } else if (warp >= 4) {
@@ -390,7 +471,7 @@ uint32_t powmod_host(uint64_t b, uint64_t e, uint64_t q) {
 }  // namespace
 
 size_t tp_dt_bytes(size_t groups) { return (size_t)2 * kN * 4 * groups * kUPad; }
-size_t tp_gt_bytes(int max_pass) { return (size_t)2 * kN * 4 * (size_t)max_pass * kUPad; }
+size_t tp_keyt_bytes(int max_pass) { return (size_t)2 * kDeff * kN * 8 * (size_t)((max_pass + 7) / 8) * 4; }
 
 int tp_pass_queries(size_t groups) {
     // queries per GEMM pass so that the accumulators fit TMEM (512 columns)
@@ -414,12 +495,14 @@ cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp
 }
 
 cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
-                               int nq_total, int q0, uint8_t* Gt, uint32_t* tp_out, int* err, unsigned* tiles,
+                               int nq_total, int q0, uint32_t* keyt, uint32_t* tp_out, int* err, unsigned* tiles,
                                int num_sms, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
     if (nq > 32 || !tiles) return cudaErrorInvalidValue;
     const int rq = 4 * nq;
-    gen_g_kernel<<<dim3(kN / 8, nq, 2), 256, 0, s>>>(keys, key_qstride, Gt, rq);
+    const int W = 8 * ((nq + 7) / 8);
+    const size_t kt_n = (size_t)2 * kDeff * kN * W;
+    keyt_kernel<<<(unsigned)((kt_n + 255) / 256), 256, 0, s>>>(keys, key_qstride, nq, W, keyt);
     cudaError_t e = cudaGetLastError();
     if (e) return e;
     TpParams P{};
@@ -428,6 +511,8 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     P.q0 = q0;
     P.nq = nq;
     P.rq = rq;
+    P.w8 = W / 8;
+    P.keyt = keyt;
     P.G = (int)G;
     const int nmt = (int)std::max<size_t>(1, (4 * G + 127) / 128);
     P.mti = std::min(nmt, 4);
@@ -460,16 +545,14 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     const size_t stage_bytes = a_region + (size_t)P.nb * 128;
     P.stages = (int)std::min<size_t>(8, (200 * 1024) / stage_bytes);
     if (P.stages < 2) return cudaErrorInvalidValue;
-    CUtensorMap ma, mb;
+    CUtensorMap ma;
     if (!make_map(&ma, Dt, (uint64_t)2 * kN * 4 * G, (uint32_t)P.rows_box)) return cudaErrorInvalidValue;
-    // Box rows past the last slot's keys read zeros (TMA out-of-range fill).
-    if (!make_map(&mb, Gt, (uint64_t)2 * kN * rq, (uint32_t)P.nb)) return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
     e = allow_max_smem(tp_tc_kernel);
     if (e) return e;
     const int items = (2 * kN / P.spi) * P.n_mg;
     if ((e = cudaMemsetAsync(tiles, 0, sizeof(unsigned), s))) return e;
-    tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), 256, smem, s>>>(ma, mb, P);
+    tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), kTpThreads, smem, s>>>(ma, P);
     return cudaGetLastError();
 }
 

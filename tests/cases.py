@@ -50,4 +50,6 @@ def get_case(name):
         return Case(524288, 120, 2048, crs=7)
     if name == "cfg1":       # setup(65536, w=30): 32768 x 2048, CRS seed 1, DB seed 0
         return Case(65536, 30, 0, crs=1, db_seed=0)
+    if name == "g128":       # 2048 x 262144 (1 GB DB), G = 128: the 16 GB geometry's group count
+        return Case(8388608, 120, 2048, crs=3, db_seed=5)
     raise KeyError(name)
