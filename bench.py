@@ -56,7 +56,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="batch", choices=["batch", "serve"])
+    ap.add_argument("--mode", default="batch", choices=["batch", "serve", "matvec"])
+    ap.add_argument("--mv-entries", type=int, default=1 << 31,
+                    help="matvec mode: setup(N, 30) sizes the DB (2^31: 32768 x 1048576 u16 = 68.7 GB)")
+    ap.add_argument("--mv-batches", default="1,16,32,64,128,256")
     ap.add_argument("--n-entries", type=int, default=1 << 29)
     ap.add_argument("--entry-bytes", type=int, default=30)
     ap.add_argument("--batch", type=int, default=32)
@@ -577,6 +580,113 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def splitmix_mod(idx, seed):
+    """Host copy of the synthetic DB formula on an index array (u64)."""
+    with np.errstate(over="ignore"):
+        x = (idx ^ np.uint64(seed)) + np.uint64(0x9e3779b97f4a7c15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xbf58476d1ce4e5b9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94d049bb133111eb)
+        x ^= x >> np.uint64(31)
+    return x % np.uint64(65535)
+
+
+def run_matvec(args):
+    """Exact mat-vec microbench: DB x B queries on the tensor cores and on the
+    CUDA cores, each B's schedule autotuned, sampled columns checked against
+    exact host dot products."""
+    import torch
+    import inspire_b200 as ib
+    torch.cuda.set_device(0)
+    params = ib.setup(args.mv_entries, 30)
+    R, Cc = params["db_rows"], params["db_cols"]
+    db_seed, q_seed = 0, 5
+    db = torch.empty(R * Cc, dtype=torch.int16, device="cuda")
+    ib.fill_db_device(db.data_ptr(), R * Cc, db_seed)
+    Bs = [int(x) for x in args.mv_batches.split(",")]
+    Bmax = max(Bs)
+    rng = np.random.default_rng(q_seed)
+    qh = np.empty((Bmax, 2, R), np.uint64)
+    qh[:, 0, :] = rng.integers(0, Q[0], (Bmax, R), dtype=np.uint64)
+    qh[:, 1, :] = rng.integers(0, Q[1], (Bmax, R), dtype=np.uint64)
+    q = torch.from_numpy(qh.view(np.int64).reshape(-1)).cuda()
+    out = torch.empty(Bmax * 2 * Cc, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    db_bytes = R * Cc * 2
+    hbm_peak, peak_kind = measured_peaks()
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            int8_peak = 2 * float(json.load(f)["bf16_tflops"])   # dense int8 = 2x dense bf16 (4.5 vs 2.25 P nominal)
+        int8_kind = "2 x measured bf16 GEMM"
+    except Exception:
+        int8_peak, int8_kind = 4500.0, "nominal"
+    # sampled columns for the exact check (the host regenerates them)
+    cs = np.sort(np.random.default_rng(1).choice(Cc, 24, replace=False)).astype(np.uint64)
+    rows_idx = np.arange(R, dtype=np.uint64)[:, None] * np.uint64(Cc)
+    dcols = splitmix_mod(rows_idx + cs[None, :], db_seed)          # (R, 24) u64, < 2^16
+
+    def timed(B, path, qpp, kc, reps):
+        ib.matvec_ex(db.data_ptr(), R, Cc, q.data_ptr(), B, out.data_ptr(), path, qpp, kc, sh, True)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            ib.matvec_ex(db.data_ptr(), R, Cc, q.data_ptr(), B, out.data_ptr(), path, qpp, kc, sh, False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def check(B):
+        oh = out[:B * 2 * Cc].cpu().numpy().view(np.uint32).reshape(B, 2, Cc)
+        bad = 0
+        for l, mod in enumerate(Q):
+            exp = (qh[:B, l, :] @ dcols) % np.uint64(mod)             # exact: sums < 2^59
+            bad += int((oh[:, l, cs.astype(np.int64)].astype(np.uint64) != exp).sum())
+        return bad
+
+    results = {}
+    for B in Bs:
+        row = {}
+        for path in (0, 1):
+            if path == 0:
+                qpps = sorted({min(B, 32)} | ({16, 8} if B > 16 else set()) | ({B} if B < 32 else set()))
+                kcs = [0] + [k for k in (8192, 16384) if R % k == 0 and k < R]
+            else:
+                qpps, kcs = [min(B, 4)], [0]
+            best = None
+            for qpp in qpps:
+                for kc in kcs:
+                    passes = -(-B // qpp)
+                    reps = max(1, min(5, int(4000 / (passes * (12 if path == 0 else 60)))))
+                    ms = timed(B, path, qpp, kc, reps)
+                    if best is None or ms < best[0]:
+                        best = (ms, qpp, kc)
+            ms, qpp, kc = best
+            ib.matvec_ex(db.data_ptr(), R, Cc, q.data_ptr(), B, out.data_ptr(), path, qpp, kc, sh, True)
+            torch.cuda.synchronize()
+            passes = -(-B // qpp)
+            ops = 2 * 16 * B * R * Cc           # 8 query planes x 2 DB bytes per (row, col), 2 ops per MAC
+            d = {"ms": ms, "q_per_s": B * 1e3 / ms, "db_passes": passes,
+                 "hbm_gbs": passes * db_bytes / (ms * 1e-3) / 1e9,
+                 "hbm_frac": passes * db_bytes / (ms * 1e-3) / 1e9 / hbm_peak,
+                 "schedule": {"queries_per_pass": qpp, "kchunk_rows": kc or "auto"},
+                 "sampled_mismatches": check(B)}
+            if path == 0:
+                d["int8_tops"] = ops / (ms * 1e-3) / 1e12
+                d["int8_frac"] = d["int8_tops"] / int8_peak
+            row["tensor_cores" if path == 0 else "cuda_cores"] = d
+        results[str(B)] = row
+    line = {"metric": "exact mat-vec microbench: ms, q/s, HBM GB/s and int8 TOPS per batch (tensor vs CUDA cores)",
+            "mode": "matvec", "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": f"setup(2^{args.mv_entries.bit_length() - 1}, w=30): {R} x {Cc} u16 DB "
+                                   f"({db_bytes / 1e9:.1f} GB, splitmix64 seed {db_seed}), queries uniform in [0, q) "
+                                   f"per limb (seed {q_seed})",
+                       "check": "24 sampled columns x all queries x both limbs vs exact host dot products"},
+            "peaks": {"hbm_gbs": hbm_peak, "hbm_source": peak_kind, "int8_tops": int8_peak, "int8_source": int8_kind},
+            "results": results,
+            "bit_exact": all(v[p]["sampled_mismatches"] == 0 for v in results.values() for p in v)}
+    print(json.dumps(line), flush=True)
+
+
 def C_wait(loop, ticket, out):
     import inspire_b200 as ib
     try:
@@ -593,6 +703,10 @@ def main():
         rank, _, _ = dist_env()
         if rank == 0:
             run_serve(args)
+    elif args.mode == "matvec":
+        rank, _, _ = dist_env()
+        if rank == 0:
+            run_matvec(args)
     else:
         run_ours(args)
 

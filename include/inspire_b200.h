@@ -155,6 +155,18 @@ int ipir_b200_expand_seed(const uint8_t* seed64, const char* domain, uint64_t in
 int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
                      uint32_t* out, void* stream, int sync);
 
+/* Schedule of one ipir_b200_matvec_ex call.  Zero fields take the defaults. */
+typedef struct {
+    int path;             /* 0: tcgen05 int8 tensor cores (default), 1: CUDA cores (cols a multiple of 2048) */
+    int queries_per_pass; /* queries sharing one DB pass: 1..32 (tensor cores, default 32), 1..4 (CUDA cores) */
+    int kchunk_rows;      /* tensor cores: rows per exact s32 accumulation, a multiple of 1024 dividing rows and
+                             <= 32768 (default: the largest that still gives every SM work) */
+} ipir_matvec_opts;
+/* ipir_b200_matvec with an explicit kernel schedule (opts may be NULL);
+ * every schedule gives the same result.  No counterpart in the reference. */
+int ipir_b200_matvec_ex(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
+                        uint32_t* out, void* stream, int sync, const ipir_matvec_opts* opts);
+
 /* Same result as ipir_b200_matvec, for callers that may not allocate device
  * memory: processes whose device memory belongs to an allocator or pool they
  * must not bypass, or code that cannot afford cudaMalloc's implicit device
@@ -176,6 +188,8 @@ int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t cols, const
 /* Synthetic database for benchmarks and tests: out[k] = splitmix64(seed ^ k)
  * mod 65535 for k < count, filled on all host threads. */
 int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed);
+/* Same values written by a kernel into device memory (enqueued on stream). */
+int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* stream);
 
 /* Kernel schedule for one batch size: mat-vec on the tensor cores
  * (matvec_tc = 1) or the CUDA cores (0); queries per tensor-pass GEMM

@@ -96,6 +96,9 @@ cudaError_t launch_collapse_final(const uint32_t* ends, const uint32_t* kn1, con
                                   uint32_t* df, uint32_t* pre_a, size_t ngroups, cudaStream_t s);
 
 // ---------------------------------------------------------------- primitives
+// out[k] = splitmix64(seed ^ k) mod 65535 for k < count (the host
+// ipir_b200_fill_db formula), on the device.
+cudaError_t launch_fill_db(uint16_t* out, size_t count, uint64_t seed, cudaStream_t s);
 // In-place forward/inverse NTT of n polys of N u32 (< q); limb of poly i is
 // (i / limb_run) & 1.
 cudaError_t launch_ntt_batch(uint32_t* polys, size_t n, int limb_run, bool inverse,

@@ -9,6 +9,8 @@
 //   horner    one persistent CTA per response ciphertext runs the whole
 //             ExtProd chain (INTT, decomp, NTT, MAC) in shared memory
 // All arithmetic is exact mod q_l, so every output equals the reference's.
+#include <algorithm>
+
 #include "ipb_common.cuh"
 #include "host_util.h"
 #include "ipb_launch.h"
@@ -456,7 +458,27 @@ __global__ void decomp_kernel(const uint32_t* __restrict__ in, uint32_t* __restr
     o[(1 * 2 + 1) * kN + x] = signed_res(s2, kQ1);
 }
 
+__global__ void __launch_bounds__(256) fill_db_kernel(uint16_t* __restrict__ out, size_t count, uint64_t seed) {
+    for (size_t k = (size_t)blockIdx.x * 256 + threadIdx.x; k < count; k += (size_t)gridDim.x * 256) {
+        uint64_t x = (seed ^ k) + 0x9e3779b97f4a7c15ULL;
+        x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+        x ^= x >> 31;
+        out[k] = (uint16_t)(x % 65535u);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_fill_db(uint16_t* out, size_t count, uint64_t seed, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t blocks = std::min<size_t>((count + 255) / 256, (size_t)sms * 16);
+    fill_db_kernel<<<(unsigned)blocks, 256, 0, s>>>(out, count, seed);
+    return cudaGetLastError();
+}
 
 // ==================================================================== wrappers
 cudaError_t launch_qprep(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,

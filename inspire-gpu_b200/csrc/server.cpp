@@ -871,13 +871,31 @@ std::mutex g_mv_mu;
 MvScratch g_mv[64];
 }  // namespace
 
-int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
-                     uint32_t* out, void* stream, int sync) {
+int ipir_b200_matvec_ex(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
+                        uint32_t* out, void* stream, int sync, const ipir_matvec_opts* opts) {
     if (!db || !queries || !out) return 1;
     if (count == 0) return 0;
-    if (rows == 0 || rows % 1024 || cols == 0 || cols % 128 || (rows > 32768 && rows % 32768)) {
+    ipir_matvec_opts o{};
+    if (opts) o = *opts;
+    const bool cores = o.path == 1;
+    if (o.path != 0 && o.path != 1) {
+        ipb::g_last_error = "ipir_b200_matvec_ex: path must be 0 (tensor cores) or 1 (CUDA cores)";
+        return 2;
+    }
+    if (rows == 0 || rows % 1024 || cols == 0 || cols % (cores ? 2048 : 128) || (rows > 32768 && rows % 32768)) {
         ipb::g_last_error = "ipir_b200_matvec: rows must be a multiple of 1024 (of 32768 above 32768), "
-                            "cols a multiple of 128";
+                            "cols a multiple of 128 (2048 on the CUDA-core path)";
+        return 2;
+    }
+    const int max_pass = cores ? 4 : 32;
+    const int qpp = o.queries_per_pass ? o.queries_per_pass : max_pass;
+    if (qpp < 1 || qpp > max_pass) {
+        ipb::g_last_error = "ipir_b200_matvec_ex: queries_per_pass out of range";
+        return 2;
+    }
+    if (!cores && o.kchunk_rows &&
+        (o.kchunk_rows % 1024 || o.kchunk_rows > 32768 || rows % (size_t)o.kchunk_rows)) {
+        ipb::g_last_error = "ipir_b200_matvec_ex: kchunk_rows must be a multiple of 1024 dividing rows, <= 32768";
         return 2;
     }
     return guarded(
@@ -896,27 +914,43 @@ int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_
                 IPB_CK(cudaMemset(M.err, 0, sizeof(int)));
                 IPB_CK(cudaDeviceSynchronize());  // tables visible to any stream
             }
-            const size_t kchunk = rows < 32768 ? rows : 32768;
+            // exact K-chunks: tensor cores accumulate s32 over <= 32768 rows, the
+            // CUDA cores stage <= 4096 rows of query words per CTA
+            size_t kchunk;
+            if (cores) {
+                kchunk = std::min<size_t>(rows, 4096);
+                while (kchunk > 1024 && (cols / 2048) * (rows / kchunk) < (size_t)(4 * sms)) kchunk /= 2;
+            } else {
+                kchunk = o.kchunk_rows ? (size_t)o.kchunk_rows : (size_t)ipb::matvec_tc_kchunk_rows(rows, cols, sms);
+            }
             const int chunks = (int)(rows / kchunk);
-            const size_t pbytes = ipb::mv_tc_planes_bytes(rows, (int)count);
-            if (pbytes > M.planes_cap) {
-                M.planes = M.arena.alloc<uint8_t>(pbytes);
-                M.planes_cap = pbytes;
+            const size_t pq = (size_t)chunks * 2 * cols;  // partials of one query
+            if (chunks > 1 && pq * qpp > M.part_cap) {
+                M.part = M.arena.alloc<uint32_t>(pq * qpp);
+                M.part_cap = pq * qpp;
             }
-            const size_t pq = (size_t)chunks * 2 * cols;
-            if (chunks > 1 && pq * count > M.part_cap) {
-                M.part = M.arena.alloc<uint32_t>(pq * count);
-                M.part_cap = pq * count;
+            if (!cores) {
+                const size_t pbytes = ipb::mv_tc_planes_bytes(rows, (int)count);
+                if (pbytes > M.planes_cap) {
+                    M.planes = M.arena.alloc<uint8_t>(pbytes);
+                    M.planes_cap = pbytes;
+                }
+                IPB_CK(ipb::launch_qplanes(queries, 2 * rows, rows, M.T, M.planes, (int)count, s));
             }
-            IPB_CK(ipb::launch_qplanes(queries, 2 * rows, rows, M.T, M.planes, (int)count, s));
-            for (size_t q0 = 0; q0 < count; q0 += 32) {
-                const int n = (int)std::min<size_t>(32, count - q0);
-                uint32_t* dst = chunks == 1 ? out + q0 * 2 * cols : M.part + q0 * pq;
-                IPB_CK(ipb::launch_matvec_tc(db, rows, cols, M.planes + 8 * q0 * rows, n, M.T, dst,
-                                             chunks == 1 ? 2 * cols : pq, M.err, M.tiles, sms, (int)kchunk, s));
+            for (size_t q0 = 0; q0 < count; q0 += (size_t)qpp) {
+                const int n = (int)std::min<size_t>((size_t)qpp, count - q0);
+                uint32_t* dst = chunks == 1 ? out + q0 * 2 * cols : M.part;
+                const size_t dst_qstride = chunks == 1 ? 2 * cols : pq;
+                if (cores)
+                    IPB_CK(ipb::launch_matvec(db, rows, cols, chunks, queries + q0 * 2 * rows, 2 * rows, M.T, dst,
+                                              dst_qstride, n, s));
+                else
+                    IPB_CK(ipb::launch_matvec_tc(db, rows, cols, M.planes + 8 * q0 * rows, n, M.T, dst, dst_qstride,
+                                                 M.err, M.tiles, sms, (int)kchunk, s));
+                if (chunks > 1)
+                    IPB_CK(ipb::launch_mv_chunk_reduce(M.part, pq, chunks, cols, M.T, out + q0 * 2 * cols, 2 * cols, n,
+                                                       s));
             }
-            if (chunks > 1)
-                IPB_CK(ipb::launch_mv_chunk_reduce(M.part, pq, chunks, cols, M.T, out, 2 * cols, (int)count, s));
             if (sync) {
                 IPB_CK(cudaStreamSynchronize(s));
                 int e = 0;
@@ -927,6 +961,22 @@ int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_
                     return 5;
                 }
             }
+            return 0;
+        },
+        4);
+}
+
+int ipir_b200_matvec(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries, size_t count,
+                     uint32_t* out, void* stream, int sync) {
+    return ipir_b200_matvec_ex(db, rows, cols, queries, count, out, stream, sync, nullptr);
+}
+
+int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* stream) {
+    if (!out && count) return 1;
+    if (count == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            IPB_CK(ipb::launch_fill_db(out, count, seed, static_cast<cudaStream_t>(stream)));
             return 0;
         },
         4);

@@ -112,6 +112,13 @@ class IpirServeCounters(C.Structure):
                 ("queued", C.c_size_t), ("free_slots", C.c_size_t), ("max_notice_ms", C.c_double)]
 
 
+class IpirMatvecOpts(C.Structure):
+    _fields_ = [("path", C.c_int), ("queries_per_pass", C.c_int), ("kchunk_rows", C.c_int)]
+
+
+_L.ipir_b200_matvec_ex.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
+                                   C.c_void_p, C.c_int, C.POINTER(IpirMatvecOpts)]
+_L.ipir_b200_fill_db_device.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, C.c_void_p]
 _L.ipir_b200_autotune.argtypes = [C.c_void_p]
 _L.ipir_b200_get_schedule.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirSchedule)]
 _L.ipir_b200_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
@@ -144,7 +151,8 @@ EXPORTED = [
     "ipir_b200_decomp", "ipir_b200_shake256", "ipir_b200_expand_seed", "ipir_b200_fill_db",
     "ipir_b200_matvec", "ipir_b200_matvec_noalloc", "ipir_b200_autotune", "ipir_b200_get_schedule",
     "ipir_b200_launch_count", "ipir_serve_create", "ipir_serve_submit", "ipir_serve_poll", "ipir_serve_wait",
-    "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy",
+    "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy", "ipir_b200_matvec_ex",
+    "ipir_b200_fill_db_device",
 ]
 
 
@@ -502,6 +510,24 @@ def matvec(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0, sync=True)
                              C.c_void_p(out_ptr), C.c_void_p(stream or 0), 1 if sync else 0)
     if rc:
         raise InspireError(f"ipir_b200_matvec rc={rc}: {last_error()}")
+
+
+def matvec_ex(db_ptr, rows, cols, queries_ptr, count, out_ptr, path=0, queries_per_pass=0, kchunk_rows=0,
+              stream=0, sync=True):
+    """ipir_b200_matvec_ex: the mat-vec with an explicit schedule (path 0 =
+    tensor cores, 1 = CUDA cores); device pointers as in matvec()."""
+    o = IpirMatvecOpts(path, queries_per_pass, kchunk_rows)
+    rc = _L.ipir_b200_matvec_ex(C.c_void_p(db_ptr), rows, cols, C.c_void_p(queries_ptr), count, C.c_void_p(out_ptr),
+                                C.c_void_p(stream or 0), 1 if sync else 0, C.byref(o))
+    if rc:
+        raise InspireError(f"matvec_ex rc={rc}: {last_error()}")
+
+
+def fill_db_device(ptr, count, seed, stream=0):
+    """Device-side fill_db (same values) into device memory at ptr."""
+    rc = _L.ipir_b200_fill_db_device(C.c_void_p(ptr), count, seed, C.c_void_p(stream or 0))
+    if rc:
+        raise InspireError(f"fill_db_device rc={rc}: {last_error()}")
 
 
 def matvec_noalloc_rc(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0):
