@@ -67,10 +67,12 @@ cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_
                           const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                           size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s);
 
-// Same on a cluster of four CTAs per chain (one per polynomial and limb).
+// Same on a cluster of four CTAs per chain (one per polynomial and limb);
+// *err receives a nonzero code if a wait for a peer's data times out.
 cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
-                                  size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s);
+                                  size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
+                                  cudaStream_t s);
 
 // ---------------------------------------------------------------- preprocess
 // Encode pass over the rows [0, nrows) of a chunk: levels [l0, l0+nl) of the

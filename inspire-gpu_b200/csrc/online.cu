@@ -294,15 +294,19 @@ __global__ void __launch_bounds__(1024, 1) horner_kernel(const uint32_t* __restr
 // The same chain on a cluster of four CTAs, CTA rank r = 2p + l owning
 // polynomial p (0 = a, 1 = b) in limb l.  Each CTA has two NTT groups:
 // group 0 holds the accumulator and runs the inverse NTT; both groups then
-// decompose (CRT needs the partner limb's coefficients, received through
-// distributed shared memory) and transform one gadget digit each; each
-// digit is multiplied by the RGSW rows of its polynomial (held in registers
-// for the whole chain), the contribution to the other polynomial is stored
-// into that CTA's shared memory, and group 0 sums.  Two cluster barriers per
-// step; the four SMs share the NTT work and only two NTTs sit on the
-// critical path.  Shared buffers alternate with the step parity.
+// decompose (CRT needs the partner limb's coefficients) and transform one
+// gadget digit each; each digit is multiplied by the RGSW rows of its
+// polynomial (held in registers for the whole chain), the contribution to
+// the own polynomial stays local, the one to the other polynomial goes to
+// that CTA, and group 0 sums.  Remote data moves with st.async into the
+// receiver's shared memory and completes bytes on the receiver's mbarrier
+// (partner coefficients: 8 KB per step; other-poly contributions: 16 KB per
+// step), so the loop has no cluster-wide barrier.  Buffers alternate with
+// the step parity; a remote write for step t is issued only after its
+// receiver has finished reading the same buffer at step t - 2 (it depends on
+// data the receiver sent after that read).  Every wait is bounded.
 constexpr size_t kHornerClSmem =
-    2 * kN * sizeof(uint2) + (2 * 2 * kN + 2 * 2 * kN + 2 * 4 * kN) * sizeof(uint32_t);
+    2 * kN * sizeof(uint2) + (2 * 2 * kN + 2 * 2 * kN + 2 * 4 * kN) * sizeof(uint32_t) + 64;
 
 __device__ __forceinline__ uint32_t cluster_rank() {
     uint32_t r;
@@ -319,24 +323,54 @@ __device__ __forceinline__ uint32_t map_peer(const void* local, uint32_t rank) {
                  : "r"((uint32_t)__cvta_generic_to_shared(local)), "r"(rank));
     return r;
 }
-__device__ __forceinline__ void st_peer4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    asm volatile("st.shared::cluster.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d)
+// 16 bytes into a peer CTA's shared memory, completing 16 bytes on its mbarrier.
+__device__ __forceinline__ void st_async4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                                          uint32_t mbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+                     addr),
+                 "r"(a), "r"(b), "r"(c), "r"(d), "r"(mbar)
                  : "memory");
 }
-__device__ __forceinline__ void st_peer(uint32_t addr, uint32_t v) {
-    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+__device__ __forceinline__ void hb_init(uint64_t* b) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(b)));
+}
+__device__ __forceinline__ void hb_expect(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(b)),
+                 "r"(bytes)
+                 : "memory");
+}
+// Bounded wait on a cluster-filled mbarrier phase; false (and *err set) on timeout.
+__device__ __forceinline__ bool hb_wait(uint64_t* b, uint32_t parity, int* err, int code) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(b);
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    atomicCAS(err, 0, code);
+    return false;
 }
 
 __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     horner_cl_kernel(const uint32_t* __restrict__ pre_a, const uint32_t* __restrict__ packed_b, size_t pb_qstride,
                      const uint32_t* __restrict__ rgsw32, const DevTables* __restrict__ T, size_t groups,
-                     size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride) {
+                     size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride, int* err) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint2* twf = reinterpret_cast<uint2*>(smem);
     uint2* twi = twf + kN;
     uint32_t* nbuf = reinterpret_cast<uint32_t*>(twi + kN);   // [2 groups][2][N]
     uint32_t* xc = nbuf + 2 * 2 * kN;                         // [parity][own | partner limb][N]
     uint32_t* cin = xc + 2 * 2 * kN;                          // [parity][local j0 | local j1 | peer j0 | peer j1][N]
+    uint64_t* mbx = reinterpret_cast<uint64_t*>(cin + 2 * 4 * kN);  // [parity] partner coefficients
+    uint64_t* mbc = mbx + 2;                                         // [parity] other-poly contributions
+    __shared__ volatile int abort_flag;
     const uint32_t rank = cluster_rank();
     const int p = (int)(rank >> 1), l = (int)(rank & 1);
     const int ct = blockIdx.x >> 2, b = blockIdx.y;
@@ -346,6 +380,11 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     const LimbTables& L = T->limb[l];
     const uint32_t q = L.q;
     for (int i = threadIdx.x; i < kN; i += 512) { twf[i] = L.fwd[i]; twi[i] = L.inv[i]; }
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int k = 0; k < 2; ++k) { hb_init(&mbx[k]); hb_init(&mbc[k]); }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     const uint32_t rank_limb = (uint32_t)((p << 1) | (1 - l));   // same poly, other limb
     const uint32_t rank_poly = (uint32_t)(((1 - p) << 1) | l);   // other poly, same limb
     const size_t start = (size_t)ct * d_act;
@@ -361,24 +400,40 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     ld8(rg + (size_t)(((2 * p + (1 - p)) * kDeff + gp) * 2 + l) * kN + 8 * t, r_oth);
     uint32_t acc[8];
     if (gp == 0) ld8(src_of(start + len - 1) + 8 * t, acc);
-    cluster_sync_all();  // every CTA of the cluster is running before any remote access
-    int par = 0;
-    for (long i = (long)len - 2; i >= 0; --i, par ^= 1) {
+    cluster_sync_all();  // every CTA runs and its mbarriers are initialised before any remote access
+    const uint32_t peer_x = map_peer(xc, rank_limb);       // partner's xc base
+    const uint32_t peer_c = map_peer(cin, rank_poly);      // other poly CTA's cin base
+    const uint32_t peer_mbx = map_peer(mbx, rank_limb);
+    const uint32_t peer_mbc = map_peer(mbc, rank_poly);
+    int step = 0;
+    for (long i = (long)len - 2; i >= 0; --i, ++step) {
+        const int par = step & 1;
+        const uint32_t ph = (uint32_t)(step >> 1) & 1;
         uint32_t* xown = xc + (par * 2 + 0) * kN;
-        uint32_t* xpart = xc + (par * 2 + 1) * kN;
+        const uint32_t* xpart = xc + (par * 2 + 1) * kN;
         uint32_t* cp = cin + (size_t)par * 4 * kN;
+        if (threadIdx.x == 0) {
+            hb_expect(&mbx[par], kN * 4);
+            hb_expect(&mbc[par], 2 * kN * 4);
+        }
         uint32_t pk[8];
         if (gp == 0) {
             ld8(src_of(start + (size_t)i) + 8 * t, pk);
-            ntt_inv(acc, nbuf, twi, q, L.inv_n, L.inv_n_p, t, bar);
-            const uint32_t peer = map_peer(xpart, rank_limb);
+            ntt_inv(acc, nbuf, twi, q, L.inv_n, L.inv_n_p, t, bar);   // acc: index t + 256 e
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                xown[t + 256 * e] = acc[e];
-                st_peer(peer + 4 * (t + 256 * e), acc[e]);
-            }
+            for (int e = 0; e < 8; ++e) xown[t + 256 * e] = acc[e];
         }
-        cluster_sync_all();
+        __syncthreads();  // xown complete; abort_flag is read only here, after a block barrier,
+                          // so every thread takes the same branch
+        if (abort_flag) break;
+        if (gp == 0) {
+            // the partner's copy, sent as the contiguous block 8t..8t+7 (16-byte stores)
+            const uint32_t* src = xown + 8 * t;
+            const uint32_t dst = peer_x + (uint32_t)((par * 2 + 1) * kN + 8 * t) * 4;
+            st_async4(dst, src[0], src[1], src[2], src[3], peer_mbx + 8 * par);
+            st_async4(dst + 16, src[4], src[5], src[6], src[7], peer_mbx + 8 * par);
+        }
+        if (!hb_wait(&mbx[par], ph, err, 31)) abort_flag = 1;
         uint32_t d[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
@@ -395,11 +450,12 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
             eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], L.cr, q);
         }
         st8(cp + (size_t)gp * kN + 8 * t, es);
-        const uint32_t peer = map_peer(cp + (size_t)(2 + gp) * kN + 8 * t, rank_poly);
-        st_peer4(peer, eo[0], eo[1], eo[2], eo[3]);
-        st_peer4(peer + 16, eo[4], eo[5], eo[6], eo[7]);
-        cluster_sync_all();
+        const uint32_t dstc = peer_c + (uint32_t)((size_t)par * 4 * kN + (size_t)(2 + gp) * kN + 8 * t) * 4;
+        st_async4(dstc, eo[0], eo[1], eo[2], eo[3], peer_mbc + 8 * par);
+        st_async4(dstc + 16, eo[4], eo[5], eo[6], eo[7], peer_mbc + 8 * par);
+        __syncthreads();  // local contributions complete
         if (gp == 0) {
+            if (!hb_wait(&mbc[par], ph, err, 32)) abort_flag = 1;
             uint32_t v0[8], v1[8], w0[8], w1[8];
             ld8(cp + 8 * t, v0);
             ld8(cp + kN + 8 * t, v1);
@@ -541,13 +597,14 @@ cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_
 
 cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
-                                  size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, cudaStream_t s) {
+                                  size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
+                                  cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
     cudaError_t e = allow_max_smem(horner_cl_kernel);
     if (e) return e;
     horner_cl_kernel<<<dim3((unsigned)(4 * num_cts), nq), 512, kHornerClSmem, s>>>(pre_a, packed_b, pb_qstride,
                                                                                    rgsw32, T, groups, d_act, resp,
-                                                                                   resp_qstride);
+                                                                                   resp_qstride, err);
     return cudaGetLastError();
 }
 

@@ -333,7 +333,7 @@ static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t co
     if (ev) IPB_CK(cudaEventRecord(ev[4], st));
     if (sc.horner_cluster)
         IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts,
-                                     L.resp, S.resp_qstride, nq, st));
+                                     L.resp, S.resp_qstride, nq, L.d_err, st));
     else
         IPB_CK(launch_horner(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts, L.resp,
                              S.resp_qstride, nq, st));
