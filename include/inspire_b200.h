@@ -193,8 +193,9 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
 
 /* Kernel schedule for one batch size: mat-vec on the tensor cores
  * (matvec_tc = 1) or the CUDA cores (0); queries per tensor-pass GEMM
- * (tp_pass); Horner on a 4-CTA cluster per chain (horner_cluster = 1) or one
- * CTA per chain (0).  Every schedule gives the same responses. */
+ * (tp_pass); Horner on a 4-CTA cluster per chain (horner_cluster = 1), an
+ * 8-CTA cluster (2) or one CTA per chain (0).  Every schedule gives the same
+ * responses. */
 typedef struct {
     int matvec_tc;
     int tp_pass;
@@ -207,6 +208,10 @@ typedef struct {
 int ipir_b200_autotune(ipir_server* srv);
 /* The schedule the handle uses for `count` queries. */
 int ipir_b200_get_schedule(const ipir_server* srv, size_t count, ipir_serve_schedule* out);
+/* Pin the schedule the handle uses for `count` queries (tp_pass at most
+ * the handle's tensor-pass capacity, min(max_batch, 32) or less for large
+ * group counts): 0, 1 null argument, 2 out of range. */
+int ipir_b200_set_schedule(ipir_server* srv, size_t count, const ipir_serve_schedule* sc);
 /* Kernels launched by the handle's answer pipeline since create. */
 int ipir_b200_launch_count(const ipir_server* srv, unsigned long long* out);
 

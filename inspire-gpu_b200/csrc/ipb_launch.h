@@ -73,6 +73,11 @@ cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_
                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                                   size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
                                   cudaStream_t s);
+// Same on a cluster of eight CTAs per chain (polynomial x limb x digit).
+cudaError_t launch_horner_cluster8(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
+                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
+                                   size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
+                                   cudaStream_t s);
 
 // ---------------------------------------------------------------- preprocess
 // Encode pass over the rows [0, nrows) of a chunk: levels [l0, l0+nl) of the

@@ -475,6 +475,138 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     cluster_sync_all();  // no CTA leaves while a peer may still write into its shared memory
 }
 
+// ------------------------------------------------------------------ horner (8-CTA cluster)
+// The chain on a cluster of eight CTAs of 256 threads, CTA rank
+// r = 4p + 2l + j owning polynomial p, limb l and gadget digit j.  Both digit
+// CTAs of (p, l) hold the same accumulator and run its inverse NTT; each
+// sends its coefficients to the other limb's CTA of the same digit (CRT needs
+// both limbs), decomposes and forward-transforms only its digit, and
+// multiplies it by the RGSW rows of its polynomial.  The contribution to its
+// own polynomial goes to the sibling digit CTA, the one to the other
+// polynomial to both digit CTAs of that polynomial; every CTA then sums its
+// own, its sibling's and the two other-polynomial contributions (modular
+// sums of canonical residues: both siblings get the same accumulator).
+// Remote data moves with st.async and completes on the receiver's
+// transaction mbarriers (8 KB of coefficients, 24 KB of contributions per
+// step); buffers alternate with the step parity, and every remote write for
+// step t depends on data its receiver sent after reading the same buffer at
+// step t - 2.  Half the warps per SM of the 4-CTA version, twice the SMs.
+constexpr size_t kHornerCl8Smem =
+    2 * kN * sizeof(uint2) + (2 * kN + 2 * 2 * kN + 2 * 4 * kN) * sizeof(uint32_t) + 64;
+
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
+    horner_cl8_kernel(const uint32_t* __restrict__ pre_a, const uint32_t* __restrict__ packed_b, size_t pb_qstride,
+                      const uint32_t* __restrict__ rgsw32, const DevTables* __restrict__ T, size_t groups,
+                      size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride, int* err) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint2* twf = reinterpret_cast<uint2*>(smem);
+    uint2* twi = twf + kN;
+    uint32_t* nbuf = reinterpret_cast<uint32_t*>(twi + kN);  // [2][N] NTT scratch
+    uint32_t* xc = nbuf + 2 * kN;                            // [parity][own | partner limb][N]
+    uint32_t* cin = xc + 2 * 2 * kN;                         // [parity][own | sibling | other j0 | other j1][N]
+    uint64_t* mbx = reinterpret_cast<uint64_t*>(cin + 2 * 4 * kN);  // [parity] partner coefficients
+    uint64_t* mbc = mbx + 2;                                         // [parity] contributions
+    __shared__ volatile int abort_flag;
+    const uint32_t rank = cluster_rank();
+    const int p = (int)(rank >> 2), l = (int)((rank >> 1) & 1), j = (int)(rank & 1);
+    const int ct = blockIdx.x >> 3, b = blockIdx.y;
+    const uint32_t t = threadIdx.x;
+    const LimbTables& L = T->limb[l];
+    const uint32_t q = L.q;
+    for (int i = threadIdx.x; i < kN; i += 256) { twf[i] = L.fwd[i]; twi[i] = L.inv[i]; }
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int k = 0; k < 2; ++k) { hb_init(&mbx[k]); hb_init(&mbc[k]); }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    const uint32_t rank_limb = (uint32_t)((p << 2) | ((1 - l) << 1) | j);   // same poly and digit, other limb
+    const uint32_t rank_sib = (uint32_t)((p << 2) | (l << 1) | (1 - j));    // same poly and limb, other digit
+    const uint32_t rank_o0 = (uint32_t)(((1 - p) << 2) | (l << 1) | 0);     // other poly, same limb, digit 0
+    const uint32_t rank_o1 = (uint32_t)(((1 - p) << 2) | (l << 1) | 1);     //                        digit 1
+    const size_t start = (size_t)ct * d_act;
+    const size_t len = (start + d_act <= groups) ? d_act : groups - start;
+    const uint32_t* pbq = packed_b + (size_t)b * pb_qstride;
+    auto src_of = [&](size_t i) -> const uint32_t* {
+        return p ? pbq + (i * 2 + l) * kN : pre_a + (i * 2 + l) * kN;
+    };
+    const uint32_t* rg = rgsw32 + (size_t)b * (4 * kDeff * 2 * kN);
+    uint32_t r_self[8], r_oth[8];
+    ld8(rg + (size_t)(((2 * p + p) * kDeff + j) * 2 + l) * kN + 8 * t, r_self);
+    ld8(rg + (size_t)(((2 * p + (1 - p)) * kDeff + j) * 2 + l) * kN + 8 * t, r_oth);
+    uint32_t acc[8];
+    ld8(src_of(start + len - 1) + 8 * t, acc);
+    cluster_sync_all();  // every CTA runs and its mbarriers are initialised before any remote access
+    const uint32_t peer_x = map_peer(xc, rank_limb);
+    const uint32_t peer_mbx = map_peer(mbx, rank_limb);
+    const uint32_t sib_c = map_peer(cin, rank_sib), sib_mbc = map_peer(mbc, rank_sib);
+    const uint32_t o0_c = map_peer(cin, rank_o0), o0_mbc = map_peer(mbc, rank_o0);
+    const uint32_t o1_c = map_peer(cin, rank_o1), o1_mbc = map_peer(mbc, rank_o1);
+    int step = 0;
+    for (long i = (long)len - 2; i >= 0; --i, ++step) {
+        const int par = step & 1;
+        const uint32_t ph = (uint32_t)(step >> 1) & 1;
+        uint32_t* xown = xc + (par * 2 + 0) * kN;
+        const uint32_t* xpart = xc + (par * 2 + 1) * kN;
+        uint32_t* cp = cin + (size_t)par * 4 * kN;
+        if (threadIdx.x == 0) {
+            hb_expect(&mbx[par], kN * 4);
+            hb_expect(&mbc[par], 3 * kN * 4);
+        }
+        uint32_t pk[8];
+        ld8(src_of(start + (size_t)i) + 8 * t, pk);
+        ntt_inv(acc, nbuf, twi, q, L.inv_n, L.inv_n_p, t, 0);   // acc: index t + 256 e
+#pragma unroll
+        for (int e = 0; e < 8; ++e) xown[t + 256 * e] = acc[e];
+        __syncthreads();  // xown complete; abort_flag is read only here, after a block barrier
+        if (abort_flag) break;
+        {
+            const uint32_t* src = xown + 8 * t;
+            const uint32_t dst = peer_x + (uint32_t)((par * 2 + 1) * kN + 8 * t) * 4;
+            st_async4(dst, src[0], src[1], src[2], src[3], peer_mbx + 8 * par);
+            st_async4(dst + 16, src[4], src[5], src[6], src[7], peer_mbx + 8 * par);
+        }
+        if (!hb_wait(&mbx[par], ph, err, 33)) abort_flag = 1;
+        uint32_t d[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const uint32_t own = xown[t + 256 * e], oth = xpart[t + 256 * e];
+            int64_t s1, s2;
+            decomp2(l ? oth : own, l ? own : oth, *T, s1, s2);
+            d[e] = signed_res(j ? s2 : s1, q);
+        }
+        ntt_fwd(d, nbuf, twf, q, t, 0);
+        uint32_t es[8], eo[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            es[e] = mod_u64((uint64_t)d[e] * r_self[e], L.cr, q);
+            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], L.cr, q);
+        }
+        const uint32_t off = (uint32_t)((size_t)par * 4 * kN + 8 * t) * 4;
+        st_async4(sib_c + off + kN * 4, es[0], es[1], es[2], es[3], sib_mbc + 8 * par);
+        st_async4(sib_c + off + kN * 4 + 16, es[4], es[5], es[6], es[7], sib_mbc + 8 * par);
+        const uint32_t off_o = off + (uint32_t)(2 + j) * kN * 4;
+        st_async4(o0_c + off_o, eo[0], eo[1], eo[2], eo[3], o0_mbc + 8 * par);
+        st_async4(o0_c + off_o + 16, eo[4], eo[5], eo[6], eo[7], o0_mbc + 8 * par);
+        st_async4(o1_c + off_o, eo[0], eo[1], eo[2], eo[3], o1_mbc + 8 * par);
+        st_async4(o1_c + off_o + 16, eo[4], eo[5], eo[6], eo[7], o1_mbc + 8 * par);
+        if (!hb_wait(&mbc[par], ph, err, 34)) abort_flag = 1;
+        uint32_t v1[8], w0[8], w1[8];
+        ld8(cp + kN + 8 * t, v1);
+        ld8(cp + 2 * kN + 8 * t, w0);
+        ld8(cp + 3 * kN + 8 * t, w1);
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+            acc[e] = add_mod(add_mod(add_mod(es[e], v1[e], q), add_mod(w0[e], w1[e], q), q), pk[e], q);
+    }
+    if (j == 0) {
+        uint64_t* dst = resp + (size_t)b * resp_qstride + ((size_t)ct * 4 + p * 2 + l) * kN + 8 * t;
+#pragma unroll
+        for (int e = 0; e < 8; e += 2)
+            *reinterpret_cast<ulonglong2*>(dst + e) = make_ulonglong2(acc[e], acc[e + 1]);
+    }
+    cluster_sync_all();  // no CTA leaves while a peer may still write into its shared memory
+}
+
 // ------------------------------------------------------------------ primitives
 __global__ void __launch_bounds__(1024) ntt_batch_kernel(uint32_t* polys, size_t n, int limb_run, bool inverse,
                                                          const DevTables* __restrict__ T) {
@@ -605,6 +737,18 @@ cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_
     horner_cl_kernel<<<dim3((unsigned)(4 * num_cts), nq), 512, kHornerClSmem, s>>>(pre_a, packed_b, pb_qstride,
                                                                                    rgsw32, T, groups, d_act, resp,
                                                                                    resp_qstride, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_horner_cluster8(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
+                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
+                                   size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
+                                   cudaStream_t s) {
+    if (nq <= 0) return cudaSuccess;
+    cudaError_t e = allow_max_smem(horner_cl8_kernel);
+    if (e) return e;
+    horner_cl8_kernel<<<dim3((unsigned)(8 * num_cts), nq), 256, kHornerCl8Smem, s>>>(
+        pre_a, packed_b, pb_qstride, rgsw32, T, groups, d_act, resp, resp_qstride, err);
     return cudaGetLastError();
 }
 

@@ -275,7 +275,8 @@ std::vector<Sched> default_sched(const Server&, size_t cap, int gt_pass) {
     Sched def;
     def.tp_pass = gt_pass;
     if (const char* m = std::getenv("IPB_MATVEC")) def.matvec_tc = std::strcmp(m, "simt") != 0;
-    if (const char* h = std::getenv("IPB_HORNER")) def.horner_cluster = std::strcmp(h, "cta") != 0;
+    if (const char* h = std::getenv("IPB_HORNER"))
+        def.horner_cluster = std::strcmp(h, "cta") == 0 ? 0 : (std::strcmp(h, "cl8") == 0 ? 2 : 1);
     return std::vector<Sched>(cap + 1, def);
 }
 
@@ -331,7 +332,10 @@ static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t co
     const size_t G = pp.n_packed, d_act = std::min(pp.D, G);
     const int nq = (int)count;
     if (ev) IPB_CK(cudaEventRecord(ev[4], st));
-    if (sc.horner_cluster)
+    if (sc.horner_cluster == 2)
+        IPB_CK(launch_horner_cluster8(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts,
+                                      L.resp, S.resp_qstride, nq, L.d_err, st));
+    else if (sc.horner_cluster)
         IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts,
                                      L.resp, S.resp_qstride, nq, L.d_err, st));
     else
@@ -383,10 +387,10 @@ static void fetch(Server* S, size_t count, uint64_t* out) {
 // For batch sizes 1, 2, 4, ... up to the lane's capacity (and the capacity
 // itself) time every candidate schedule end to end on the device -- mat-vec
 // kernel (tcgen05 / CUDA-core; the CUDA-core kernel streams the DB once per
-// 4 queries, so it is tried up to 8), queries per tensor-pass GEMM (the Gt
-// capacity and its half: fewer queries per pass re-read the tensors but
-// double-buffer the accumulators), Horner kernel (cluster / single CTA) --
-// and keep the fastest.  Sizes between two measured ones use the smaller's.
+// 4 queries, so it is tried up to 8), queries per tensor-pass GEMM (the
+// key-table capacity and its half: fewer queries per pass re-read the
+// tensors but double-buffer the accumulators), Horner kernel (4-CTA
+// cluster, 8-CTA cluster, single CTA) -- and keep the fastest.  Sizes between two measured ones use the smaller's.
 std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
     IPB_CK(cudaSetDevice(S.device));
     std::vector<size_t> sizes;
@@ -404,7 +408,7 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
             for (int mv : {1, 0}) {
                 if (!mv && b > 8) continue;
                 for (int p : passes)
-                    for (int h : {1, 0}) cands.push_back(Sched{mv, p, h});
+                    for (int h : {1, 2, 0}) cands.push_back(Sched{mv, p, h});
             }
             float best_ms = 1e30f;
             Sched pick = cands[0];
@@ -757,6 +761,19 @@ int ipir_b200_get_schedule(const ipir_server* srv, size_t count, ipir_serve_sche
     out->matvec_tc = sc.matvec_tc;
     out->tp_pass = sc.tp_pass;
     out->horner_cluster = sc.horner_cluster;
+    return 0;
+}
+
+int ipir_b200_set_schedule(ipir_server* srv, size_t count, const ipir_serve_schedule* sc) {
+    if (!srv || !sc) return 1;
+    ipb::Server* S = srv->s;
+    if (count == 0 || count > S->max_batch) return 2;
+    if (sc->matvec_tc < 0 || sc->matvec_tc > 1 || sc->horner_cluster < 0 || sc->horner_cluster > 2 ||
+        sc->tp_pass < 1 || sc->tp_pass > S->lane.gt_pass) {
+        ipb::g_last_error = "ipir_b200_set_schedule: matvec_tc 0/1, horner_cluster 0/1/2, tp_pass 1..capacity";
+        return 2;
+    }
+    S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster};
     return 0;
 }
 

@@ -84,7 +84,7 @@ struct Precomp {
 struct Sched {
     int matvec_tc = 1;       // 1: tcgen05 int8 mat-vec, 0: CUDA-core mat-vec
     int tp_pass = 32;        // queries per tensor-pass GEMM (<= the lane's Gt capacity)
-    int horner_cluster = 1;  // 1: 4-CTA cluster per chain, 0: one CTA per chain
+    int horner_cluster = 1;  // 1: 4-CTA cluster per chain, 2: 8-CTA cluster, 0: one CTA per chain
 };
 
 // Per-batch device scratch for up to `cap` queries.

@@ -122,6 +122,7 @@ _L.ipir_b200_fill_db_device.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, C.c_
 _L.ipir_b200_autotune.argtypes = [C.c_void_p]
 _L.ipir_b200_get_schedule.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirSchedule)]
 _L.ipir_b200_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
+_L.ipir_b200_set_schedule.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirSchedule)]
 _L.ipir_serve_create.restype = C.c_void_p
 _L.ipir_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, C.POINTER(IpirServeConfig)]
 _L.ipir_serve_submit.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirQueryView), C.POINTER(C.c_uint64)]
@@ -152,7 +153,7 @@ EXPORTED = [
     "ipir_b200_matvec", "ipir_b200_matvec_noalloc", "ipir_b200_autotune", "ipir_b200_get_schedule",
     "ipir_b200_launch_count", "ipir_serve_create", "ipir_serve_submit", "ipir_serve_poll", "ipir_serve_wait",
     "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy", "ipir_b200_matvec_ex",
-    "ipir_b200_fill_db_device",
+    "ipir_b200_fill_db_device", "ipir_b200_set_schedule",
 ]
 
 
@@ -346,6 +347,15 @@ class Server:
         if rc:
             raise InspireError(f"get_schedule rc={rc}")
         return s.as_dict()
+
+    def set_schedule(self, count, matvec_tc=1, tp_pass=None, horner_cluster=1):
+        """Pin the kernel schedule for batches of `count` queries."""
+        self._check()
+        s = IpirSchedule(matvec_tc, tp_pass if tp_pass is not None else self.schedule(count)["tp_pass"],
+                         horner_cluster)
+        rc = _L.ipir_b200_set_schedule(self._h, count, C.byref(s))
+        if rc:
+            raise InspireError(f"set_schedule rc={rc}: {last_error()}")
 
     def launch_count(self):
         """Kernels launched by this handle's answer pipeline so far."""

@@ -72,3 +72,21 @@ def test_capi_error_codes_write_nothing(batch_env):
     assert srv.answer_batch_rc(views, 1, None) == 1          # null output
     assert srv.answer_batch_rc(views, 0, out) == 0           # empty batch is a no-op
     assert (out == 7).all()
+
+
+@pytest.mark.parametrize("horner", [0, 1, 2])
+@pytest.mark.parametrize("matvec_tc", [1, 0])
+def test_every_schedule_gives_the_same_responses(batch_env, horner, matvec_tc):
+    """Each Horner kernel (one CTA, 4-CTA and 8-CTA clusters) and both
+    mat-vec kernels, pinned through ipir_b200_set_schedule, give the
+    oracle-checked single answers."""
+    c, srv, qs, sts = batch_env
+    want = np.stack([srv.answer(q) for q in qs[:4]])
+    for n in (1, 4):
+        srv.set_schedule(n, matvec_tc=matvec_tc, horner_cluster=horner)
+    got = np.stack([srv.answer(q) for q in qs[:2]])
+    assert (got == want[:2]).all()
+    assert (srv.answer_batch(qs[:4]) == want).all()
+    assert (got[0] == c.oracle_answer(qs[0])).all()
+    for n in (1, 4):
+        srv.set_schedule(n, matvec_tc=1, horner_cluster=1)

@@ -73,7 +73,7 @@ def test_mix_equals_alone(env):
     for d in info:
         assert d["lanes"] == 2 and d["max_batch"] == 4
         for c, s in d["schedule"].items():
-            assert s["matvec_tc"] in (0, 1) and s["horner_cluster"] in (0, 1)
+            assert s["matvec_tc"] in (0, 1) and s["horner_cluster"] in (0, 1, 2)
             assert (c + 1) // 2 <= s["tp_pass"] <= 4, (c, s)
 
 
@@ -151,7 +151,7 @@ def test_handle_autotune_keeps_results(env):
     sb.autotune()
     for c in range(1, 5):
         s = sb.schedule(c)
-        assert s["matvec_tc"] in (0, 1) and s["horner_cluster"] in (0, 1) and 1 <= s["tp_pass"] <= 4
+        assert s["matvec_tc"] in (0, 1) and s["horner_cluster"] in (0, 1, 2) and 1 <= s["tp_pass"] <= 4
         # sizes between the measured ones keep the measured split: at most two tensor passes
         assert s["tp_pass"] >= (c + 1) // 2, (c, s)
     qs = [q for d, _, q, _ in reqs if d == 1][:4]
