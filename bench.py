@@ -324,6 +324,8 @@ def run_ours(args):
         for _ in range(steps):
             srv.run(count)
         e1.record(stream)
+        while not e1.query():      # sleep-polling releases the GIL for the clock sampler thread
+            time.sleep(0.0002)
         torch.cuda.synchronize()
         if sampler:
             torch.cuda.nvtx.range_pop()
@@ -371,6 +373,22 @@ def run_ours(args):
         assert rc == 0, ib.last_error()
     t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
     e2e_qps = world * B / t_e2e
+    # e2e with the client library's wire formats: packed queries in (unpacked
+    # on the device), compressed responses out
+    qb, rb, cb = srv.wire_sizes()
+    wq_t = torch.empty(B * qb, dtype=torch.uint8, pin_memory=True)
+    wq = wq_t.numpy()
+    wq[:] = np.random.default_rng(2000 + rank).integers(0, 256, wq.size, dtype=np.uint8)
+    wo_t = torch.empty((B, cb), dtype=torch.uint8, pin_memory=True)
+    wo = wo_t.numpy()
+    for _ in range(args.warmup):
+        srv.answer_wire(wq, B, ib.RESP_COMPRESSED, out=wo)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        srv.answer_wire(wq, B, ib.RESP_COMPRESSED, out=wo)
+    t_wire = max_over_ranks((time.perf_counter() - t0) / args.steps)
     # plain path latency distribution (one query per call, e2e)
     lat = []
     for _ in range(max(args.steps, 20)):
@@ -412,6 +430,9 @@ def run_ours(args):
         "tensor_pass_gbs_b1": tensor_bytes / (st1["collapse"] * 1e-3) / 1e9,
         "e2e": {"value": e2e_qps, "unit": "q/s", "h2d_bytes_per_step": B * qn * 8,
                 "d2h_bytes_per_step": B * rn * 8},
+        "e2e_wire": {"value": world * B / t_wire, "unit": "q/s", "h2d_bytes_per_step": B * qb,
+                     "d2h_bytes_per_step": B * cb,
+                     "formats": "packed queries (53-bit), compressed responses (28/20-bit)"},
         "gpu_launches": launches,
         "clocks": clocks,
     }

@@ -215,6 +215,28 @@ int ipir_b200_set_schedule(ipir_server* srv, size_t count, const ipir_serve_sche
 /* Kernels launched by the handle's answer pipeline since create. */
 int ipir_b200_launch_count(const ipir_server* srv, unsigned long long* out);
 
+/* Wire formats on the GPU: the reference client library's packed query
+ * (ipir_query_pack, 53-bit CRT-combined values), packed response
+ * (ipir_response_pack) and compressed response (ipir_response_compress,
+ * modulus switching to 28 / 20 bits), src/capi_client.cpp:156-385.
+ * wire_sizes gives their per-query byte counts (as ipir_query_packed_bytes,
+ * ipir_response_packed_bytes, ipir_response_compressed_bytes); any out
+ * pointer may be NULL. */
+#define IPIR_B200_RESP_FLAT 0
+#define IPIR_B200_RESP_PACKED 1
+#define IPIR_B200_RESP_COMPRESSED 2
+int ipir_b200_wire_sizes(const ipir_params* params, size_t* query_packed, size_t* response_packed,
+                         size_t* response_compressed);
+/* ipir_answer_batch on packed queries: `packed` holds count queries back to
+ * back (query_packed bytes each, as ipir_query_pack writes them); they cross
+ * PCIe packed and are unpacked on the device.  The responses are written to
+ * out back to back in resp_format: FLAT (ipir_response_u64s u64 each, the
+ * ipir_answer_batch layout), PACKED (response_packed bytes each, identical to
+ * ipir_response_pack of the flat response) or COMPRESSED (response_compressed
+ * bytes each, identical to ipir_response_compress).  Returns 0, 1 null
+ * argument, 2 count > max_batch, 3 unknown format, 4 CUDA failure. */
+int ipir_b200_answer_wire(ipir_server* srv, const uint8_t* packed, size_t count, int resp_format, void* out);
+
 /* ===================================================== part 3: serving loop
  *
  * Continuous batching over one or more resident databases: server handles

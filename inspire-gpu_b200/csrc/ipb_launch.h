@@ -79,6 +79,22 @@ cudaError_t launch_horner_cluster8(const uint32_t* pre_a, const uint32_t* packed
                                    size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
                                    cudaStream_t s);
 
+// ---------------------------------------------------------------- wire codecs (codec.cu)
+// Byte sizes of the client library's formats: packed query, packed
+// response, compressed response (per query).
+size_t wire_query_bytes(size_t rows);
+size_t wire_response_bytes(size_t num_cts);
+size_t wire_compressed_bytes(size_t num_cts);
+// nq packed queries (in_stride bytes apart) -> flat u64 queries.
+cudaError_t launch_query_unpack(const uint8_t* in, size_t in_stride, size_t rows, uint64_t* out, size_t out_stride,
+                                int nq, const DevTables* T, cudaStream_t s);
+// nq flat u64 responses -> packed responses (out_stride bytes apart).
+cudaError_t launch_response_pack(const uint64_t* flat, size_t flat_stride, size_t num_cts, uint8_t* out,
+                                 size_t out_stride, int nq, const DevTables* T, cudaStream_t s);
+// nq flat u64 responses -> compressed responses; tmp: nq * num_cts * 4 * N u32.
+cudaError_t launch_response_compress(const uint64_t* flat, size_t flat_stride, size_t num_cts, uint32_t* tmp,
+                                     uint8_t* out, size_t out_stride, int nq, const DevTables* T, cudaStream_t s);
+
 // ---------------------------------------------------------------- preprocess
 // Encode pass over the rows [0, nrows) of a chunk: levels [l0, l0+nl) of the
 // inverse DFT over Z_P[X]/(X^N+1) across each ct-block of d_act polys.

@@ -185,7 +185,8 @@ size_t lane_bytes(const Server& S, size_t cap, int gt_pass) {
     const size_t R = S.pp.db_rows, G = S.pp.n_packed;
     return cap * S.qstride * 8 + cap * kKeyStride * 4 + cap * kRgswStride * 4 + cap * S.mv_qstride * 4 +
            tp_keyt_bytes(gt_pass) + (size_t)2 * kN * cap * G * 4 + cap * S.pb_qstride * 4 + cap * S.resp_qstride * 8 +
-           mv_tc_planes_bytes(R, (int)cap) + sizeof(int) + 2 * sizeof(unsigned);
+           mv_tc_planes_bytes(R, (int)cap) + sizeof(int) + 2 * sizeof(unsigned) + cap * S.wire_q +
+           cap * std::max(S.wire_r, S.wire_c) + cap * S.pp.num_cts * 4 * kN * 4;
 }
 
 void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
@@ -204,6 +205,9 @@ void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
     L.planes = A.alloc<uint8_t>(mv_tc_planes_bytes(R, (int)cap));
     L.d_err = A.alloc<int>(1);
     L.tiles = A.alloc<unsigned>(2);
+    L.wire_in = A.alloc<uint8_t>(cap * S.wire_q);
+    L.wire_out = A.alloc<uint8_t>(cap * std::max(S.wire_r, S.wire_c));
+    L.codec_tmp = A.alloc<uint32_t>(cap * S.pp.num_cts * 4 * kN);
     // Defined contents before any pipeline run (the autotuner runs on them).
     IPB_CK(cudaMemset(L.qraw, 0, cap * S.qstride * 8));
     IPB_CK(cudaMemset(L.planes, 0, mv_tc_planes_bytes(R, (int)cap)));
@@ -236,6 +240,9 @@ static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_
     S->mv_qstride = (size_t)std::max(S->mv_chunks, S->tc_kchunks) * 2 * C;
     S->pb_qstride = G * 2 * kN;
     S->resp_qstride = pp.num_cts * 4 * kN;
+    S->wire_q = wire_query_bytes(R);
+    S->wire_r = wire_response_bytes(pp.num_cts);
+    S->wire_c = wire_compressed_bytes(pp.num_cts);
     const int gt_pass = lane_gt_pass(*S, max_batch);
     S->sched = default_sched(*S, max_batch, gt_pass);
     alloc_lane(*S, S->lane, max_batch, gt_pass);
@@ -456,6 +463,31 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
     }
     table[0] = table[1];
     return table;
+}
+
+// ipir_answer_batch on packed queries: H2D of the packed bytes, unpack on
+// the device, the pipeline, then the response in the requested format.
+static void answer_wire(Server* S, const uint8_t* packed, size_t count, int fmt, void* out) {
+    IPB_CK(cudaSetDevice(S->device));
+    Lane& L = S->lane;
+    const Precomp& P = *S->pre;
+    cudaStream_t st = S->stream;
+    IPB_CK(cudaMemcpyAsync(L.wire_in, packed, count * S->wire_q, cudaMemcpyHostToDevice, st));
+    IPB_CK(launch_query_unpack(L.wire_in, S->wire_q, S->pp.db_rows, L.qraw, S->qstride, (int)count, P.tables, st));
+    run_pipeline(S, count);
+    if (fmt == 0) {
+        IPB_CK(cudaMemcpyAsync(out, L.resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, st));
+    } else if (fmt == 1) {
+        IPB_CK(launch_response_pack(L.resp, S->resp_qstride, S->pp.num_cts, L.wire_out, S->wire_r, (int)count,
+                                    P.tables, st));
+        IPB_CK(cudaMemcpyAsync(out, L.wire_out, count * S->wire_r, cudaMemcpyDeviceToHost, st));
+    } else {
+        IPB_CK(launch_response_compress(L.resp, S->resp_qstride, S->pp.num_cts, L.codec_tmp, L.wire_out, S->wire_c,
+                                        (int)count, P.tables, st));
+        IPB_CK(cudaMemcpyAsync(out, L.wire_out, count * S->wire_c, cudaMemcpyDeviceToHost, st));
+    }
+    IPB_CK(cudaStreamSynchronize(st));
+    check_device_error(L);
 }
 
 static int validate_batch(const Server* S, const ipir_query_view* qs, size_t count, const void* out) {
@@ -739,6 +771,23 @@ int ipir_b200_stage_times(const ipir_server* srv, float* ms_out, size_t n) {
     if (!srv || !ms_out) return 1;
     for (size_t i = 0; i < n && i < 5; ++i) ms_out[i] = srv->s->stage_ms[i];
     return 0;
+}
+
+int ipir_b200_wire_sizes(const ipir_params* params, size_t* query_packed, size_t* response_packed,
+                         size_t* response_compressed) {
+    if (!params) return 1;
+    if (query_packed) *query_packed = ipb::wire_query_bytes(params->db_rows);
+    if (response_packed) *response_packed = ipb::wire_response_bytes(params->num_cts);
+    if (response_compressed) *response_compressed = ipb::wire_compressed_bytes(params->num_cts);
+    return 0;
+}
+
+int ipir_b200_answer_wire(ipir_server* srv, const uint8_t* packed, size_t count, int resp_format, void* out) {
+    if (!srv || !packed || !out) return 1;
+    if (count > srv->s->max_batch) return 2;
+    if (resp_format < 0 || resp_format > 2) return 3;
+    if (count == 0) return 0;
+    return guarded([&]() -> int { ipb::answer_wire(srv->s, packed, count, resp_format, out); return 0; }, 4);
 }
 
 int ipir_b200_autotune(ipir_server* srv) {

@@ -103,6 +103,9 @@ struct Lane {
     uint8_t* planes = nullptr;   // query byte planes for the tensor-core mat-vec
     int* d_err = nullptr;        // device error word (pipeline wait timeouts)
     unsigned* tiles = nullptr;   // work-item counters: [0] mat-vec, [1] tensor pass
+    uint8_t* wire_in = nullptr;  // packed queries
+    uint8_t* wire_out = nullptr; // packed or compressed responses
+    uint32_t* codec_tmp = nullptr;  // coefficient-form responses for compression
     ~Lane() { arena.free_all(); }
 };
 
@@ -116,6 +119,7 @@ struct Server {
     Lane lane;
     // geometry derived at setup
     size_t qstride = 0, mv_qstride = 0, pb_qstride = 0, resp_qstride = 0;
+    size_t wire_q = 0, wire_r = 0, wire_c = 0;  // bytes per query: packed query, packed / compressed response
     int mv_chunks = 1;
     int num_sms = 148;
     int tc_kchunk_rows = 0, tc_kchunks = 1;

@@ -123,6 +123,10 @@ _L.ipir_b200_autotune.argtypes = [C.c_void_p]
 _L.ipir_b200_get_schedule.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirSchedule)]
 _L.ipir_b200_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
 _L.ipir_b200_set_schedule.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirSchedule)]
+_L.ipir_b200_wire_sizes.argtypes = [C.POINTER(IpirParams), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                    C.POINTER(C.c_size_t)]
+_L.ipir_b200_answer_wire.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_void_p]
+RESP_FLAT, RESP_PACKED, RESP_COMPRESSED = 0, 1, 2
 _L.ipir_serve_create.restype = C.c_void_p
 _L.ipir_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, C.POINTER(IpirServeConfig)]
 _L.ipir_serve_submit.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirQueryView), C.POINTER(C.c_uint64)]
@@ -153,7 +157,7 @@ EXPORTED = [
     "ipir_b200_matvec", "ipir_b200_matvec_noalloc", "ipir_b200_autotune", "ipir_b200_get_schedule",
     "ipir_b200_launch_count", "ipir_serve_create", "ipir_serve_submit", "ipir_serve_poll", "ipir_serve_wait",
     "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy", "ipir_b200_matvec_ex",
-    "ipir_b200_fill_db_device", "ipir_b200_set_schedule",
+    "ipir_b200_fill_db_device", "ipir_b200_set_schedule", "ipir_b200_wire_sizes", "ipir_b200_answer_wire",
 ]
 
 
@@ -331,6 +335,35 @@ class Server:
         rc = _L.ipir_b200_export_db(self._h, row0, nrows, _ptr(out, u16p))
         if rc:
             raise InspireError(f"export_db rc={rc}: {last_error()}")
+        return out
+
+    # wire formats ------------------------------------------------------
+    def wire_sizes(self):
+        """(packed query, packed response, compressed response) bytes per query."""
+        p = IpirParams()
+        for k, v in self.params.items():
+            if k == "seed":
+                p.seed[:] = list(v)
+            else:
+                setattr(p, k, v)
+        a, b_, c = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        _L.ipir_b200_wire_sizes(C.byref(p), C.byref(a), C.byref(b_), C.byref(c))
+        return a.value, b_.value, c.value
+
+    def answer_wire(self, packed, count, resp_format=RESP_COMPRESSED, out=None):
+        """Answer `count` packed queries (uint8, count x packed-query bytes);
+        returns the responses in resp_format (u64 rows for RESP_FLAT, bytes otherwise)."""
+        self._check()
+        qb, rb, cb = self.wire_sizes()
+        packed = np.ascontiguousarray(packed, dtype=np.uint8).reshape(-1)
+        if packed.size != count * qb:
+            raise ValueError(f"packed queries: {packed.size} bytes, expected {count * qb}")
+        if out is None:
+            out = (np.zeros((count, response_u64s(self.params)), np.uint64) if resp_format == RESP_FLAT else
+                   np.zeros((count, rb if resp_format == RESP_PACKED else cb), np.uint8))
+        rc = _L.ipir_b200_answer_wire(self._h, packed.ctypes.data, count, resp_format, out.ctypes.data)
+        if rc:
+            raise InspireError(f"answer_wire rc={rc}: {last_error()}")
         return out
 
     # schedules ---------------------------------------------------------

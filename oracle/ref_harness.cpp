@@ -147,6 +147,37 @@ int refh_decrypt(void* state, const uint64_t* resp, uint64_t* out_m) {
     return 0;
 }
 
+// extract_compressed() of src/protocol.cpp on compressed response bytes in
+// the client library's layout (src/capi_client.cpp:360-385): per ciphertext
+// N x 28-bit mask values then N x 20-bit body values, MSB first.
+int refh_extract_compressed(void* state, const uint8_t* in, uint16_t* out_slots, uint64_t* n_out) {
+    State* st = static_cast<State*>(state);
+    if (!st || !in) return 1;
+    std::vector<CompressedCt> cts(st->pp.num_cts);
+    uint64_t acc = 0;
+    int nbits = 0;
+    auto get = [&](int bits) -> uint32_t {
+        while (nbits < bits) {
+            acc = (acc << 8) | *in++;
+            nbits += 8;
+        }
+        nbits -= bits;
+        uint32_t v = (uint32_t)(acc >> nbits);
+        acc &= (1ULL << nbits) - 1;
+        return v;
+    };
+    for (size_t g = 0; g < st->pp.num_cts; g++) {
+        cts[g].a.resize(N);
+        cts[g].b.resize(N);
+        for (size_t i = 0; i < N; i++) cts[g].a[i] = get(28);
+        for (size_t i = 0; i < N; i++) cts[g].b[i] = get(20);
+    }
+    std::vector<uint16_t> s = extract_compressed(st->pp, st->st, cts);
+    std::memcpy(out_slots, s.data(), s.size() * 2);
+    *n_out = s.size();
+    return 0;
+}
+
 void refh_state_free(void* state) { delete static_cast<State*>(state); }
 
 void refh_ntt_forward(uint64_t* data, int limb) { ntt_forward(data, limb); }

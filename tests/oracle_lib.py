@@ -160,6 +160,24 @@ class Oracle:
         return out
 
 
+class RefParams(C.Structure):
+    """ipir_params of the reference's capi.h (src/capi.h:27-38)."""
+    _fields_ = [("n_entries", C.c_size_t), ("entry_bytes", C.c_size_t), ("db_rows", C.c_size_t),
+                ("db_cols", C.c_size_t), ("n_packed", C.c_size_t), ("interp_d", C.c_size_t),
+                ("num_cts", C.c_size_t), ("ring_n", C.c_size_t), ("d_eff", C.c_size_t),
+                ("seed", C.c_uint8 * 64)]
+
+
+def ref_params(geom, entry_bytes_and_entries, crs_seed):
+    """RefParams from a setup() geometry [n_entries, w, R, C, G, D, num_cts]."""
+    p = RefParams()
+    p.n_entries, p.entry_bytes = entry_bytes_and_entries
+    p.db_rows, p.db_cols, p.n_packed, p.interp_d, p.num_cts = geom[2], geom[3], geom[4], geom[5], geom[6]
+    p.ring_n, p.d_eff = N, 2
+    p.seed[:] = list(bytes(crs_seed))
+    return p
+
+
 class RefLib:
     def __init__(self, path=REF_SO):
         if not os.path.exists(path):
@@ -182,6 +200,17 @@ class RefLib:
         L.refh_automorphism_ntt.argtypes = [u64p, C.c_uint64, u64p]
         L.refh_ext_prod.argtypes = [u64p, u64p, u64p]
         L.refh_horner_eval.argtypes = [u64p, u64p, C.c_uint64, u64p]
+        L.refh_extract_compressed.argtypes = [C.c_void_p, u8p, u16p, u64p]
+        L.refh_extract_compressed.restype = C.c_int
+        # the reference client library's wire codecs (src/capi_client.cpp)
+        for fn in ("ipir_query_packed_bytes", "ipir_response_packed_bytes", "ipir_response_compressed_bytes"):
+            getattr(L, fn).argtypes = [C.POINTER(RefParams)]
+            getattr(L, fn).restype = C.c_size_t
+        for fn in ("ipir_query_pack", "ipir_response_pack", "ipir_response_compress"):
+            getattr(L, fn).argtypes = [C.POINTER(RefParams), u64p, u8p]
+            getattr(L, fn).restype = C.c_int
+        L.ipir_query_unpack.argtypes = [C.POINTER(RefParams), u8p, u64p]
+        L.ipir_query_unpack.restype = C.c_int
 
     def setup(self, n_entries, w, db_rows=0):
         g = np.zeros(7, np.uint64)
@@ -189,6 +218,14 @@ class RefLib:
         if rc != 0:
             raise ValueError("setup() rejected the geometry")
         return [int(x) for x in g]
+
+    def wire(self, params, fn, flat, nbytes_fn):
+        """Run one of the reference's packers on a flat u64 array."""
+        nb = getattr(self.L, nbytes_fn)(C.byref(params))
+        out = np.zeros(nb, np.uint8)
+        flat = np.ascontiguousarray(flat, np.uint64)
+        assert getattr(self.L, fn)(C.byref(params), ptr(flat, u64p), ptr(out, u8p)) == 0
+        return out
 
     def query(self, geom, crs_seed, idx, rng_seed):
         g = np.array(geom, np.uint64)
@@ -255,6 +292,14 @@ class RefState:
         n = np.zeros(1, np.uint64)
         resp = np.ascontiguousarray(resp, np.uint64)
         rc = self.lib.L.refh_extract(self.h, ptr(resp, u64p), ptr(slots, u16p), ptr(n, u64p))
+        assert rc == 0
+        return slots[: int(n[0])]
+
+    def extract_compressed(self, data):
+        slots = np.zeros(N, np.uint16)
+        n = np.zeros(1, np.uint64)
+        data = np.ascontiguousarray(data, np.uint8)
+        rc = self.lib.L.refh_extract_compressed(self.h, ptr(data, u8p), ptr(slots, u16p), ptr(n, u64p))
         assert rc == 0
         return slots[: int(n[0])]
 

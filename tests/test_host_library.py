@@ -104,3 +104,20 @@ def test_serve_entry_points_reject_null_without_gpu_work():
     assert L.ipir_b200_autotune(None) == 1
     v = C.c_ulonglong()
     assert L.ipir_b200_launch_count(None, C.byref(v)) == 1
+
+
+@pytest.mark.parametrize("args", [(256, 120, 2048), (262144, 120, 2048), (65536, 30, 0), (1 << 29, 30, 0)])
+def test_wire_sizes_match_reference_client(ref, args):
+    import ctypes as C
+    import inspire_b200 as ib
+    from oracle_lib import crs_seed_from, ref_params
+    g = ref.setup(*args)
+    rp = ref_params(g, args[:2], crs_seed_from(1))
+    p = ib.IpirParams()
+    assert ib.library_handle().ipir_b200_setup(args[0], args[1], args[2], C.byref(p)) == 0
+    a, b, c = C.c_size_t(), C.c_size_t(), C.c_size_t()
+    assert ib.library_handle().ipir_b200_wire_sizes(C.byref(p), C.byref(a), C.byref(b), C.byref(c)) == 0
+    L = ref.L
+    assert (a.value, b.value, c.value) == (L.ipir_query_packed_bytes(C.byref(rp)),
+                                           L.ipir_response_packed_bytes(C.byref(rp)),
+                                           L.ipir_response_compressed_bytes(C.byref(rp)))
