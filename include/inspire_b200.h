@@ -308,6 +308,17 @@ int ipir_serve_stats(ipir_serve* sv, ipir_serve_counters* out);
  * max_batch) of sched) the loop chose for database db. */
 int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_batch, ipir_serve_schedule* sched,
                        size_t sched_len);
+/* Replace database `db` by its next generation `next` (a handle of the same
+ * geometry on the same device, e.g. the refreshed DB preprocessed while the
+ * loop kept serving the old one): admission to db pauses, its batches in
+ * flight finish on the old generation, its graphs are re-captured for the
+ * new one, and admission resumes; requests still queued at that point are
+ * answered by the new generation.  Blocks until the switch is done; the old
+ * handle is then no longer referenced and may be destroyed.  Returns 0,
+ * 1 null argument or bad index, 2 geometry or device differs, 4 the loop
+ * failed, 6 another swap of db is in progress. */
+int ipir_serve_replace_db(ipir_serve* sv, size_t db, ipir_server* next);
+
 /* One lane batch, for tracing. */
 typedef struct {
     double t_issue_s;  /* steady (CLOCK_MONOTONIC) seconds when the batch was issued */

@@ -77,6 +77,9 @@ struct DbState {
     std::deque<uint32_t> pending;
     int last_lane = -1;  // lane of the most recently issued batch
     uint64_t batches = 0, queries = 0;
+    Server* swap_to = nullptr;  // next generation, installed once the lanes are idle
+    bool swap_done = false;
+    std::string swap_err;
 };
 
 struct Engine {
@@ -90,7 +93,7 @@ struct Engine {
     bool use_graphs = true;
     bool overlap_db = false;  // admit without waiting for the previous DB phase
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_swap;
     std::thread worker;
     bool stop = false;
     bool failed = false;
@@ -106,6 +109,7 @@ struct Engine {
     void issue(DbState& d, LaneRun& r);
     void finish(DbState& d, LaneRun& r);
     void fail_all_locked(const std::string& why);
+    void swap_locked(DbState& d, std::unique_lock<std::mutex>& lk);
 };
 
 void Engine::issue(DbState& d, LaneRun& r) {
@@ -207,11 +211,18 @@ void Engine::run() {
                     }
                 }
         if (!poll_err.empty()) fail_all_locked(poll_err);
+        for (auto& dp : dbs) {
+            if (!dp->swap_to) continue;
+            bool idle = true;
+            for (auto& r : dp->lanes) idle &= !r->busy;
+            if (idle) swap_locked(*dp, lk);
+            else any_busy = true;
+        }
         if (stop && !any_busy) break;
         if (!stop && !failed) {
             for (auto& dp : dbs) {
                 DbState& d = *dp;
-                if (d.pending.empty()) continue;
+                if (d.pending.empty() || d.swap_to) continue;
                 if (!overlap_db && d.last_lane >= 0 && d.lanes[d.last_lane]->busy) {
                     const cudaError_t q = cudaEventQuery(d.lanes[d.last_lane]->ev_db);
                     if (q == cudaErrorNotReady) continue;  // previous DB pass still running
@@ -316,16 +327,43 @@ cudaGraphExec_t capture_phase(DbState& d, LaneRun& r, size_t c, int phase) {
     return ge;
 }
 
-void capture_graphs(DbState& d, LaneRun& r) {
+void capture_graphs(DbState& d, LaneRun& r, bool warm = true) {
+    for (auto g : r.graphs_db)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto g : r.graphs_horner)
+        if (g) cudaGraphExecDestroy(g);
     r.graphs_db.assign(d.max_batch + 1, nullptr);
     r.graphs_horner.assign(d.max_batch + 1, nullptr);
     for (size_t c = 1; c <= d.max_batch; ++c) {
         // An eager run first: kernel attributes are set outside the capture.
-        run_pipeline(*d.S, r.lane, d.sched[c], c, r.st, nullptr);
+        if (warm) run_pipeline(*d.S, r.lane, d.sched[c], c, r.st, nullptr);
         r.graphs_db[c] = capture_phase(d, r, c, kPhaseDb);
         r.graphs_horner[c] = capture_phase(d, r, c, kPhaseHorner);
     }
     IPB_CK(cudaStreamSynchronize(r.st));
+}
+
+// Called by the worker with the lock held once every lane of d is idle:
+// point d at the next generation and re-capture its graphs (same geometry,
+// so the lane buffers and schedules carry over; kernels are already set up).
+void Engine::swap_locked(DbState& d, std::unique_lock<std::mutex>& lk) {
+    Server* next = d.swap_to;
+    d.S = next;  // under the lock: collectors read the response size through d.S
+    lk.unlock();
+    std::string err;
+    try {
+        IPB_CK(cudaSetDevice(next->device));
+        if (use_graphs)
+            for (auto& r : d.lanes) capture_graphs(d, *r, false);
+    } catch (const std::exception& e) {
+        err = e.what();
+    }
+    lk.lock();
+    d.swap_to = nullptr;
+    d.swap_err = err;
+    d.swap_done = true;
+    if (!err.empty()) fail_all_locked(err);
+    cv_swap.notify_all();
 }
 
 }  // namespace
@@ -579,6 +617,42 @@ int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_bat
             sched[c].tp_pass = d.sched[c].tp_pass;
             sched[c].horner_cluster = d.sched[c].horner_cluster;
         }
+    return 0;
+}
+
+int ipir_serve_replace_db(ipir_serve* sv, size_t db, ipir_server* next) {
+    if (!sv || !next || !next->s) return 1;
+    ipb::Engine& E = *sv->e;
+    if (db >= E.dbs.size()) return 1;
+    ipb::DbState& d = *E.dbs[db];
+    const ipb::Server& a = *d.S;
+    const ipb::Server& b = *next->s;
+    if (a.device != b.device || a.pp.db_rows != b.pp.db_rows || a.pp.db_cols != b.pp.db_cols ||
+        a.pp.n_packed != b.pp.n_packed || a.pp.D != b.pp.D || a.pp.num_cts != b.pp.num_cts ||
+        a.qstride != b.qstride || a.mv_qstride != b.mv_qstride || a.tc_kchunk_rows != b.tc_kchunk_rows ||
+        a.mv_chunks != b.mv_chunks) {
+        ipb::set_last_error("ipir_serve_replace_db: the new generation must have the same geometry and device");
+        return 2;
+    }
+    std::unique_lock<std::mutex> lk(E.mu);
+    if (E.failed) {
+        ipb::set_last_error(E.fail_text.c_str());
+        return 4;
+    }
+    if (d.swap_to) {
+        ipb::set_last_error("ipir_serve_replace_db: a swap of this database is in progress");
+        return 6;
+    }
+    if (d.S == next->s) return 0;
+    d.swap_to = next->s;
+    d.swap_done = false;
+    E.cv_work.notify_one();
+    E.cv_swap.wait(lk, [&] { return d.swap_done || E.stop; });
+    if (!d.swap_done) return 4;
+    if (!d.swap_err.empty()) {
+        ipb::set_last_error(d.swap_err.c_str());
+        return 4;
+    }
     return 0;
 }
 

@@ -137,6 +137,7 @@ _L.ipir_serve_stats.argtypes = [C.c_void_p, C.POINTER(IpirServeCounters)]
 _L.ipir_serve_db_info.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                   C.POINTER(IpirSchedule), C.c_size_t]
 _L.ipir_serve_destroy.argtypes = [C.c_void_p]
+_L.ipir_serve_replace_db.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
 
 
 class IpirServeBatchRecord(C.Structure):
@@ -158,6 +159,7 @@ EXPORTED = [
     "ipir_b200_launch_count", "ipir_serve_create", "ipir_serve_submit", "ipir_serve_poll", "ipir_serve_wait",
     "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy", "ipir_b200_matvec_ex",
     "ipir_b200_fill_db_device", "ipir_b200_set_schedule", "ipir_b200_wire_sizes", "ipir_b200_answer_wire",
+    "ipir_serve_replace_db",
 ]
 
 
@@ -466,6 +468,13 @@ class ServeLoop:
         c = IpirServeCounters()
         _L.ipir_serve_stats(self._h, C.byref(c))
         return {f: getattr(c, f) for f, _ in c._fields_}
+
+    def replace_db(self, db, server):
+        """Switch database `db` to the next generation `server` (same geometry)."""
+        rc = _L.ipir_serve_replace_db(self._h, db, server._h)
+        if rc:
+            raise InspireError(f"replace_db rc={rc}: {last_error()}")
+        self.servers[db] = server
 
     def trace(self, max_records=4096):
         """The most recent lane batches, oldest first (dicts of ipir_serve_batch_record)."""

@@ -160,3 +160,49 @@ def test_handle_autotune_keeps_results(env):
     assert sb.launch_count() > n0
     want = np.stack([a for (d, _, _, _), a in zip(reqs, alone) if d == 1][:4])
     assert (got == want).all()
+
+
+def test_generation_swap(env):
+    """Replace a resident database by its next generation (same geometry,
+    new contents) while the loop serves: before the swap every response is
+    the old generation's, after it the new one's, and requests racing the
+    swap get one of the two."""
+    import threading
+    import inspire_b200 as ib
+    ca, cb, sa, sb, reqs, alone = env
+    db2 = ib.fill_db(ca.R * ca.C, 77)
+    sa2 = ib.Server(ca.n_entries, ca.w, db2, db_rows=2048, max_batch=4, crs_seed=ca.seed)
+    try:
+        qa = [q for d, _, q, _ in reqs if d == 0]
+        new = [sa2.answer(q) for q in qa]
+        old = [a for (d, _, _, _), a in zip(reqs, alone) if d == 0]
+        assert not (new[0] == old[0]).all()
+        loop = ib.ServeLoop([sa, sb], max_batch=4, lanes_per_db=2, queue_slots=64, autotune=False)
+        try:
+            r = np.zeros(ib.response_u64s(sa.params), np.uint64)
+            t = loop.submit(0, qa[0])
+            loop.wait(t, out=r)
+            assert (r == old[0]).all()
+            # requests racing the swap
+            racing = [(i % len(qa), loop.submit(0, qa[i % len(qa)])) for i in range(12)]
+            th = threading.Thread(target=loop.replace_db, args=(0, sa2))
+            th.start()
+            racing += [(i % len(qa), loop.submit(0, qa[i % len(qa)])) for i in range(12, 20)]
+            th.join()
+            for i, t in racing:
+                loop.wait(t, out=r)
+                assert (r == old[i]).all() or (r == new[i]).all(), i
+            for i, q in enumerate(qa):
+                t = loop.submit(0, q)
+                loop.wait(t, out=r)
+                assert (r == new[i]).all(), i
+            # the other database is untouched
+            t = loop.submit(1, reqs[len(qa)][2])
+            loop.wait(t, out=r[: ib.response_u64s(sb.params)])
+            assert (r[: ib.response_u64s(sb.params)] == alone[len(qa)]).all()
+            st = loop.stats()
+            assert st["failed"] == 0
+        finally:
+            loop.close()
+    finally:
+        sa2.close()
