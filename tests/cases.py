@@ -52,4 +52,6 @@ def get_case(name):
         return Case(65536, 30, 0, crs=1, db_seed=0)
     if name == "g128":       # 2048 x 262144 (1 GB DB), G = 128: the 16 GB geometry's group count
         return Case(8388608, 120, 2048, crs=3, db_seed=5)
+    if name == "g512":       # 2048 x 1048576 (4.3 GB DB), G = 512 > D = 256: two response ciphertexts
+        return Case(33554432, 120, 2048, crs=4, db_seed=6)
     raise KeyError(name)
