@@ -80,6 +80,21 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def max_over_ranks(x, world, device):
+    """Max of a per-rank time over all ranks (a collective: every rank calls it)."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(per_step_ms, batch, world):
+    """Whole-job q/s of `world` replicas each answering `batch` queries per step."""
+    return world * batch * 1000.0 / per_step_ms
+
+
 def describe(params):
     R, C, G = params["db_rows"], params["db_cols"], params["n_packed"]
     ne, w = params["n_entries"], params["entry_bytes"]
@@ -302,12 +317,8 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    def ranks_max(x):
+        return max_over_ranks(x, world, "cuda")
 
     def device_time(count, steps, sampler=None):
         srv.stage_views(views, count)
@@ -332,7 +343,7 @@ def run_ours(args):
         launches = srv.launch_count() - n0
         clocks = sampler.stop() if sampler else None
         barrier()
-        return max_over_ranks(e0.elapsed_time(e1) / steps), launches, clocks
+        return ranks_max(e0.elapsed_time(e1) / steps), launches, clocks
 
     def stage_ms(count, reps):
         srv.enable_stage_timing(True)
@@ -349,7 +360,7 @@ def run_ours(args):
     stB = stage_ms(B, 3)
     ms1, _, _ = device_time(1, args.steps)
     msB, launches, clocks = device_time(B, args.steps, ClockSampler(local_rank))
-    value = world * B * 1000.0 / msB
+    value = replicas_value(msB, B, world)
     sweep_out = {}
     for b in sorted(set(sweep + [1, B])):
         if b == B:
@@ -371,7 +382,7 @@ def run_ours(args):
     for _ in range(args.steps):
         rc = srv.answer_batch_rc(views, B, obuf)
         assert rc == 0, ib.last_error()
-    t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    t_e2e = ranks_max((time.perf_counter() - t0) / args.steps)
     e2e_qps = world * B / t_e2e
     # e2e with the client library's wire formats: packed queries in (unpacked
     # on the device), compressed responses out
@@ -388,7 +399,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         srv.answer_wire(wq, B, ib.RESP_COMPRESSED, out=wo)
-    t_wire = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    t_wire = ranks_max((time.perf_counter() - t0) / args.steps)
     # plain path latency distribution (one query per call, e2e)
     lat = []
     for _ in range(max(args.steps, 20)):
