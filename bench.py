@@ -179,6 +179,13 @@ class ClockSampler:
         return d
 
 
+# DRAM bytes per algorithmic byte of mv_tc_kernel, from one ncu capture of a
+# batch-1 launch on the 1 GB geometry (dram__bytes_read.sum 1,074,673,152 +
+# dram__bytes_write.sum 3,670,016 for 1,074,266,112 algorithmic bytes); the
+# kernel streams the DB once, so its traffic scales with the DB size.
+MV_TC_TRAFFIC_RATIO = (1074673152 + 3670016) / 1074266112
+
+
 def measured_peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -436,7 +443,10 @@ def run_ours(args):
         "roofline": {"kernel": ("mv_tc_kernel (tcgen05 int8 DB pass, batch 1)" if sched1["matvec_tc"]
                                 else "matvec_kernel<1,8> (CUDA-core DB pass, batch 1)"), "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": None,
+                     "peak_source": peak_kind,
+                     "traffic": alg_bytes * MV_TC_TRAFFIC_RATIO if sched1["matvec_tc"] else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch on the 1 GB "
+                                       "geometry, scaled by the DB size",
                      "alg_bytes_per_launch": alg_bytes},
         "tensor_pass_gbs_b1": tensor_bytes / (st1["collapse"] * 1e-3) / 1e9,
         "e2e": {"value": e2e_qps, "unit": "q/s", "h2d_bytes_per_step": B * qn * 8,
