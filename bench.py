@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="batch", choices=["batch", "serve", "matvec"])
+    ap.add_argument("--mode", default="batch", choices=["batch", "serve", "matvec", "refgpu"])
     ap.add_argument("--mv-entries", type=int, default=1 << 31,
                     help="matvec mode: setup(N, 30) sizes the DB (2^31: 32768 x 1048576 u16 = 68.7 GB)")
     ap.add_argument("--mv-batches", default="1,16,32,64,128,256")
@@ -729,6 +729,67 @@ def run_matvec(args):
     print(json.dumps(line), flush=True)
 
 
+def run_refgpu(args):
+    """The reference's own GPU server library (compiled for sm_100a from its
+    sources into oracle/_ref by oracle/Makefile) on the same workload,
+    through its own C ABI: preprocess time, plain batch-1 latency and
+    batch-B q/s from host buffers (its ipir_answer_batch copies queries in
+    and responses out, like our e2e)."""
+    import ctypes as C
+    path = os.path.join(REPO, "oracle", "_ref", "libinspire_ref_gpu.so")
+    if not os.path.exists(path):
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "oracle/_ref/libinspire_ref_gpu.so not built"}))
+        return
+    import inspire_b200 as ib
+    R_ = C.CDLL(path)  # RTLD_LOCAL: its ipir_* names do not interpose on ours
+    R_.ipir_server_create.restype = C.c_void_p
+    R_.ipir_server_create.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p,
+                                      C.POINTER(ib.IpirParams)]
+    R_.ipir_answer_batch.argtypes = [C.c_void_p, C.POINTER(ib.IpirQueryView), C.c_size_t, C.c_void_p]
+    R_.ipir_server_destroy.argtypes = [C.c_void_p]
+    B = args.batch
+    params = ib.setup(args.n_entries, args.entry_bytes)
+    R, Cc = params["db_rows"], params["db_cols"]
+    db = ib.fill_db(R * Cc, 0)
+    seed = np.frombuffer(bytes(range(64)), np.uint8).copy()
+    p = ib.IpirParams()
+    t0 = time.perf_counter()
+    h = R_.ipir_server_create(args.n_entries, args.entry_bytes, 0, B, db.ctypes.data, seed.ctypes.data, C.byref(p))
+    t_pre = time.perf_counter() - t0
+    del db
+    if not h:
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "ipir_server_create failed"}))
+        return
+    qn, rn = ib.query_u64s(params), ib.response_u64s(params)
+    qbuf = np.zeros((B, qn), np.uint64)
+    synth_queries(params, B, 1000, qbuf)
+    obuf = np.zeros((B, rn), np.uint64)
+    views = (ib.IpirQueryView * B)()
+    for i in range(B):
+        views[i] = ib.query_view_from_flat(params, qbuf[i])
+    for _ in range(args.warmup):
+        assert R_.ipir_answer_batch(h, views, 1, obuf.ctypes.data) == 0
+    lat = []
+    for _ in range(max(args.steps, 20)):
+        t0 = time.perf_counter()
+        R_.ipir_answer_batch(h, views, 1, obuf.ctypes.data)
+        lat.append((time.perf_counter() - t0) * 1e3)
+    lat.sort()
+    for _ in range(args.warmup):
+        R_.ipir_answer_batch(h, views, B, obuf.ctypes.data)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        assert R_.ipir_answer_batch(h, views, B, obuf.ctypes.data) == 0
+    t_b = (time.perf_counter() - t0) / args.steps
+    R_.ipir_server_destroy(h)
+    print(json.dumps({"impl": "reference_gpu", "metric": "reference GPU server on this B200: preprocess s, plain "
+                      "latency, batch q/s (host buffers)", "config": {"workload": describe(params), "batch": B},
+                      "preprocess_s": t_pre, "plain_p50_ms": lat[len(lat) // 2], "plain_p99_ms": lat[-1],
+                      "batch_ms": t_b * 1e3, "batch_q_per_s": B / t_b,
+                      "build": "oracle/Makefile ref_gpu: its five .cu files + CPU sources, nvcc sm_100a -O3"}),
+          flush=True)
+
+
 def C_wait(loop, ticket, out):
     import inspire_b200 as ib
     try:
@@ -749,6 +810,10 @@ def main():
         rank, _, _ = dist_env()
         if rank == 0:
             run_matvec(args)
+    elif args.mode == "refgpu":
+        rank, _, _ = dist_env()
+        if rank == 0:
+            run_refgpu(args)
     else:
         run_ours(args)
 
