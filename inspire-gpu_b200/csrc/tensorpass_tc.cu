@@ -405,16 +405,40 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                 const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;  // g*4 + a
                 const int g = grow >> 2, a = grow & 3;
                 const bool valid = grow >= 0 && grow < slot_rows;
-                for (int q = 0; q < P.nq; ++q) {
-                    uint32_t v[4];
+                // four queries (16 columns) per TMEM load where the block has
+                // them; the block's last columns one query at a time
+                const int lim = P.spi > 1 ? P.nb : (mt + 1) * P.nb;
+                for (int q = 0; q < P.nq; q += 4) {
                     const int col = (P.spi > 1 ? mt * P.rq : mt * P.nb) + 4 * q;
-                    tmem_ld4(tmem_base + lane_base + (uint32_t)(as * acc_cols + col), v);
-                    uint64_t part = (uint64_t)c[a] * v[0] + (uint64_t)c[a + 1] * v[1] + (uint64_t)c[a + 2] * v[2] +
-                                    (uint64_t)c[a + 3] * v[3];
-                    part += __shfl_down_sync(0xffffffffu, part, 1);
-                    part += __shfl_down_sync(0xffffffffu, part, 2);
-                    if (a == 0 && valid)
-                        P.out[((size_t)li * P.nq_total + P.q0 + q) * P.G + g] = mod_u64(part, P.cr[l], P.q[l]);
+                    const uint32_t ta = tmem_base + lane_base + (uint32_t)(as * acc_cols + col);
+                    uint32_t v[16];
+                    if (col + 16 <= lim) {
+                        tmem_ld16(ta, v);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            uint32_t t[4] = {0, 0, 0, 0};
+                            if (col + 4 * k + 4 <= lim) tmem_ld4(ta + 4 * k, t);
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) v[4 * k + e] = t[e];
+                        }
+                    }
+                    uint64_t part[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        part[k] = (uint64_t)c[a] * v[4 * k] + (uint64_t)c[a + 1] * v[4 * k + 1] +
+                                  (uint64_t)c[a + 2] * v[4 * k + 2] + (uint64_t)c[a + 3] * v[4 * k + 3];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) part[k] += __shfl_down_sync(0xffffffffu, part[k], 1);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) part[k] += __shfl_down_sync(0xffffffffu, part[k], 2);
+                    if (a == 0 && valid) {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (q + k < P.nq)
+                                P.out[((size_t)li * P.nq_total + P.q0 + q + k) * P.G + g] =
+                                    mod_u64(part[k], P.cr[l], P.q[l]);
+                    }
                 }
             }
             tc_fence_before();

@@ -19,7 +19,7 @@ def env():
     import inspire_b200 as ib
     c = get_case("g128")
     assert c.G == 128
-    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=8, crs_seed=c.seed)
+    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=32, crs_seed=c.seed)
     qs, sts = [], []
     for k, idx in enumerate(IDX):
         q, st = c.query(idx, 7000 + k)
@@ -37,3 +37,16 @@ def test_batches_equal_singles_and_decrypt(env):
     for i, st in enumerate(sts):
         assert (st.extract(singles[i]) == c.expected_slots(IDX[i])).all(), i
     assert not (singles[4] == singles[7]).all()               # same entry, fresh keys
+
+
+def test_full_pass_of_32_queries(env):
+    """32 queries in one pass: N = 128 key columns per M tile, so the four
+    M tiles' accumulators fill TMEM and the epilogue drains one item before
+    the next item's MMAs start; 29 queries leave a ragged last column block."""
+    c, srv, qs, sts = env
+    more = [c.query(int(i), 7100 + k) for k, i in enumerate(np.random.default_rng(9).integers(0, c.n_entries, 24))]
+    qs32 = qs + [q for q, _ in more]
+    singles = np.stack([srv.answer(q) for q in qs32])
+    assert (srv.answer_batch(qs32) == singles).all()
+    assert (srv.answer_batch(qs32[:29]) == singles[:29]).all()
+    assert (srv.answer_batch(qs32[3:20]) == singles[3:20]).all()
