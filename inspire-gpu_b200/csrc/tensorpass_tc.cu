@@ -147,6 +147,25 @@ __device__ __forceinline__ void st_sw128(uint8_t* tile, uint32_t row, uint32_t c
     *reinterpret_cast<uint32_t*>(tile + row * 128 + ((((col >> 4) ^ (row & 7)) & 7) << 4) + (col & 15)) = w;
 }
 
+// One lane's row (g, a) over 4 queries' 16 accumulator columns (byte plane
+// b of query k at column 4k + b): part_k = sum_b (256^(a+b) mod q) P[4k + b]
+// (< 2^60, unreduced), then summed over the 4 lanes a of group g as a
+// reduce-scatter, so that lane a returns query a's total.  Round 1 (xor 1) keeps queries a & 1 and
+// (a & 1) + 2, round 2 (xor 2) keeps query a.
+__device__ __forceinline__ uint64_t tp_reduce4(const uint32_t (&v)[16], const uint32_t* c, int a) {
+    uint64_t part[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        part[k] = (uint64_t)c[a] * v[4 * k] + (uint64_t)c[a + 1] * v[4 * k + 1] + (uint64_t)c[a + 2] * v[4 * k + 2] +
+                  (uint64_t)c[a + 3] * v[4 * k + 3];
+    const int b0 = a & 1, b1 = (a >> 1) & 1;
+    const uint64_t keep0 = b0 ? part[1] : part[0], keep1 = b0 ? part[3] : part[2];
+    const uint64_t send0 = b0 ? part[0] : part[1], send1 = b0 ? part[2] : part[3];
+    const uint64_t s0 = keep0 + __shfl_xor_sync(0xffffffffu, send0, 1);
+    const uint64_t s1 = keep1 + __shfl_xor_sync(0xffffffffu, send1, 1);
+    return (b1 ? s1 : s0) + __shfl_xor_sync(0xffffffffu, b1 ? s0 : s1, 2);
+}
+
 // ------------------------------------------------------------------ GEMM
 struct TpParams {
     uint32_t* out;         // tp_out[l][i][q][g]
@@ -423,22 +442,9 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                             for (int e = 0; e < 4; ++e) v[4 * k + e] = t[e];
                         }
                     }
-                    uint64_t part[4];
-#pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        part[k] = (uint64_t)c[a] * v[4 * k] + (uint64_t)c[a + 1] * v[4 * k + 1] +
-                                  (uint64_t)c[a + 2] * v[4 * k + 2] + (uint64_t)c[a + 3] * v[4 * k + 3];
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) part[k] += __shfl_down_sync(0xffffffffu, part[k], 1);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) part[k] += __shfl_down_sync(0xffffffffu, part[k], 2);
-                    if (a == 0 && valid) {
-#pragma unroll
-                        for (int k = 0; k < 4; ++k)
-                            if (q + k < P.nq)
-                                P.out[((size_t)li * P.nq_total + P.q0 + q + k) * P.G + g] =
-                                    mod_u64(part[k], P.cr[l], P.q[l]);
-                    }
+                    const uint64_t tot = tp_reduce4(v, c, a);
+                    if (valid && q + a < P.nq)
+                        P.out[((size_t)li * P.nq_total + P.q0 + q + a) * P.G + g] = mod_u64(tot, P.cr[l], P.q[l]);
                 }
             }
             tc_fence_before();
