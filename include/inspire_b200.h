@@ -194,12 +194,16 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
 /* Kernel schedule for one batch size: mat-vec on the tensor cores
  * (matvec_tc = 1) or the CUDA cores (0); queries per tensor-pass GEMM
  * (tp_pass); Horner on a 4-CTA cluster per chain (horner_cluster = 1), an
- * 8-CTA cluster (2) or one CTA per chain (0).  Every schedule gives the same
- * responses. */
+ * 8-CTA cluster (2) or one CTA per chain (0); tp_sms > 0 runs the tensor
+ * pass on that many SMs at the same time as the tensor-core mat-vec on the
+ * others (the two read disjoint data: the tensor pass is DRAM-bound, the
+ * batched mat-vec tensor-core-bound), 0 runs them one after the other.
+ * Every schedule gives the same responses. */
 typedef struct {
     int matvec_tc;
     int tp_pass;
     int horner_cluster;
+    int tp_sms;
 } ipir_serve_schedule;
 
 /* Time the candidate schedules on this handle for batch sizes 1, 2, 4, ...

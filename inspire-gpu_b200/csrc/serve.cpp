@@ -616,6 +616,7 @@ int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_bat
             sched[c].matvec_tc = d.sched[c].matvec_tc;
             sched[c].tp_pass = d.sched[c].tp_pass;
             sched[c].horner_cluster = d.sched[c].horner_cluster;
+            sched[c].tp_sms = d.sched[c].tp_sms;
         }
     return 0;
 }

@@ -208,6 +208,9 @@ void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
     L.wire_in = A.alloc<uint8_t>(cap * S.wire_q);
     L.wire_out = A.alloc<uint8_t>(cap * std::max(S.wire_r, S.wire_c));
     L.codec_tmp = A.alloc<uint32_t>(cap * S.pp.num_cts * 4 * kN);
+    IPB_CK(cudaStreamCreateWithFlags(&L.aux, cudaStreamNonBlocking));
+    IPB_CK(cudaEventCreateWithFlags(&L.fork, cudaEventDisableTiming));
+    IPB_CK(cudaEventCreateWithFlags(&L.join, cudaEventDisableTiming));
     // Defined contents before any pipeline run (the autotuner runs on them).
     IPB_CK(cudaMemset(L.qraw, 0, cap * S.qstride * 8));
     IPB_CK(cudaMemset(L.planes, 0, mv_tc_planes_bytes(R, (int)cap)));
@@ -278,12 +281,14 @@ int lane_gt_pass(const Server& S, size_t cap) {
     return (int)std::min<size_t>(cap, (size_t)tp_pass_queries(S.pp.n_packed));
 }
 
-std::vector<Sched> default_sched(const Server&, size_t cap, int gt_pass) {
+std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
     Sched def;
     def.tp_pass = gt_pass;
     if (const char* m = std::getenv("IPB_MATVEC")) def.matvec_tc = std::strcmp(m, "simt") != 0;
     if (const char* h = std::getenv("IPB_HORNER"))
         def.horner_cluster = std::strcmp(h, "cta") == 0 ? 0 : (std::strcmp(h, "cl8") == 0 ? 2 : 1);
+    if (const char* t = std::getenv("IPB_TP_SMS"))
+        def.tp_sms = def.matvec_tc ? std::max(0, std::min(std::atoi(t), S.num_sms - 1)) : 0;
     return std::vector<Sched>(cap + 1, def);
 }
 
@@ -299,6 +304,24 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
     IPB_CK(launch_qprep(L.qraw, S.qstride, R, P.tables, L.keys, L.rgsw32, nq, st));
     ++launches;
     if (ev) IPB_CK(cudaEventRecord(ev[1], st));
+    // Beside: the tensor pass (keys only) on sc.tp_sms SMs from the lane's
+    // second stream while the mat-vec (DB only) runs on the other SMs; the
+    // two persistent kernels take one CTA per SM each, so the split holds.
+    const bool beside = sc.matvec_tc && sc.tp_sms > 0 && sc.tp_sms < S.num_sms;
+    auto tensor_pass = [&](cudaStream_t ts, int sms) {
+        for (size_t c0 = 0; c0 < count; c0 += (size_t)sc.tp_pass) {
+            const int n = (int)std::min<size_t>((size_t)sc.tp_pass, count - c0);
+            IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.keyt,
+                                      L.tp_out, L.d_err, L.tiles + 1, sms, ts));
+            launches += 2;  // key table + GEMM
+        }
+    };
+    if (beside) {
+        IPB_CK(cudaEventRecord(L.fork, st));
+        IPB_CK(cudaStreamWaitEvent(L.aux, L.fork, 0));
+        tensor_pass(L.aux, sc.tp_sms);
+        IPB_CK(cudaEventRecord(L.join, L.aux));
+    }
     int mv_parts;
     if (sc.matvec_tc) {
         IPB_CK(launch_qplanes(L.qraw, S.qstride, R, P.tables, L.planes, nq, st));
@@ -306,7 +329,8 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
         for (size_t c0 = 0; c0 < count; c0 += 32) {
             const int n = (int)std::min<size_t>(32, count - c0);
             IPB_CK(launch_matvec_tc(P.db, R, C, L.planes + 8 * c0 * R, n, P.tables, L.mvpart + c0 * S.mv_qstride,
-                                    S.mv_qstride, L.d_err, L.tiles, S.num_sms, S.tc_kchunk_rows, st));
+                                    S.mv_qstride, L.d_err, L.tiles, beside ? S.num_sms - sc.tp_sms : S.num_sms,
+                                    S.tc_kchunk_rows, st));
             ++launches;
         }
         mv_parts = S.tc_kchunks;
@@ -319,13 +343,10 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
         }
         mv_parts = S.mv_chunks;
     }
+    if (beside)
+        IPB_CK(cudaStreamWaitEvent(st, L.join, 0));  // stage times: mat-vec = both, tensor pass = 0
     if (ev) IPB_CK(cudaEventRecord(ev[2], st));
-    for (size_t c0 = 0; c0 < count; c0 += (size_t)sc.tp_pass) {
-        const int n = (int)std::min<size_t>((size_t)sc.tp_pass, count - c0);
-        IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.keyt,
-                                  L.tp_out, L.d_err, L.tiles + 1, S.num_sms, st));
-        launches += 2;  // key table + GEMM
-    }
+    if (!beside) tensor_pass(st, S.num_sms);
     if (ev) IPB_CK(cudaEventRecord(ev[3], st));
     IPB_CK(launch_finalize(L.mvpart, S.mv_qstride, mv_parts, C, L.tp_out, P.pre_df, L.keys, kKeyStride, P.tables,
                            L.packed_b, S.pb_qstride, G, nq, st));
@@ -397,7 +418,10 @@ static void fetch(Server* S, size_t count, uint64_t* out) {
 // 4 queries, so it is tried up to 8), queries per tensor-pass GEMM (the
 // key-table capacity and its half: fewer queries per pass re-read the
 // tensors but double-buffer the accumulators), Horner kernel (4-CTA
-// cluster, 8-CTA cluster, single CTA) -- and keep the fastest.  Sizes between two measured ones use the smaller's.
+// cluster, 8-CTA cluster, single CTA) -- and keep the fastest; then, for the
+// tensor-core mat-vec, the number of SMs (1/18 .. 8/18 of them) that run the
+// tensor pass at the same time as the mat-vec, if that is faster still.
+// Sizes between two measured ones use the smaller's.
 std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
     IPB_CK(cudaSetDevice(S.device));
     std::vector<size_t> sizes;
@@ -417,9 +441,7 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
                 for (int p : passes)
                     for (int h : {1, 2, 0}) cands.push_back(Sched{mv, p, h});
             }
-            float best_ms = 1e30f;
-            Sched pick = cands[0];
-            for (const Sched& c : cands) {
+            auto time_of = [&](const Sched& c) {
                 run_pipeline(S, L, c, b, st, nullptr);  // warm
                 float ms = 1e30f;
                 for (int r = 0; r < 2; ++r) {
@@ -431,9 +453,29 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
                     IPB_CK(cudaEventElapsedTime(&t, e0, e1));
                     ms = std::min(ms, t);
                 }
+                return ms;
+            };
+            float best_ms = 1e30f;
+            Sched pick = cands[0];
+            for (const Sched& c : cands) {
+                const float ms = time_of(c);
                 if (ms < best_ms * 0.98f) {  // keep the earlier (default-ordered) choice on near ties
                     best_ms = ms;
                     pick = c;
+                }
+            }
+            // Then the SM split for running the tensor pass beside the mat-vec.
+            if (pick.matvec_tc) {
+                const Sched seq = pick;
+                for (int k = 1; k <= 8; ++k) {
+                    Sched c = seq;
+                    c.tp_sms = S.num_sms * k / 18;  // 1/18 .. 8/18 of the SMs
+                    if (c.tp_sms < 1) continue;
+                    const float ms = time_of(c);
+                    if (ms < best_ms * 0.98f) {
+                        best_ms = ms;
+                        pick = c;
+                    }
                 }
             }
             best.emplace_back(b, pick);
@@ -810,6 +852,7 @@ int ipir_b200_get_schedule(const ipir_server* srv, size_t count, ipir_serve_sche
     out->matvec_tc = sc.matvec_tc;
     out->tp_pass = sc.tp_pass;
     out->horner_cluster = sc.horner_cluster;
+    out->tp_sms = sc.tp_sms;
     return 0;
 }
 
@@ -818,11 +861,14 @@ int ipir_b200_set_schedule(ipir_server* srv, size_t count, const ipir_serve_sche
     ipb::Server* S = srv->s;
     if (count == 0 || count > S->max_batch) return 2;
     if (sc->matvec_tc < 0 || sc->matvec_tc > 1 || sc->horner_cluster < 0 || sc->horner_cluster > 2 ||
-        sc->tp_pass < 1 || sc->tp_pass > S->lane.gt_pass) {
-        ipb::g_last_error = "ipir_b200_set_schedule: matvec_tc 0/1, horner_cluster 0/1/2, tp_pass 1..capacity";
+        sc->tp_pass < 1 || sc->tp_pass > S->lane.gt_pass || sc->tp_sms < 0 || sc->tp_sms >= S->num_sms ||
+        (sc->tp_sms > 0 && !sc->matvec_tc)) {
+        ipb::g_last_error =
+            "ipir_b200_set_schedule: matvec_tc 0/1, horner_cluster 0/1/2, tp_pass 1..capacity, "
+            "tp_sms 0..SMs-1 (0 with the CUDA-core mat-vec)";
         return 2;
     }
-    S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster};
+    S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster, sc->tp_sms};
     return 0;
 }
 

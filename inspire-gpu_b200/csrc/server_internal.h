@@ -85,6 +85,8 @@ struct Sched {
     int matvec_tc = 1;       // 1: tcgen05 int8 mat-vec, 0: CUDA-core mat-vec
     int tp_pass = 32;        // queries per tensor-pass GEMM (<= the lane's Gt capacity)
     int horner_cluster = 1;  // 1: 4-CTA cluster per chain, 2: 8-CTA cluster, 0: one CTA per chain
+    int tp_sms = 0;          // > 0: tensor pass on this many SMs beside the tcgen05 mat-vec on the
+                             // others (the lane's second stream); 0: tensor pass after the mat-vec
 };
 
 // Per-batch device scratch for up to `cap` queries.
@@ -106,7 +108,14 @@ struct Lane {
     uint8_t* wire_in = nullptr;  // packed queries
     uint8_t* wire_out = nullptr; // packed or compressed responses
     uint32_t* codec_tmp = nullptr;  // coefficient-form responses for compression
-    ~Lane() { arena.free_all(); }
+    cudaStream_t aux = nullptr;     // second stream: the tensor pass beside the mat-vec
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~Lane() {
+        if (join) cudaEventDestroy(join);
+        if (fork) cudaEventDestroy(fork);
+        if (aux) cudaStreamDestroy(aux);
+        arena.free_all();
+    }
 };
 
 struct Server {

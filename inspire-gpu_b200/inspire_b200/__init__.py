@@ -94,7 +94,7 @@ _L.ipir_b200_matvec_noalloc.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_
 
 
 class IpirSchedule(C.Structure):
-    _fields_ = [("matvec_tc", C.c_int), ("tp_pass", C.c_int), ("horner_cluster", C.c_int)]
+    _fields_ = [("matvec_tc", C.c_int), ("tp_pass", C.c_int), ("horner_cluster", C.c_int), ("tp_sms", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -383,11 +383,12 @@ class Server:
             raise InspireError(f"get_schedule rc={rc}")
         return s.as_dict()
 
-    def set_schedule(self, count, matvec_tc=1, tp_pass=None, horner_cluster=1):
-        """Pin the kernel schedule for batches of `count` queries."""
+    def set_schedule(self, count, matvec_tc=1, tp_pass=None, horner_cluster=1, tp_sms=0):
+        """Pin the kernel schedule for batches of `count` queries (tp_sms > 0:
+        tensor pass on that many SMs beside the mat-vec)."""
         self._check()
         s = IpirSchedule(matvec_tc, tp_pass if tp_pass is not None else self.schedule(count)["tp_pass"],
-                         horner_cluster)
+                         horner_cluster, tp_sms)
         rc = _L.ipir_b200_set_schedule(self._h, count, C.byref(s))
         if rc:
             raise InspireError(f"set_schedule rc={rc}: {last_error()}")

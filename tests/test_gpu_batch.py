@@ -90,3 +90,22 @@ def test_every_schedule_gives_the_same_responses(batch_env, horner, matvec_tc):
     assert (got[0] == c.oracle_answer(qs[0])).all()
     for n in (1, 4):
         srv.set_schedule(n, matvec_tc=1, horner_cluster=1)
+
+
+@pytest.mark.parametrize("tp_sms", [1, 40, 147])
+def test_tensor_pass_beside_matvec(batch_env, tp_sms):
+    """The tensor pass on tp_sms SMs from the lane's second stream while the
+    mat-vec runs on the others (down to one SM either side) gives the same
+    responses as the two one after the other."""
+    c, srv, qs, sts = batch_env
+    want = np.stack([srv.answer(q) for q in qs])
+    for n in (1, 4, 10):
+        srv.set_schedule(n, matvec_tc=1, horner_cluster=1, tp_sms=tp_sms)
+        assert srv.schedule(n)["tp_sms"] == tp_sms
+    assert (srv.answer(qs[0]) == want[0]).all()
+    assert (srv.answer_batch(qs[:4]) == want[:4]).all()
+    assert (srv.answer_batch(qs) == want).all()
+    for n in (1, 4, 10):
+        srv.set_schedule(n, matvec_tc=1, horner_cluster=1)
+    with pytest.raises(Exception):
+        srv.set_schedule(4, matvec_tc=0, horner_cluster=1, tp_sms=8)   # CUDA-core mat-vec: no split

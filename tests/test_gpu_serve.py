@@ -116,6 +116,22 @@ def test_graphs_and_direct_launches_agree(env):
     assert stats["failed"] == 0
 
 
+def test_tensor_pass_beside_matvec_in_graphs(env, monkeypatch):
+    """Schedules that fork the tensor pass onto a second stream beside the
+    mat-vec: captured into the per-batch-size graphs (and launched
+    directly), every response equals the plain single answer."""
+    import inspire_b200 as ib
+    ca, cb, sa, sb, reqs, alone = env
+    monkeypatch.setenv("IPB_TP_SMS", "48")
+    for graphs in (True, False):
+        out, stats, info = _run_mix(ib, [sa, sb], reqs, random.Random(11), max_batch=4, lanes_per_db=2,
+                                    graphs=graphs, autotune=False, overlap_db_passes=not graphs)
+        assert all(s["tp_sms"] == 48 for db in info for s in db["schedule"].values())
+        for i in range(len(reqs)):
+            assert (out[i] == alone[i]).all(), (graphs, i)
+        assert stats["failed"] == 0
+
+
 def test_slot_and_ticket_codes(env):
     import inspire_b200 as ib
     ca, cb, sa, sb, reqs, alone = env
