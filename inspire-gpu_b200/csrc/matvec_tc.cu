@@ -13,8 +13,8 @@
 // exact integer sum_i db[i][j] b[i] (< 2^58), and reduces it mod q_l.  All
 // arithmetic stays exact, so the result equals the reference's.
 //
-// CTA roles (256 threads): warp 0 issues TMA loads (DB tile 256 x 128 rows as
-// two 128-byte boxes, query planes N x 128), warp 1 allocates TMEM and one
+// CTA roles (256 threads): warp 0 issues TMA loads (DB tile 256 x 64 rows as
+// two 128-byte boxes, query planes N x 64), warp 1 allocates TMEM and one
 // thread issues the MMAs, warps 4..7 drain TMEM (tcgen05.ld) and write
 // partial sums.  Stages are recycled through mbarriers; every wait is
 // bounded and reports a timeout through *err instead of hanging.
@@ -37,7 +37,12 @@ namespace ipb {
 namespace {
 using namespace tc;
 
-constexpr int kKT = 128;          // DB rows per pipeline stage (bytes of K)
+// DB rows per pipeline stage (bytes of K): 64, so a stage is 16 KB of DB
+// plus 64 bytes of every query plane (a SWIZZLE_64B tile), 32 KB at 32
+// queries, and six stages fit (three with 128-row stages).  Deeper DB
+// prefetch (an L2 prefetch ahead of the ring, or a separate deeper DB ring)
+// measured slower: the SMs drift apart and the DB rows lose locality.
+constexpr int kKT = 64;
 constexpr int kMT = 256;          // m' rows per tile (two M = 128 MMAs)
 constexpr int kKChunk = 32768;    // rows per exact s32 accumulation
 constexpr int kRing = 8;          // published work items in flight
@@ -63,8 +68,8 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int S = P.stages;
-    const uint32_t a_bytes = kKT * 128;              // one 128-byte m' box x 128 rows
-    const uint32_t b_bytes = (uint32_t)P.npad * 128;
+    const uint32_t a_bytes = kKT * 128;              // one 128-byte m' box x kKT rows
+    const uint32_t b_bytes = (uint32_t)P.npad * kKT;
     const uint32_t stage_bytes = 2 * a_bytes + b_bytes;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
     uint64_t* full = bars;
@@ -157,8 +162,8 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                         // K advances 32 rows = 4096 bytes per MMA.
                         const uint64_t a0 = smem_desc(st + kk * 4096, 0, 1024);
                         const uint64_t a1 = smem_desc(st + a_bytes + kk * 4096, 0, 1024);
-                        // B: K-major, 128-byte rows, 8-row groups 1024 B apart; K advances 32 bytes.
-                        const uint64_t b = smem_desc(st + 2 * a_bytes + kk * 32, 16, 1024);
+                        // B: K-major, 64-byte rows (SWIZZLE_64B), 8-row groups 512 B apart; K advances 32 bytes.
+                        const uint64_t b = smem_desc_sw64(st + 2 * a_bytes + kk * 32, 512);
                         const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
                         mma_i8(d0, a0, b, idesc, acc);
                         mma_i8(d0 + (uint32_t)P.npad, a1, b, idesc, acc);
@@ -329,10 +334,10 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     {
         cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)npad};
         cuuint64_t strides[1] = {(cuuint64_t)rows};
-        cuuint32_t box[2] = {128, (cuuint32_t)npad};
+        cuuint32_t box[2] = {(cuuint32_t)kKT, (cuuint32_t)npad};
         cuuint32_t es[2] = {1, 1};
         if (enc(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)planes, dims, strides, box, es,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return cudaErrorInvalidValue;
     }
@@ -353,7 +358,7 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     P.err = err;
     P.tiles = tiles;
     P.T = T;
-    const size_t stage_bytes = 2 * (size_t)kKT * 128 + (size_t)npad * 128;
+    const size_t stage_bytes = 2 * (size_t)kKT * 128 + (size_t)npad * kKT;
     const size_t budget = 200 * 1024;
     P.stages = (int)std::min<size_t>(8, budget / stage_bytes);
     if (P.stages < 2) return cudaErrorInvalidValue;

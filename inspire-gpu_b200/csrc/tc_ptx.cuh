@@ -60,6 +60,16 @@ __device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t lbo_bytes,
     d |= (uint64_t)2 << 61;   // layout = SWIZZLE_128B
     return d;
 }
+// Same for K-major SWIZZLE_64B tiles (64-byte rows, 8-row atoms of 512 bytes).
+__device__ __forceinline__ uint64_t smem_desc_sw64(const void* p, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_u32(p) >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;   // leading byte offset: unused for swizzled K-major
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;   // version = 1 (Blackwell)
+    d |= (uint64_t)4 << 61;   // layout = SWIZZLE_64B
+    return d;
+}
 // Instruction descriptor: kind::i8, D s32, A u8 MN-major, B u8 K-major, M = 128.
 __host__ __device__ constexpr uint32_t idesc_i8(int n) {
     return (2u << 4) | (0u << 7) | (0u << 10) | (1u << 15) | (0u << 16) | ((uint32_t)(n >> 3) << 17) |
