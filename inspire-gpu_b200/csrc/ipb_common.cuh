@@ -209,9 +209,18 @@ __device__ __forceinline__ void ntt_inv(uint32_t (&r)[8], uint32_t* sbuf, const 
 // One coefficient: CRT lift of (c0 mod q0, c1 mod q1) to [0, Q), center to
 // (-Q/2, Q/2], three signed base-2^18 digits, digit 0 dropped
 // (src/ring.cpp:205-246).  Returns digits 1 and 2 as signed values.
-__device__ __forceinline__ void decomp2(uint32_t c0, uint32_t c1, const DevTables& T, int64_t& d1, int64_t& d2) {
-    uint32_t t0 = csub(shoup_mul(c0, T.crt_c[0], T.crt_cp[0], kQ0), kQ0);
-    uint32_t t1 = csub(shoup_mul(c1, T.crt_c[1], T.crt_cp[1], kQ1), kQ1);
+// The CRT factors in registers: kernels whose loops contain asm with memory
+// clobbers (mbarrier waits, st.async) would otherwise reload them from the
+// table in global memory at every use.
+struct CrtK {
+    uint32_t c0, cp0, c1, cp1;
+};
+__device__ __forceinline__ CrtK crt_consts(const DevTables& T) {
+    return CrtK{T.crt_c[0], T.crt_cp[0], T.crt_c[1], T.crt_cp[1]};
+}
+__device__ __forceinline__ void decomp2(uint32_t c0, uint32_t c1, const CrtK& k, int64_t& d1, int64_t& d2) {
+    uint32_t t0 = csub(shoup_mul(c0, k.c0, k.cp0, kQ0), kQ0);
+    uint32_t t1 = csub(shoup_mul(c1, k.c1, k.cp1, kQ1), kQ1);
     uint64_t v = (uint64_t)t0 * kQ1 + (uint64_t)t1 * kQ0;   // < 2Q
     if (v >= kQFull) v -= kQFull;
     int64_t r = (v <= kQFull / 2) ? (int64_t)v : (int64_t)v - (int64_t)kQFull;
@@ -221,6 +230,9 @@ __device__ __forceinline__ void decomp2(uint32_t c0, uint32_t c1, const DevTable
     d1 = (int64_t)((uint64_t)r << K) >> K;
     r = (r - d1) >> kBaseLog;
     d2 = (int64_t)((uint64_t)r << K) >> K;
+}
+__device__ __forceinline__ void decomp2(uint32_t c0, uint32_t c1, const DevTables& T, int64_t& d1, int64_t& d2) {
+    decomp2(c0, c1, crt_consts(T), d1, d2);
 }
 __device__ __forceinline__ uint32_t signed_res(int64_t d, uint32_t q) {
     return d >= 0 ? (uint32_t)d : (uint32_t)((int64_t)q + d);

@@ -379,6 +379,9 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     const int bar = 1 + gp;
     const LimbTables& L = T->limb[l];
     const uint32_t q = L.q;
+    const uint64_t cr = L.cr;
+    const uint32_t inv_n = L.inv_n, inv_n_p = L.inv_n_p;
+    const CrtK ck = crt_consts(*T);
     for (int i = threadIdx.x; i < kN; i += 512) { twf[i] = L.fwd[i]; twi[i] = L.inv[i]; }
     if (threadIdx.x == 0) {
         abort_flag = 0;
@@ -419,7 +422,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
         uint32_t pk[8];
         if (gp == 0) {
             ld8(src_of(start + (size_t)i) + 8 * t, pk);
-            ntt_inv(acc, nbuf, twi, q, L.inv_n, L.inv_n_p, t, bar);   // acc: index t + 256 e
+            ntt_inv(acc, nbuf, twi, q, inv_n, inv_n_p, t, bar);   // acc: index t + 256 e
 #pragma unroll
             for (int e = 0; e < 8; ++e) xown[t + 256 * e] = acc[e];
         }
@@ -439,15 +442,15 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
         for (int e = 0; e < 8; ++e) {
             const uint32_t own = xown[t + 256 * e], oth = xpart[t + 256 * e];
             int64_t s1, s2;
-            decomp2(l ? oth : own, l ? own : oth, *T, s1, s2);
+            decomp2(l ? oth : own, l ? own : oth, ck, s1, s2);
             d[e] = signed_res(gp ? s2 : s1, q);
         }
         ntt_fwd(d, nbuf + gp * 2 * kN, twf, q, t, bar);
         uint32_t es[8], eo[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-            es[e] = mod_u64((uint64_t)d[e] * r_self[e], L.cr, q);
-            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], L.cr, q);
+            es[e] = mod_u64((uint64_t)d[e] * r_self[e], cr, q);
+            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], cr, q);
         }
         st8(cp + (size_t)gp * kN + 8 * t, es);
         const uint32_t dstc = peer_c + (uint32_t)((size_t)par * 4 * kN + (size_t)(2 + gp) * kN + 8 * t) * 4;
@@ -513,6 +516,9 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
     const uint32_t t = threadIdx.x;
     const LimbTables& L = T->limb[l];
     const uint32_t q = L.q;
+    const uint64_t cr = L.cr;
+    const uint32_t inv_n = L.inv_n, inv_n_p = L.inv_n_p;
+    const CrtK ck = crt_consts(*T);
     for (int i = threadIdx.x; i < kN; i += 256) { twf[i] = L.fwd[i]; twi[i] = L.inv[i]; }
     if (threadIdx.x == 0) {
         abort_flag = 0;
@@ -554,7 +560,7 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
         }
         uint32_t pk[8];
         ld8(src_of(start + (size_t)i) + 8 * t, pk);
-        ntt_inv(acc, nbuf, twi, q, L.inv_n, L.inv_n_p, t, 0);   // acc: index t + 256 e
+        ntt_inv(acc, nbuf, twi, q, inv_n, inv_n_p, t, 0);   // acc: index t + 256 e
 #pragma unroll
         for (int e = 0; e < 8; ++e) xown[t + 256 * e] = acc[e];
         __syncthreads();  // xown complete; abort_flag is read only here, after a block barrier
@@ -571,15 +577,15 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
         for (int e = 0; e < 8; ++e) {
             const uint32_t own = xown[t + 256 * e], oth = xpart[t + 256 * e];
             int64_t s1, s2;
-            decomp2(l ? oth : own, l ? own : oth, *T, s1, s2);
+            decomp2(l ? oth : own, l ? own : oth, ck, s1, s2);
             d[e] = signed_res(j ? s2 : s1, q);
         }
         ntt_fwd(d, nbuf, twf, q, t, 0);
         uint32_t es[8], eo[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-            es[e] = mod_u64((uint64_t)d[e] * r_self[e], L.cr, q);
-            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], L.cr, q);
+            es[e] = mod_u64((uint64_t)d[e] * r_self[e], cr, q);
+            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], cr, q);
         }
         const uint32_t off = (uint32_t)((size_t)par * 4 * kN + 8 * t) * 4;
         st_async4(sib_c + off + kN * 4, es[0], es[1], es[2], es[3], sib_mbc + 8 * par);
