@@ -379,7 +379,6 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     const int bar = 1 + gp;
     const LimbTables& L = T->limb[l];
     const uint32_t q = L.q;
-    const uint64_t cr = L.cr;
     const uint32_t inv_n = L.inv_n, inv_n_p = L.inv_n_p;
     const CrtK ck = crt_consts(*T);
     for (int i = threadIdx.x; i < kN; i += 512) { twf[i] = L.fwd[i]; twi[i] = L.inv[i]; }
@@ -401,6 +400,14 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     uint32_t r_self[8], r_oth[8];
     ld8(rg + (size_t)(((2 * p + p) * kDeff + gp) * 2 + l) * kN + 8 * t, r_self);
     ld8(rg + (size_t)(((2 * p + (1 - p)) * kDeff + gp) * 2 + l) * kN + 8 * t, r_oth);
+    // Shoup factors of the fixed RGSW values: each product below is then
+    // exact with one high multiply instead of a 64-bit Barrett reduction.
+    uint32_t r_self_p[8], r_oth_p[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        r_self_p[e] = (uint32_t)(((uint64_t)r_self[e] << 32) / q);
+        r_oth_p[e] = (uint32_t)(((uint64_t)r_oth[e] << 32) / q);
+    }
     uint32_t acc[8];
     if (gp == 0) ld8(src_of(start + len - 1) + 8 * t, acc);
     cluster_sync_all();  // every CTA runs and its mbarriers are initialised before any remote access
@@ -449,8 +456,8 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
         uint32_t es[8], eo[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-            es[e] = mod_u64((uint64_t)d[e] * r_self[e], cr, q);
-            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], cr, q);
+            es[e] = csub(shoup_mul(d[e], r_self[e], r_self_p[e], q), q);
+            eo[e] = csub(shoup_mul(d[e], r_oth[e], r_oth_p[e], q), q);
         }
         st8(cp + (size_t)gp * kN + 8 * t, es);
         const uint32_t dstc = peer_c + (uint32_t)((size_t)par * 4 * kN + (size_t)(2 + gp) * kN + 8 * t) * 4;
@@ -516,7 +523,6 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
     const uint32_t t = threadIdx.x;
     const LimbTables& L = T->limb[l];
     const uint32_t q = L.q;
-    const uint64_t cr = L.cr;
     const uint32_t inv_n = L.inv_n, inv_n_p = L.inv_n_p;
     const CrtK ck = crt_consts(*T);
     for (int i = threadIdx.x; i < kN; i += 256) { twf[i] = L.fwd[i]; twi[i] = L.inv[i]; }
@@ -539,6 +545,14 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
     uint32_t r_self[8], r_oth[8];
     ld8(rg + (size_t)(((2 * p + p) * kDeff + j) * 2 + l) * kN + 8 * t, r_self);
     ld8(rg + (size_t)(((2 * p + (1 - p)) * kDeff + j) * 2 + l) * kN + 8 * t, r_oth);
+    // Shoup factors of the fixed RGSW values: each product below is then
+    // exact with one high multiply instead of a 64-bit Barrett reduction.
+    uint32_t r_self_p[8], r_oth_p[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        r_self_p[e] = (uint32_t)(((uint64_t)r_self[e] << 32) / q);
+        r_oth_p[e] = (uint32_t)(((uint64_t)r_oth[e] << 32) / q);
+    }
     uint32_t acc[8];
     ld8(src_of(start + len - 1) + 8 * t, acc);
     cluster_sync_all();  // every CTA runs and its mbarriers are initialised before any remote access
@@ -575,7 +589,7 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
         uint32_t d[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-            const uint32_t own = xown[t + 256 * e], oth = xpart[t + 256 * e];
+            const uint32_t own = acc[e], oth = xpart[t + 256 * e];  // own: still in registers
             int64_t s1, s2;
             decomp2(l ? oth : own, l ? own : oth, ck, s1, s2);
             d[e] = signed_res(j ? s2 : s1, q);
@@ -584,8 +598,8 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
         uint32_t es[8], eo[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
-            es[e] = mod_u64((uint64_t)d[e] * r_self[e], cr, q);
-            eo[e] = mod_u64((uint64_t)d[e] * r_oth[e], cr, q);
+            es[e] = csub(shoup_mul(d[e], r_self[e], r_self_p[e], q), q);
+            eo[e] = csub(shoup_mul(d[e], r_oth[e], r_oth_p[e], q), q);
         }
         const uint32_t off = (uint32_t)((size_t)par * 4 * kN + 8 * t) * 4;
         st_async4(sib_c + off + kN * 4, es[0], es[1], es[2], es[3], sib_mbc + 8 * par);
