@@ -19,6 +19,12 @@
 //   L3: x = (t&3) + 4 e + 32 (t>>2)      s = 4, 3, 2
 //   L4: x = 8 t + e          stages s = 1, 0
 // A forward NTT takes L1 in and leaves L4; the inverse takes L4 to L1.
+// Only L1 <-> L2 moves data between warps: in L2, L3 and L4 warp w holds
+// x in [256w, 256w + 256), a region the swizzle keeps in place, so those
+// exchanges need a warp barrier only.  Each transform starts with a group
+// barrier before its first store, which orders it after the previous
+// transform's reads of the same buffer; the second buffer is only ever
+// touched warp-locally.
 // Several groups can share a CTA, each synchronising on its own named
 // barrier (bar.sync id, 256).
 #pragma once
@@ -169,11 +175,11 @@ __device__ __forceinline__ void ntt_fwd(uint32_t (&r)[8], uint32_t* sbuf, const 
     ntt_stage<5, true>(r, 2, lay_base<2>(t), tw, q);
     ntt_stage<5, true>(r, 1, lay_base<2>(t), tw, q);
     ntt_stage<5, true>(r, 0, lay_base<2>(t), tw, q);
-    lay_store<2>(r, B, t); gsync(bar); lay_load<3>(r, B, t);
+    lay_store<2>(r, B, t); __syncwarp(); lay_load<3>(r, B, t);
     ntt_stage<2, true>(r, 2, lay_base<3>(t), tw, q);
     ntt_stage<2, true>(r, 1, lay_base<3>(t), tw, q);
     ntt_stage<2, true>(r, 0, lay_base<3>(t), tw, q);
-    lay_store<3>(r, A, t); gsync(bar); lay_load<4>(r, A, t);
+    lay_store<3>(r, A, t); __syncwarp(); lay_load<4>(r, A, t);
     ntt_stage<0, true>(r, 1, lay_base<4>(t), tw, q);
     ntt_stage<0, true>(r, 0, lay_base<4>(t), tw, q);
     const uint32_t q2 = 2 * q;
@@ -189,11 +195,11 @@ __device__ __forceinline__ void ntt_inv(uint32_t (&r)[8], uint32_t* sbuf, const 
     ntt_stage<0, false>(r, 0, lay_base<4>(t), tw, q);
     ntt_stage<0, false>(r, 1, lay_base<4>(t), tw, q);
     gsync(bar);
-    lay_store<4>(r, A, t); gsync(bar); lay_load<3>(r, A, t);
+    lay_store<4>(r, A, t); __syncwarp(); lay_load<3>(r, A, t);
     ntt_stage<2, false>(r, 0, lay_base<3>(t), tw, q);
     ntt_stage<2, false>(r, 1, lay_base<3>(t), tw, q);
     ntt_stage<2, false>(r, 2, lay_base<3>(t), tw, q);
-    lay_store<3>(r, B, t); gsync(bar); lay_load<2>(r, B, t);
+    lay_store<3>(r, B, t); __syncwarp(); lay_load<2>(r, B, t);
     ntt_stage<5, false>(r, 0, lay_base<2>(t), tw, q);
     ntt_stage<5, false>(r, 1, lay_base<2>(t), tw, q);
     ntt_stage<5, false>(r, 2, lay_base<2>(t), tw, q);
