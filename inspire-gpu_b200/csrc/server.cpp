@@ -260,18 +260,36 @@ void stage_query_flat(const Server& S, Lane& L, size_t i, const uint64_t* flat, 
     IPB_CK(cudaMemcpyAsync(L.qraw + i * S.qstride, flat, S.qstride * 8, cudaMemcpyHostToDevice, st));
 }
 
+// The five parts of each query land back to back in the lane's flat query
+// buffer.  Parts that also sit back to back in host memory (a flat query, or
+// a batch of them in one array, as the reference client's flattening lays
+// them out) go in one copy: one cudaMemcpyAsync per contiguous run instead
+// of five per query, which matters at 32 queries per batch.
 static void stage_queries(Server* S, const ipir_query_view* qs, size_t count) {
     IPB_CK(cudaSetDevice(S->device));
     const size_t R = S->pp.db_rows;
+    uint64_t* d = S->lane.qraw;
+    const uint64_t* run = nullptr;  // host start of the pending run
+    size_t run_len = 0;             // its length in u64
+    auto part = [&](const uint64_t* src, size_t n) {
+        if (run && src == run + run_len) {
+            run_len += n;
+            return;
+        }
+        if (run) IPB_CK(cudaMemcpyAsync(d, run, run_len * 8, cudaMemcpyHostToDevice, S->stream));
+        d += run_len;
+        run = src;
+        run_len = n;
+    };
     for (size_t i = 0; i < count; ++i) {
-        uint64_t* d = S->lane.qraw + i * S->qstride;
         const ipir_query_view& v = qs[i];
-        IPB_CK(cudaMemcpyAsync(d, v.lwe_b_limb0, R * 8, cudaMemcpyHostToDevice, S->stream));
-        IPB_CK(cudaMemcpyAsync(d + R, v.lwe_b_limb1, R * 8, cudaMemcpyHostToDevice, S->stream));
-        IPB_CK(cudaMemcpyAsync(d + 2 * R, v.ksk5_b, kBlk * 8, cudaMemcpyHostToDevice, S->stream));
-        IPB_CK(cudaMemcpyAsync(d + 2 * R + kBlk, v.kskneg1_b, kBlk * 8, cudaMemcpyHostToDevice, S->stream));
-        IPB_CK(cudaMemcpyAsync(d + 2 * R + 2 * kBlk, v.rgsw, 4 * kBlk * 8, cudaMemcpyHostToDevice, S->stream));
+        part(v.lwe_b_limb0, R);
+        part(v.lwe_b_limb1, R);
+        part(v.ksk5_b, kBlk);
+        part(v.kskneg1_b, kBlk);
+        part(v.rgsw, 4 * kBlk);
     }
+    if (run) IPB_CK(cudaMemcpyAsync(d, run, run_len * 8, cudaMemcpyHostToDevice, S->stream));
     S->staged = count;
 }
 

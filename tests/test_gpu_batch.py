@@ -109,3 +109,38 @@ def test_tensor_pass_beside_matvec(batch_env, tp_sms):
         srv.set_schedule(n, matvec_tc=1, horner_cluster=1)
     with pytest.raises(Exception):
         srv.set_schedule(4, matvec_tc=0, horner_cluster=1, tp_sms=8)   # CUDA-core mat-vec: no split
+
+
+def test_views_contiguous_or_scattered(batch_env):
+    """ipir_answer_batch copies each run of query parts that is contiguous in
+    host memory at once: a whole batch in one array (one copy), flat queries
+    (one copy each) and views whose five parts live in separate arrays (five
+    copies each) give the same responses."""
+    import inspire_b200 as ib
+    c, srv, qs, sts = batch_env
+    want = srv.answer_batch(qs)
+    n = len(qs)
+    rn = ib.response_u64s(srv.params)
+    batch = np.ascontiguousarray(np.stack(qs))            # [n][flat] in one array
+    views = (ib.IpirQueryView * n)()
+    for i in range(n):
+        views[i] = ib.query_view_from_flat(srv.params, batch[i])
+    out = np.zeros((n, rn), np.uint64)
+    assert srv.answer_batch_rc(views, n, out) == 0
+    assert (out == want).all()
+    R = srv.params["db_rows"]
+    blk = 2 * 2 * 2048
+    keep = []
+    scattered = (ib.IpirQueryView * n)()
+    for i in range(n - 1, -1, -1):                         # parts out of order in memory
+        q = qs[i]
+        parts = [q[:R].copy(), q[R:2 * R].copy(), q[2 * R:2 * R + blk].copy(),
+                 q[2 * R + blk:2 * R + 2 * blk].copy(), q[2 * R + 2 * blk:].copy()]
+        keep.append(parts)
+        v = ib.IpirQueryView()
+        for name, a in zip(("lwe_b_limb0", "lwe_b_limb1", "ksk5_b", "kskneg1_b", "rgsw"), parts):
+            setattr(v, name, a.ctypes.data_as(ib.u64p))
+        scattered[i] = v
+    out2 = np.zeros((n, rn), np.uint64)
+    assert srv.answer_batch_rc(scattered, n, out2) == 0
+    assert (out2 == want).all()
