@@ -293,6 +293,50 @@ static void stage_queries(Server* S, const ipir_query_view* qs, size_t count) {
     S->staged = count;
 }
 
+// Host -> device copy of parts [p0, p0 + np) of every query (0, 1: the LWE
+// limbs; 2, 3, 4: KSK5, KSK-1, RGSW) into their place in the lane's flat
+// query buffer.  One 2-D copy when each query's parts are back to back in
+// host memory at a constant stride between queries (a flat batch array),
+// else one copy per host-contiguous run.
+static void stage_parts(const Server& S, const ipir_query_view* qs, size_t count, int p0, int np, cudaStream_t st) {
+    const size_t R = S.pp.db_rows;
+    const size_t len[5] = {R, R, kBlk, kBlk, 4 * kBlk};
+    const size_t off[5] = {0, R, 2 * R, 2 * R + kBlk, 2 * R + 2 * kBlk};
+    auto ptr = [&](size_t i, int p) -> const uint64_t* {
+        const ipir_query_view& v = qs[i];
+        return p == 0 ? v.lwe_b_limb0 : p == 1 ? v.lwe_b_limb1 : p == 2 ? v.ksk5_b : p == 3 ? v.kskneg1_b : v.rgsw;
+    };
+    size_t width = 0;
+    for (int p = p0; p < p0 + np; ++p) width += len[p];
+    bool strided = true;
+    for (size_t i = 0; i < count && strided; ++i) {
+        for (int p = p0 + 1; p < p0 + np; ++p) strided = strided && ptr(i, p) == ptr(i, p - 1) + len[p - 1];
+        if (i > 0) strided = strided && ptr(i, p0) - ptr(i - 1, p0) == ptr(1, p0) - ptr(0, p0);
+    }
+    if (strided && count > 1 && ptr(1, p0) - ptr(0, p0) >= (ptrdiff_t)width) {
+        IPB_CK(cudaMemcpy2DAsync(S.lane.qraw + off[p0], S.qstride * 8, ptr(0, p0), (ptr(1, p0) - ptr(0, p0)) * 8,
+                                 width * 8, count, cudaMemcpyHostToDevice, st));
+        return;
+    }
+    for (size_t i = 0; i < count; ++i) {
+        uint64_t* d = S.lane.qraw + i * S.qstride + off[p0];
+        const uint64_t* run = ptr(i, p0);
+        size_t run_len = len[p0];
+        for (int p = p0 + 1; p <= p0 + np; ++p) {
+            if (p < p0 + np && ptr(i, p) == run + run_len) {
+                run_len += len[p];
+                continue;
+            }
+            IPB_CK(cudaMemcpyAsync(d, run, run_len * 8, cudaMemcpyHostToDevice, st));
+            d += run_len;
+            if (p < p0 + np) {
+                run = ptr(i, p);
+                run_len = len[p];
+            }
+        }
+    }
+}
+
 const Sched& sched_for(const Server& S, size_t c) { return S.sched[std::min(c, S.sched.size() - 1)]; }
 
 int lane_gt_pass(const Server& S, size_t cap) {
@@ -312,7 +356,11 @@ std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
 
 // Query prep, mat-vec, tensor pass, finalize: the part that streams the DB
 // and the precomputed tensors.
-static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev) {
+// lwe_ready (optional): the queries' LWE vectors arrive later than their
+// key parts (copied on another stream, this event marks them); the key side
+// (query prep, tensor pass) then runs first and the mat-vec after the event.
+static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
+                        cudaEvent_t lwe_ready = nullptr) {
     const Params& pp = S.pp;
     const Precomp& P = *S.pre;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
@@ -340,6 +388,10 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
         tensor_pass(L.aux, sc.tp_sms);
         IPB_CK(cudaEventRecord(L.join, L.aux));
     }
+    if (lwe_ready && !beside) {
+        tensor_pass(st, S.num_sms);
+        IPB_CK(cudaStreamWaitEvent(st, lwe_ready, 0));
+    }
     int mv_parts;
     if (sc.matvec_tc) {
         IPB_CK(launch_qplanes(L.qraw, S.qstride, R, P.tables, L.planes, nq, st));
@@ -364,7 +416,7 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
     if (beside)
         IPB_CK(cudaStreamWaitEvent(st, L.join, 0));  // stage times: mat-vec = both, tensor pass = 0
     if (ev) IPB_CK(cudaEventRecord(ev[2], st));
-    if (!beside) tensor_pass(st, S.num_sms);
+    if (!beside && !lwe_ready) tensor_pass(st, S.num_sms);
     if (ev) IPB_CK(cudaEventRecord(ev[3], st));
     IPB_CK(launch_finalize(L.mvpart, S.mv_qstride, mv_parts, C, L.tp_out, P.pre_df, L.keys, kKeyStride, P.tables,
                            L.packed_b, S.pb_qstride, G, nq, st));
@@ -407,6 +459,30 @@ static void run_pipeline(Server* S, size_t count) {
     IPB_CK(cudaSetDevice(S->device));
     S->launches += (unsigned long long)run_pipeline(*S, S->lane, sched_for(*S, count), count, S->stream,
                                                     S->timing ? S->ev : nullptr);
+}
+
+// The blocking answer from host views: the key parts are copied first and
+// the query prep and tensor pass (which need only them) start while the
+// LWE vectors are still crossing PCIe on the lane's second stream; the
+// mat-vec waits for those.  Schedules that already run the tensor pass on
+// the second stream stage everything first instead.
+static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
+    IPB_CK(cudaSetDevice(S->device));
+    const Sched& sc = sched_for(*S, count);
+    if (sc.tp_sms > 0 || S->timing) {
+        stage_queries(S, qs, count);
+        S->launches += (unsigned long long)run_pipeline(*S, S->lane, sc, count, S->stream, S->timing ? S->ev : nullptr);
+        return;
+    }
+    Lane& L = S->lane;
+    IPB_CK(cudaEventRecord(L.fork, S->stream));  // the lane's buffers are free from here on
+    IPB_CK(cudaStreamWaitEvent(L.aux, L.fork, 0));
+    stage_parts(*S, qs, count, 2, 3, S->stream);  // keys and RGSW: needed first
+    stage_parts(*S, qs, count, 0, 2, L.aux);      // LWE vectors: needed by the mat-vec only
+    IPB_CK(cudaEventRecord(L.join, L.aux));
+    S->staged = count;
+    S->launches += (unsigned long long)run_db_phase(*S, L, sc, count, S->stream, nullptr, L.join);
+    S->launches += (unsigned long long)run_horner_phase(*S, L, sc, count, S->stream, nullptr);
 }
 
 // A kernel whose pipeline wait ran out of iterations leaves a code in the
@@ -669,8 +745,7 @@ void gpu_answer_batch(GpuServerCtx* ctx, const ipir_query_view* queries, size_t 
     if (rc == 2) throw std::invalid_argument("gpu_answer_batch: count exceeds max_batch");
     if (rc) throw std::invalid_argument("gpu_answer_batch: null argument");
     if (count == 0) return;
-    ipb::stage_queries(ctx->s, queries, count);
-    ipb::run_pipeline(ctx->s, count);
+    ipb::stage_and_run(ctx->s, queries, count);
     ipb::fetch(ctx->s, count, out);
 }
 
@@ -776,8 +851,7 @@ int ipir_answer_batch(ipir_server* srv, const ipir_query_view* queries, size_t c
     if (count == 0) return 0;
     return guarded(
         [&]() -> int {
-            ipb::stage_queries(srv->s, queries, count);
-            ipb::run_pipeline(srv->s, count);
+            ipb::stage_and_run(srv->s, queries, count);
             ipb::fetch(srv->s, count, out_resp);
             return 0;
         },
