@@ -31,7 +31,8 @@
 // Warp roles (768 threads): 0 TMA producer (one thread), 1 TMEM allocation
 // and MMA issue (one thread), 4..7 epilogue, 8..23 key planes in four
 // groups of 128 threads, group g filling the K tiles kt = g mod 4, so four
-// stages' gathers are in flight at once.
+// stages' gathers are in flight at once.  With fewer stages than groups the
+// groups that fill none join the epilogue.
 #include <cuda.h>
 
 #include <algorithm>
@@ -150,8 +151,8 @@ __device__ __forceinline__ void st_sw128(uint8_t* tile, uint32_t row, uint32_t c
 // One lane's row (g, a) over 4 queries' 16 accumulator columns (byte plane
 // b of query k at column 4k + b): part_k = sum_b (256^(a+b) mod q) P[4k + b]
 // (< 2^60, unreduced), then summed over the 4 lanes a of group g as a
-// reduce-scatter, so that lane a returns query a's total.  Round 1 (xor 1) keeps queries a & 1 and
-// (a & 1) + 2, round 2 (xor 2) keeps query a.
+// reduce-scatter, so that lane a returns query a's total.  Round 1 (xor 1)
+// keeps queries a & 1 and (a & 1) + 2, round 2 (xor 2) keeps query a.
 __device__ __forceinline__ uint64_t tp_reduce4(const uint32_t (&v)[16], const uint32_t* c, int a) {
     uint64_t part[4];
 #pragma unroll
@@ -227,7 +228,10 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
         abort_flag = 0;
         // full: the producer's expect_tx arrival (A bytes) + the key group of the stage
         for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1 + kKeyGroup); mbar_init(&empty[s], 1); }
-        for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128); }
+        // tempty: 128 epilogue threads per share (warps 4..7 and each key
+        // group that fills no stages)
+        const int shares = 1 + kKeyGroups - (S < kKeyGroups ? S : kKeyGroups);
+        for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128 * shares); }
         for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 128 + kKeyThreads); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -245,6 +249,70 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
     const int acc_cols = P.mti * P.nb;
     const int slot_rows = 4 * P.G;  // A rows of one slot
 
+    // Epilogue (TMEM -> reduced tensor-pass values) for the rows of lane
+    // quarter wq: warps 4..7 run it, and so do the warps of key groups that
+    // fill no stages (fewer stages than groups), each taking every nshare-th
+    // 16-column chunk, so the accumulators drain sooner when the MMA waits
+    // for them (one TMEM accumulator stage at 32 queries and G >= 97).
+    auto epilogue = [&](const int wq, const int share, const int nshare) {
+        const uint32_t lane_base = (uint32_t)(wq * 32) << 16;
+        int as = 0;
+        uint32_t aph = 0;
+        for (int it = 0;; ++it) {
+            const int r = it % kRing;
+            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 18)) { abort_flag = 1; break; }
+            const int item = item_ring[r];
+            mbar_arrive(&iempty[r]);
+            if (item < 0) break;
+            if (!mbar_wait(&tfull[as], aph, P.err, 15)) { abort_flag = 1; break; }
+            tc_fence_after();
+            const int li0 = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
+            const int l = li0 / kN;
+            const uint32_t* c = P.c[l];
+            // spi == 1: TMEM block mt (columns mt * nb) holds M-tile mt of the
+            // slot's 4G rows.  spi > 1: lane row = sl * 4G + g*4 + a, and slot
+            // sl's keys are columns sl * rq ..; the loop runs over the slots
+            // this warp's 32 lanes touch (warp-uniform bounds for tcgen05.ld).
+            const int row = wq * 32 + lane;
+            const int nblk = P.spi > 1 ? min(P.spi - 1, (wq * 32 + 31) / slot_rows) - (wq * 32) / slot_rows + 1
+                                       : P.mti;
+            const int blk0 = P.spi > 1 ? (wq * 32) / slot_rows : 0;
+            const int nqc = (P.nq + 3) / 4;  // 16-column chunks per block
+            for (int bi = 0; bi < nblk; ++bi) {
+                const int mt = blk0 + bi;
+                const int li = li0 + (P.spi > 1 ? mt : 0);
+                const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;  // g*4 + a
+                const int g = grow >> 2, a = grow & 3;
+                const bool valid = grow >= 0 && grow < slot_rows;
+                // four queries (16 columns) per TMEM load where the block has
+                // them; the block's last columns one query at a time
+                const int lim = P.spi > 1 ? P.nb : (mt + 1) * P.nb;
+                for (int q = 0; q < P.nq; q += 4) {
+                    if ((bi * nqc + q / 4) % nshare != share) continue;  // this warp's share of the chunks
+                    const int col = (P.spi > 1 ? mt * P.rq : mt * P.nb) + 4 * q;
+                    const uint32_t ta = tmem_base + lane_base + (uint32_t)(as * acc_cols + col);
+                    uint32_t v[16];
+                    if (col + 16 <= lim) {
+                        tmem_ld16(ta, v);
+                    } else {
+    #pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            uint32_t t[4] = {0, 0, 0, 0};
+                            if (col + 4 * k + 4 <= lim) tmem_ld4(ta + 4 * k, t);
+    #pragma unroll
+                            for (int e = 0; e < 4; ++e) v[4 * k + e] = t[e];
+                        }
+                    }
+                    const uint64_t tot = tp_reduce4(v, c, a);
+                    if (valid && q + a < P.nq)
+                        P.out[((size_t)li * P.nq_total + P.q0 + q + a) * P.G + g] = mod_u64(tot, P.cr[l], P.q[l]);
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[as]);
+            if (++as == P.acc_stages) { as = 0; aph ^= 1; }
+        }
+    };
     if (warp == 0) {
         if (lane == 0) {
             int s = 0;
@@ -337,120 +405,69 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
         const int kid = (warp - 8) * 32 + lane;
         const int grp = kid / kKeyGroup, gk = kid % kKeyGroup;
         const int ngrp = S < kKeyGroups ? S : kKeyGroups;
-        const int units = P.spi * P.w8 * 32;
-        const int W = 8 * P.w8;
-        int base = 0;  // stages issued before this item
-        for (int it = 0;; ++it, base += ktiles) {
-            const int r = it % kRing;
-            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 19)) { abort_flag = 1; break; }
-            const int item = item_ring[r];
-            mbar_arrive(&iempty[r]);
-            if (item < 0) break;
-            const int li0 = (item / P.n_mg) * P.spi;
-            const int l = li0 / kN;
-            const uint32_t* kl = P.keyt + (size_t)l * kDeff * kN * W;  // [j][p][W]
-            for (int kt = grp; grp < ngrp && kt < ktiles; kt += ngrp) {
-                const int seq = base + kt, s = seq % S;
-                const uint32_t ph = (uint32_t)(seq / S) & 1;
-                if (!mbar_wait(&empty[s], ph ^ 1, P.err, 20)) { abort_flag = 1; break; }
-                uint8_t* bt = smem + (size_t)s * stage_bytes + a_region;
-                for (int unit = gk; unit < units; unit += kKeyGroup) {
-                    const int u4 = unit & 31, sq = unit >> 5;
-                    const int sl = sq / P.w8, q8 = sq - sl * P.w8;
-                    const uint32_t odd = 2 * brev11((uint32_t)((li0 + sl) & (kN - 1))) + 1;
-                    const int w0 = kt * 64 + u4 * 2;  // even: w0 and w0 + 1 both < 2046 or both not
-                    uint32_t v[4][8];
-                    if (w0 < 2 * kSteps) {
-                        const uint2 tt = *reinterpret_cast<const uint2*>(&tw[w0]);
-                        const uint32_t p0 = perm_from_odd(tt.x, odd), p1 = perm_from_odd(tt.y, odd);
-                        ld_sector(kl + (size_t)p0 * W + 8 * q8, v[0]);          // w0, j = 0
-                        ld_sector(kl + ((size_t)kN + p0) * W + 8 * q8, v[1]);   // w0, j = 1
-                        ld_sector(kl + (size_t)p1 * W + 8 * q8, v[2]);          // w0 + 1, j = 0
-                        ld_sector(kl + ((size_t)kN + p1) * W + 8 * q8, v[3]);   // w0 + 1, j = 1
-                    } else {
+        if (grp >= ngrp) {
+            epilogue(warp & 3, 1 + grp - ngrp, 1 + kKeyGroups - ngrp);
+        } else {
+            const int units = P.spi * P.w8 * 32;
+            const int W = 8 * P.w8;
+            int base = 0;  // stages issued before this item
+            for (int it = 0;; ++it, base += ktiles) {
+                const int r = it % kRing;
+                if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 19)) { abort_flag = 1; break; }
+                const int item = item_ring[r];
+                mbar_arrive(&iempty[r]);
+                if (item < 0) break;
+                const int li0 = (item / P.n_mg) * P.spi;
+                const int l = li0 / kN;
+                const uint32_t* kl = P.keyt + (size_t)l * kDeff * kN * W;  // [j][p][W]
+                for (int kt = grp; grp < ngrp && kt < ktiles; kt += ngrp) {
+                    const int seq = base + kt, s = seq % S;
+                    const uint32_t ph = (uint32_t)(seq / S) & 1;
+                    if (!mbar_wait(&empty[s], ph ^ 1, P.err, 20)) { abort_flag = 1; break; }
+                    uint8_t* bt = smem + (size_t)s * stage_bytes + a_region;
+                    for (int unit = gk; unit < units; unit += kKeyGroup) {
+                        const int u4 = unit & 31, sq = unit >> 5;
+                        const int sl = sq / P.w8, q8 = sq - sl * P.w8;
+                        const uint32_t odd = 2 * brev11((uint32_t)((li0 + sl) & (kN - 1))) + 1;
+                        const int w0 = kt * 64 + u4 * 2;  // even: w0 and w0 + 1 both < 2046 or both not
+                        uint32_t v[4][8];
+                        if (w0 < 2 * kSteps) {
+                            const uint2 tt = *reinterpret_cast<const uint2*>(&tw[w0]);
+                            const uint32_t p0 = perm_from_odd(tt.x, odd), p1 = perm_from_odd(tt.y, odd);
+                            ld_sector(kl + (size_t)p0 * W + 8 * q8, v[0]);          // w0, j = 0
+                            ld_sector(kl + ((size_t)kN + p0) * W + 8 * q8, v[1]);   // w0, j = 1
+                            ld_sector(kl + (size_t)p1 * W + 8 * q8, v[2]);          // w0 + 1, j = 0
+                            ld_sector(kl + ((size_t)kN + p1) * W + 8 * q8, v[3]);   // w0 + 1, j = 1
+                        } else {
 #pragma unroll
-                        for (int e = 0; e < 4; ++e)
+                            for (int e = 0; e < 4; ++e)
 #pragma unroll
-                            for (int c = 0; c < 8; ++c) v[e][c] = 0;
+                                for (int c = 0; c < 8; ++c) v[e][c] = 0;
+                        }
+                        const uint32_t col = (uint32_t)u4 * 4;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            const int q = q8 * 8 + c;
+                            if (q >= P.nq) break;
+                            const uint32_t lo01 = __byte_perm(v[0][c], v[1][c], 0x5140);
+                            const uint32_t lo23 = __byte_perm(v[2][c], v[3][c], 0x5140);
+                            const uint32_t hi01 = __byte_perm(v[0][c], v[1][c], 0x7362);
+                            const uint32_t hi23 = __byte_perm(v[2][c], v[3][c], 0x7362);
+                            const uint32_t row0 = (uint32_t)(sl * P.rq + q * 4);
+                            st_sw128(bt, row0 + 0, col, __byte_perm(lo01, lo23, 0x5410));  // byte 0 of u..u+3
+                            st_sw128(bt, row0 + 1, col, __byte_perm(lo01, lo23, 0x7632));  // byte 1
+                            st_sw128(bt, row0 + 2, col, __byte_perm(hi01, hi23, 0x5410));  // byte 2
+                            st_sw128(bt, row0 + 3, col, __byte_perm(hi01, hi23, 0x7632));  // byte 3
+                        }
                     }
-                    const uint32_t col = (uint32_t)u4 * 4;
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        const int q = q8 * 8 + c;
-                        if (q >= P.nq) break;
-                        const uint32_t lo01 = __byte_perm(v[0][c], v[1][c], 0x5140);
-                        const uint32_t lo23 = __byte_perm(v[2][c], v[3][c], 0x5140);
-                        const uint32_t hi01 = __byte_perm(v[0][c], v[1][c], 0x7362);
-                        const uint32_t hi23 = __byte_perm(v[2][c], v[3][c], 0x7362);
-                        const uint32_t row0 = (uint32_t)(sl * P.rq + q * 4);
-                        st_sw128(bt, row0 + 0, col, __byte_perm(lo01, lo23, 0x5410));  // byte 0 of u..u+3
-                        st_sw128(bt, row0 + 1, col, __byte_perm(lo01, lo23, 0x7632));  // byte 1
-                        st_sw128(bt, row0 + 2, col, __byte_perm(hi01, hi23, 0x5410));  // byte 2
-                        st_sw128(bt, row0 + 3, col, __byte_perm(hi01, hi23, 0x7632));  // byte 3
-                    }
+                    // generic-proxy stores -> visible to the tensor core's async proxy
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    mbar_arrive(&full[s]);
                 }
-                // generic-proxy stores -> visible to the tensor core's async proxy
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(&full[s]);
             }
         }
     } else if (warp >= 4) {
-        const int wq = warp & 3;
-        const uint32_t lane_base = (uint32_t)(wq * 32) << 16;
-        int as = 0;
-        uint32_t aph = 0;
-        for (int it = 0;; ++it) {
-            const int r = it % kRing;
-            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 18)) { abort_flag = 1; break; }
-            const int item = item_ring[r];
-            mbar_arrive(&iempty[r]);
-            if (item < 0) break;
-            if (!mbar_wait(&tfull[as], aph, P.err, 15)) { abort_flag = 1; break; }
-            tc_fence_after();
-            const int li0 = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
-            const int l = li0 / kN;
-            const uint32_t* c = P.c[l];
-            // spi == 1: TMEM block mt (columns mt * nb) holds M-tile mt of the
-            // slot's 4G rows.  spi > 1: lane row = sl * 4G + g*4 + a, and slot
-            // sl's keys are columns sl * rq ..; the loop runs over the slots
-            // this warp's 32 lanes touch (warp-uniform bounds for tcgen05.ld).
-            const int row = wq * 32 + lane;
-            const int nblk = P.spi > 1 ? min(P.spi - 1, (wq * 32 + 31) / slot_rows) - (wq * 32) / slot_rows + 1
-                                       : P.mti;
-            const int blk0 = P.spi > 1 ? (wq * 32) / slot_rows : 0;
-            for (int bi = 0; bi < nblk; ++bi) {
-                const int mt = blk0 + bi;
-                const int li = li0 + (P.spi > 1 ? mt : 0);
-                const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;  // g*4 + a
-                const int g = grow >> 2, a = grow & 3;
-                const bool valid = grow >= 0 && grow < slot_rows;
-                // four queries (16 columns) per TMEM load where the block has
-                // them; the block's last columns one query at a time
-                const int lim = P.spi > 1 ? P.nb : (mt + 1) * P.nb;
-                for (int q = 0; q < P.nq; q += 4) {
-                    const int col = (P.spi > 1 ? mt * P.rq : mt * P.nb) + 4 * q;
-                    const uint32_t ta = tmem_base + lane_base + (uint32_t)(as * acc_cols + col);
-                    uint32_t v[16];
-                    if (col + 16 <= lim) {
-                        tmem_ld16(ta, v);
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            uint32_t t[4] = {0, 0, 0, 0};
-                            if (col + 4 * k + 4 <= lim) tmem_ld4(ta + 4 * k, t);
-#pragma unroll
-                            for (int e = 0; e < 4; ++e) v[4 * k + e] = t[e];
-                        }
-                    }
-                    const uint64_t tot = tp_reduce4(v, c, a);
-                    if (valid && q + a < P.nq)
-                        P.out[((size_t)li * P.nq_total + P.q0 + q + a) * P.G + g] = mod_u64(tot, P.cr[l], P.q[l]);
-                }
-            }
-            tc_fence_before();
-            mbar_arrive(&tempty[as]);
-            if (++as == P.acc_stages) { as = 0; aph ^= 1; }
-        }
+        epilogue(warp & 3, 0, 1 + kKeyGroups - (S < kKeyGroups ? S : kKeyGroups));
     }
     tc_fence_before();
     __syncthreads();
