@@ -4,7 +4,7 @@
 
 #include <cstring>
 #include <mutex>
-#include <set>
+#include <map>
 #include <utility>
 #include <stdexcept>
 
@@ -171,22 +171,24 @@ int setup_geometry(size_t n_entries, size_t w, size_t db_rows, Params* out, cons
     return 0;
 }
 
-cudaError_t allow_max_dynamic_smem(const void* kernel) {
+cudaError_t allow_max_dynamic_smem(const void* kernel, size_t* max_dynamic) {
     static std::mutex mu;
-    static std::set<std::pair<const void*, int>> done;
+    static std::map<std::pair<const void*, int>, size_t> done;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e) return e;
     std::lock_guard<std::mutex> lk(mu);
-    if (done.count({kernel, dev})) return cudaSuccess;
-    int optin = 0;
-    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
-    cudaFuncAttributes fa{};
-    if ((e = cudaFuncGetAttributes(&fa, kernel))) return e;
-    if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  optin - (int)fa.sharedSizeBytes)))
-        return e;
-    done.insert({kernel, dev});
+    auto it = done.find({kernel, dev});
+    if (it == done.end()) {
+        int optin = 0;
+        if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev))) return e;
+        cudaFuncAttributes fa{};
+        if ((e = cudaFuncGetAttributes(&fa, kernel))) return e;
+        const int dyn = optin - (int)fa.sharedSizeBytes;
+        if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn))) return e;
+        it = done.emplace(std::make_pair(kernel, dev), (size_t)dyn).first;
+    }
+    if (max_dynamic) *max_dynamic = it->second;
     return cudaSuccess;
 }
 

@@ -38,11 +38,12 @@ void set_last_error(const char* msg);
 // Raises a kernel's dynamic shared-memory limit to the device's opt-in
 // maximum (less the kernel's static shared memory), once per kernel and
 // device.  The limit is then the same for every later launch and for every
-// captured graph, whatever size one launch asks for.
-cudaError_t allow_max_dynamic_smem(const void* kernel);
+// captured graph, whatever size one launch asks for.  *max_dynamic (if
+// given) receives that limit in bytes.
+cudaError_t allow_max_dynamic_smem(const void* kernel, size_t* max_dynamic = nullptr);
 template <class K>
-inline cudaError_t allow_max_smem(K* kernel) {
-    return allow_max_dynamic_smem(reinterpret_cast<const void*>(kernel));
+inline cudaError_t allow_max_smem(K* kernel, size_t* max_dynamic = nullptr) {
+    return allow_max_dynamic_smem(reinterpret_cast<const void*>(kernel), max_dynamic);
 }
 
 }  // namespace ipb

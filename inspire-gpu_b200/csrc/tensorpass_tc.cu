@@ -590,13 +590,16 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     }
     const size_t a_region = (size_t)P.mti * 128 * 128;
     const size_t stage_bytes = a_region + (size_t)P.nb * 128;
-    P.stages = (int)std::min<size_t>(8, (200 * 1024) / stage_bytes);
+    // As many stages as the device's shared memory takes (1 KB alignment
+    // slack, 256 B of barriers): at 128 groups, three up to 16 queries.
+    size_t max_dyn = 0;
+    e = allow_max_smem(tp_tc_kernel, &max_dyn);
+    if (e) return e;
+    P.stages = (int)std::min<size_t>(8, (max_dyn - 1024 - 256) / stage_bytes);
     if (P.stages < 2) return cudaErrorInvalidValue;
     CUtensorMap ma;
     if (!make_map(&ma, Dt, (uint64_t)2 * kN * 4 * G, (uint32_t)P.rows_box)) return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
-    e = allow_max_smem(tp_tc_kernel);
-    if (e) return e;
     const int items = (2 * kN / P.spi) * P.n_mg;
     if ((e = cudaMemsetAsync(tiles, 0, sizeof(unsigned), s))) return e;
     tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), kTpThreads, smem, s>>>(ma, P);

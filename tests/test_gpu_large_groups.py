@@ -1,6 +1,7 @@
 """128 packing groups (the 16 GB geometry's group count) on a 2048-row DB:
 the tensor-pass GEMM then holds four 128-row M tiles per slot and only two
-or three pipeline stages fit in shared memory.  The oracle is too slow at
+or three pipeline stages fit in shared memory (the key groups that fill no
+stage share the epilogue).  The oracle is too slow at
 this size, so parity is size-independent: batches equal single answers,
 and every response decrypts through the reference client's extract() to
 the queried entry."""
@@ -32,7 +33,7 @@ def env():
 def test_batches_equal_singles_and_decrypt(env):
     c, srv, qs, sts = env
     singles = np.stack([srv.answer(q) for q in qs])           # 1 query per pass: 3 stages
-    assert (srv.answer_batch(qs) == singles).all()            # 8 queries per pass: 2 stages
+    assert (srv.answer_batch(qs) == singles).all()            # 8 queries per pass: 3 stages
     assert (srv.answer_batch(qs[:3]) == singles[:3]).all()    # 3 queries per pass: 3 stages
     for i, st in enumerate(sts):
         assert (st.extract(singles[i]) == c.expected_slots(IDX[i])).all(), i
@@ -42,7 +43,8 @@ def test_batches_equal_singles_and_decrypt(env):
 def test_full_pass_of_32_queries(env):
     """32 queries in one pass: N = 128 key columns per M tile, so the four
     M tiles' accumulators fill TMEM and the epilogue drains one item before
-    the next item's MMAs start; 29 queries leave a ragged last column block."""
+    the next item's MMAs start; two stages, so two key groups share the
+    epilogue; 29 queries leave a ragged last column block."""
     c, srv, qs, sts = env
     more = [c.query(int(i), 7100 + k) for k, i in enumerate(np.random.default_rng(9).integers(0, c.n_entries, 24))]
     qs32 = qs + [q for q, _ in more]
