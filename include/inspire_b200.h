@@ -129,6 +129,25 @@ int ipir_b200_export_precomp(const ipir_server* srv, size_t group, uint32_t* a, 
 /* Copy rows [row0, row0+nrows) of the encoded device DB to the host. */
 int ipir_b200_export_db(const ipir_server* srv, size_t row0, size_t nrows, uint16_t* out);
 
+/* Server checkpoints.  No counterpart in the reference, whose server state
+ * lives only in device memory (a restart re-runs gpu_preprocess on the raw
+ * DB).  save writes the handle's resident state -- the encoded DB, the
+ * precomputed a, D (as the tensor pass's byte planes) and D_final tensors,
+ * and the public parameters including the CRS seed -- to `path`, each
+ * section with a checksum computed on the device: 0, 1 null argument,
+ * 4 CUDA failure, 5 I/O error (text in ipir_b200_last_error).  load
+ * restores it into a new handle on the current device without the raw DB
+ * and without preprocessing; responses are bit-identical to the saved
+ * handle's.  It returns NULL (text in ipir_b200_last_error) for a missing,
+ * truncated or foreign file, a geometry setup() rejects, or a checksum
+ * mismatch; the file is checked before any device memory is allocated.
+ * Layout (little-endian): "IPIRB200", u32 version 1, u32 header bytes 256,
+ * u64 n_entries, entry_bytes, db_rows, db_cols, n_packed, interp_d, num_cts,
+ * 64 seed bytes, u64 section bytes[4] and checksums[4] (db, a, d byte
+ * planes, d_final), zero padding to 256, then the sections. */
+int ipir_b200_save_server(const ipir_server* srv, const char* path);
+ipir_server* ipir_b200_load_server(const char* path, size_t max_batch, ipir_params* out_params);
+
 /* GPU primitives on host buffers (current device), the kernels the server
  * runs.  ntt: in-place forward (inverse = 0) or inverse NTT of n polys of
  * 2048 residues; poly i is mod q_((i / limb_run) & 1).  decomp: n polys

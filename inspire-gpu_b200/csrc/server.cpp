@@ -61,16 +61,21 @@ DevTables* upload_tables(DevArena& A, cudaStream_t s) {
 }
 
 // gpu_preprocess (reference src/gpu_protocol.cu:535-817) on one stream.
-static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s) {
-    const Params& pp = P.pp;
-    const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
-    const size_t d_act = std::min(pp.D, G);
+void alloc_precomp(Precomp& P, cudaStream_t s) {
+    const size_t R = P.pp.db_rows, C = P.pp.db_cols, G = P.pp.n_packed;
     DevArena& A = P.arena;
     P.tables = upload_tables(A, s);
     P.db = A.alloc<uint16_t>(R * C);
     P.pre_a = A.alloc<uint32_t>(G * kGroupStrideA);
     P.pre_dt = A.alloc<uint8_t>(tp_dt_bytes(G));
     P.pre_df = A.alloc<uint32_t>(G * kGroupStrideF);
+}
+
+static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s) {
+    const Params& pp = P.pp;
+    const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
+    const size_t d_act = std::min(pp.D, G);
+    alloc_precomp(P, s);
 
     DevArena tmp;
     try {
@@ -220,7 +225,7 @@ void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
     IPB_CK(cudaDeviceSynchronize());
 }
 
-static Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_t max_batch) {
+Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_t max_batch) {
     if (max_batch == 0) throw std::invalid_argument("gpu_setup_server: max_batch must be >= 1");
     if (!pre || pre->adopted) throw std::invalid_argument("gpu_setup_server: preprocess data missing or adopted");
     auto S = std::make_unique<Server>();
@@ -773,7 +778,9 @@ int guarded(F&& f, int fail_code) {
     }
     return fail_code;
 }
-void fill_params(const ipb::Params& pp, ipir_params* o) {
+}  // namespace
+
+void ipb::fill_params(const ipb::Params& pp, ipir_params* o) {
     o->n_entries = pp.n_entries;
     o->entry_bytes = pp.w;
     o->db_rows = pp.db_rows;
@@ -785,7 +792,8 @@ void fill_params(const ipb::Params& pp, ipir_params* o) {
     o->d_eff = ipb::kDeff;
     std::memcpy(o->seed, pp.seed, 64);
 }
-}  // namespace
+
+using ipb::fill_params;
 
 extern "C" {
 

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "host_util.h"
+#include "inspire_b200.h"
 #include "ipb_launch.h"
 
 namespace ipb {
@@ -148,6 +149,12 @@ struct Server {
 // Bytes of a lane of `cap` queries whose Gt holds `gt_pass` queries.
 size_t lane_bytes(const Server& S, size_t cap, int gt_pass);
 void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass);
+// Device buffers of a server's resident state (tables, DB, a, D byte planes,
+// D_final) for P.pp, on P.device.
+void alloc_precomp(Precomp& P, cudaStream_t s);
+// A server handle over preprocessed (or restored) state.
+Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_t max_batch);
+void fill_params(const Params& pp, ipir_params* o);
 // Pipeline phases: the DB-bound part (query prep, mat-vec, tensor pass,
 // finalize) and the Horner chains.
 constexpr int kPhaseDb = 1, kPhaseHorner = 2, kPhaseAll = 3;

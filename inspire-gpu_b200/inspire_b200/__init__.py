@@ -138,6 +138,10 @@ _L.ipir_serve_db_info.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t),
                                   C.POINTER(IpirSchedule), C.c_size_t]
 _L.ipir_serve_destroy.argtypes = [C.c_void_p]
 _L.ipir_serve_replace_db.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
+_L.ipir_b200_save_server.argtypes = [C.c_void_p, C.c_char_p]
+_L.ipir_b200_save_server.restype = C.c_int
+_L.ipir_b200_load_server.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(IpirParams)]
+_L.ipir_b200_load_server.restype = C.c_void_p
 
 
 class IpirServeBatchRecord(C.Structure):
@@ -159,7 +163,7 @@ EXPORTED = [
     "ipir_b200_launch_count", "ipir_serve_create", "ipir_serve_submit", "ipir_serve_poll", "ipir_serve_wait",
     "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy", "ipir_b200_matvec_ex",
     "ipir_b200_fill_db_device", "ipir_b200_set_schedule", "ipir_b200_wire_sizes", "ipir_b200_answer_wire",
-    "ipir_serve_replace_db",
+    "ipir_serve_replace_db", "ipir_b200_save_server", "ipir_b200_load_server",
 ]
 
 
@@ -236,6 +240,29 @@ class Server:
         self._h = h
         self.params = p.as_dict()
         self.max_batch = max_batch
+
+    @classmethod
+    def load(cls, path, max_batch=16):
+        """A handle restored from a checkpoint written by save() (no raw DB,
+        no preprocessing); raises InspireError for a missing, truncated,
+        foreign or corrupted file."""
+        p = IpirParams()
+        h = _L.ipir_b200_load_server(os.fsencode(path), max_batch, C.byref(p))
+        if not h:
+            raise InspireError(f"ipir_b200_load_server failed: {last_error()}")
+        self = cls.__new__(cls)
+        self._h = h
+        self.params = p.as_dict()
+        self.max_batch = max_batch
+        return self
+
+    def save(self, path):
+        """Write this handle's resident state (encoded DB, precomputed
+        tensors, public parameters) to `path`."""
+        self._check()
+        rc = _L.ipir_b200_save_server(self._h, os.fsencode(path))
+        if rc:
+            raise InspireError(f"ipir_b200_save_server rc={rc}: {last_error()}")
 
     def _check(self):
         if not self._h:
