@@ -23,12 +23,14 @@ cudaError_t launch_matvec(const uint16_t* db, size_t rows, size_t cols, int chun
                           const uint64_t* qraw, size_t qstride, const DevTables* T,
                           uint32_t* part, size_t part_qstride, int nq, cudaStream_t s);
 
-// Tensor-core mat-vec (tcgen05 kind::i8).  qplanes writes the byte planes
-// planes[8q + 4l + k][rows] of nq queries; launch_matvec_tc runs nq <= 32
-// queries whose planes start at `planes`, writing part[q][chunk][limb][cols]
-// with chunks = rows / kchunk_rows.  *err receives a nonzero code if a
-// pipeline wait times out.
+// Tensor-core mat-vec (tcgen05 kind::i8).  qplanes writes the CRT byte
+// planes planes[7q + k][rows] of nq queries (byte k of CRT(b_0, b_1) < q0 q1);
+// launch_matvec_tc runs nq <= 32 queries whose planes start at `planes`
+// (mv_tc_planes_offset of the first query), writing
+// part[q][chunk][limb][cols] with chunks = rows / kchunk_rows.  *err
+// receives a nonzero code if a pipeline wait times out.
 size_t mv_tc_planes_bytes(size_t rows, int max_queries);
+size_t mv_tc_planes_offset(size_t first_query, size_t rows);
 int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms);
 cudaError_t launch_qplanes(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
                            uint8_t* planes, int nq, cudaStream_t s);

@@ -4,14 +4,18 @@
 //
 // The row-major u16 DB is read, unchanged, as a u8 matrix A'[m'][i] with
 // m' = 2j + byte (lo byte at even m', hi byte at odd m'): consecutive m' are
-// contiguous, i.e. an MN-major operand.  Each query word b < 2^27 is split
-// into 4 bytes; B[n][i] with n = 8q + 4l + k holds byte k of b_{q,l}[i]
-// (K-major rows built by qplanes_kernel).  One tcgen05.mma.kind::i8 chain
-// accumulates D[m'][n] = sum_i A'[m'][i] B[n][i] in s32 TMEM.  With K <= 32768
-// rows per chunk every D entry is <= 255*255*32768 < 2^31: exact.  The
-// epilogue forms sum_k 256^k (D[2j][n_k] + 256 D[2j+1][n_k]), which is the
-// exact integer sum_i db[i][j] b[i] (< 2^58), and reduces it mod q_l.  All
-// arithmetic stays exact, so the result equals the reference's.
+// contiguous, i.e. an MN-major operand.  A query's two limbs are combined
+// by CRT into one word B[i] < q0*q1 < 2^53 (B = b_{q,l}[i] mod q_l for both
+// limbs), split into 7 bytes: B[n][i] with n = 7q + k holds byte k of query
+// q's B[i] (K-major rows built by qplanes_kernel).  One
+// tcgen05.mma.kind::i8 chain accumulates D[m'][n] = sum_i A'[m'][i] B[n][i]
+// in s32 TMEM.  With K <= 32768 rows per chunk every D entry is
+// <= 255*255*32768 < 2^31: exact.  The epilogue forms, per limb,
+// sum_k (256^k mod q_l) D[m'][n_k] (< 2^61) in each of the lo and hi byte
+// rows and combines them as (lo + 256 (hi mod q_l)) mod q_l: the exact
+// sum_i db[i][j] b_{q,l}[i] mod q_l.  All arithmetic stays exact, so the
+// result equals the reference's.  Seven planes per query instead of four
+// per limb: 12.5 % fewer MMAs and query-plane bytes.
 //
 // CTA roles (256 threads): warp 0 issues TMA loads (DB tile 256 x 64 rows as
 // two 128-byte boxes, query planes N x 64), warp 1 allocates TMEM and one
@@ -46,12 +50,14 @@ constexpr int kKT = 64;
 constexpr int kMT = 256;          // m' rows per tile (two M = 128 MMAs)
 constexpr int kKChunk = 32768;    // rows per exact s32 accumulation
 constexpr int kRing = 8;          // published work items in flight
+constexpr int kPlanes = 7;        // CRT byte planes per query
 struct TcParams {
     uint32_t* part;        // [q][chunk][limb][cols]
     size_t part_qstride;
     size_t cols;
     int nq;                // queries in this pass (<= 32)
-    int npad;              // N (multiple of 16, <= 256)
+    int npad;              // N = 16 ceil(7 nq / 16) (<= 224)
+    uint32_t c[2][kPlanes];  // 256^k mod q_l
     int n_mtiles;
     int n_kchunks;
     int kchunk_rows;
@@ -193,25 +199,39 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
             const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
             for (int mb = 0; mb < 2; ++mb) {
                 const size_t j = ((size_t)mt * kMT + mb * 128 + wq * 32 + lane) >> 1;
-                for (int q = 0; q < P.nq; ++q) {
-                    uint32_t v[8];
-                    tmem_ld8(tmem_base + lane_base + (uint32_t)(as * 2 * P.npad + mb * P.npad + 8 * q), v);
-                    uint32_t h[8];
+                for (int q0 = 0; q0 < P.nq; q0 += 8) {
+                    // queries q0..q0+7: columns 7 q0 .. 7 q0 + 55, seven 8-column
+                    // loads (those at or past N are not loaded: they hold no query)
+                    uint32_t v[kPlanes * 8];
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) h[e] = __shfl_down_sync(0xffffffffu, v[e], 1);
-                    if ((lane & 1) == 0) {
-                        uint64_t r[2];
+                    for (int c = 0; c < kPlanes; ++c) {
+                        uint32_t t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                        const int col = kPlanes * q0 + 8 * c;
+                        if (col < P.npad)
+                            tmem_ld8(tmem_base + lane_base + (uint32_t)(as * 2 * P.npad + mb * P.npad + col), t);
 #pragma unroll
-                        for (int l = 0; l < 2; ++l) {
-                            uint64_t s = 0;
+                        for (int e = 0; e < 8; ++e) v[8 * c + e] = t[e];
+                    }
+                    // per limb sum_k (256^k mod q) D[row][7 q + k] (< 2^61); lane
+                    // 2j+1 holds the hi DB byte's sums, lane 2j the lo byte's:
+                    // result = (lo + 256 (hi mod q)) mod q
 #pragma unroll
-                            for (int k = 0; k < 4; ++k)
-                                s += ((uint64_t)v[4 * l + k] + ((uint64_t)h[4 * l + k] << 8)) << (8 * k);
-                            r[l] = s;
+                    for (int e = 0; e < 8; ++e) {
+                        uint64_t a0 = 0, a1 = 0;
+#pragma unroll
+                        for (int k = 0; k < kPlanes; ++k) {
+                            a0 += (uint64_t)P.c[0][k] * v[kPlanes * e + k];
+                            a1 += (uint64_t)P.c[1][k] * v[kPlanes * e + k];
                         }
-                        uint32_t* dst = P.part + (size_t)q * P.part_qstride + (size_t)kc * 2 * P.cols + j;
-                        dst[0] = mod_u64(r[0], cr0, kQ0);
-                        dst[P.cols] = mod_u64(r[1], cr1, kQ1);
+                        const uint32_t h0 = (lane & 1) ? mod_u64(a0, cr0, kQ0) : 0u;
+                        const uint32_t h1 = (lane & 1) ? mod_u64(a1, cr1, kQ1) : 0u;
+                        const uint32_t p0 = __shfl_down_sync(0xffffffffu, h0, 1);
+                        const uint32_t p1 = __shfl_down_sync(0xffffffffu, h1, 1);
+                        if ((lane & 1) == 0 && q0 + e < P.nq) {
+                            uint32_t* dst = P.part + (size_t)(q0 + e) * P.part_qstride + (size_t)kc * 2 * P.cols + j;
+                            dst[0] = mod_u64(a0 + ((uint64_t)p0 << 8), cr0, kQ0);
+                            dst[P.cols] = mod_u64(a1 + ((uint64_t)p1 << 8), cr1, kQ1);
+                        }
                     }
                 }
             }
@@ -228,25 +248,32 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
     }
 }
 
-// Byte planes of the query words: planes[8q + 4l + k][i] = byte k of (b_{q,l}[i] mod q_l).
+// CRT byte planes of the queries: planes[7q + k][rows] = byte k of
+// B[i] = CRT(b_0[i] mod q0, b_1[i] mod q1) < q0 q1
+// (Garner: b_1 + q1 ((b_0 - b_1) q1^-1 mod q0)).
 __global__ void __launch_bounds__(256) qplanes_kernel(const uint64_t* __restrict__ qraw, size_t qstride, size_t rows,
-                                                      const DevTables* __restrict__ T, uint8_t* __restrict__ planes) {
+                                                      const DevTables* __restrict__ T,
+                                                      uint8_t* __restrict__ planes) {
     const int q = blockIdx.y;
     const size_t i4 = ((size_t)blockIdx.x * 256 + threadIdx.x) * 4;
     if (i4 >= rows) return;
+    const uint64_t* src = qraw + (size_t)q * qstride;
+    uint64_t B[4];
 #pragma unroll
-    for (int l = 0; l < 2; ++l) {
-        const uint64_t* src = qraw + (size_t)q * qstride + (size_t)l * rows + i4;
-        uint32_t w[4];
+    for (int c = 0; c < 4; ++c) {
+        const uint32_t v0 = mod_u64(src[i4 + c], T->limb[0].cr, kQ0);
+        const uint32_t v1 = mod_u64(src[rows + i4 + c], T->limb[1].cr, kQ1);
+        const uint32_t v1r = v1 >= kQ0 ? v1 - kQ0 : v1;
+        const uint32_t diff = v0 >= v1r ? v0 - v1r : v0 + kQ0 - v1r;
+        const uint32_t h = mod_u64((uint64_t)diff * T->crt_c[0], T->limb[0].cr, kQ0);
+        B[c] = (uint64_t)v1 + (uint64_t)kQ1 * h;
+    }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) w[c] = mod_u64(src[c], T->limb[l].cr, T->limb[l].q);
+    for (int k = 0; k < kPlanes; ++k) {
+        uint32_t packed = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            uint32_t packed = 0;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) packed |= ((w[c] >> (8 * k)) & 0xFFu) << (8 * c);
-            *reinterpret_cast<uint32_t*>(planes + ((size_t)(8 * q + 4 * l + k)) * rows + i4) = packed;
-        }
+        for (int c = 0; c < 4; ++c) packed |= (uint32_t)((B[c] >> (8 * k)) & 0xFFu) << (8 * c);
+        *reinterpret_cast<uint32_t*>(planes + ((size_t)kPlanes * q + k) * rows + i4) = packed;
     }
 }
 
@@ -282,7 +309,8 @@ EncodeTiledFn encode_fn() {
 
 }  // namespace
 
-size_t mv_tc_planes_bytes(size_t rows, int max_queries) { return (size_t)8 * max_queries * rows + 16 * rows; }
+size_t mv_tc_planes_bytes(size_t rows, int max_queries) { return (size_t)kPlanes * max_queries * rows + 16 * rows; }
+size_t mv_tc_planes_offset(size_t first_query, size_t rows) { return (size_t)kPlanes * first_query * rows; }
 
 cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, int chunks, size_t cols,
                                    const DevTables* T, uint32_t* out, size_t out_qstride, int nq, cudaStream_t s) {
@@ -317,7 +345,7 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     if (nq > 32 || rows % kKT || cols % 128 || !tiles) return cudaErrorInvalidValue;
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
-    const int npad = ((8 * nq + 15) / 16) * 16;
+    const int npad = ((kPlanes * nq + 15) / 16) * 16;
     const int kchunk = kchunk_rows;
     if (kchunk <= 0 || kchunk > kKChunk || kchunk % kKT || rows % (size_t)kchunk) return cudaErrorInvalidValue;
     CUtensorMap ma, mb;
@@ -347,6 +375,13 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     P.cols = cols;
     P.nq = nq;
     P.npad = npad;
+    {
+        const uint32_t qs[2] = {kQ0, kQ1};
+        for (int l = 0; l < 2; ++l) {
+            uint64_t c = 1;
+            for (int k = 0; k < kPlanes; ++k, c = c * 256 % qs[l]) P.c[l][k] = (uint32_t)c;
+        }
+    }
     P.n_mtiles = (int)((2 * cols) / kMT);
     P.kchunk_rows = kchunk;
     P.n_kchunks = (int)(rows / kchunk);

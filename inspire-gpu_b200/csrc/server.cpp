@@ -403,7 +403,7 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
         ++launches;
         for (size_t c0 = 0; c0 < count; c0 += 32) {
             const int n = (int)std::min<size_t>(32, count - c0);
-            IPB_CK(launch_matvec_tc(P.db, R, C, L.planes + 8 * c0 * R, n, P.tables, L.mvpart + c0 * S.mv_qstride,
+            IPB_CK(launch_matvec_tc(P.db, R, C, L.planes + mv_tc_planes_offset(c0, R), n, P.tables, L.mvpart + c0 * S.mv_qstride,
                                     S.mv_qstride, L.d_err, L.tiles, beside ? S.num_sms - sc.tp_sms : S.num_sms,
                                     S.tc_kchunk_rows, st));
             ++launches;
@@ -1157,7 +1157,7 @@ int ipir_b200_matvec_ex(const uint16_t* db, size_t rows, size_t cols, const uint
                     IPB_CK(ipb::launch_matvec(db, rows, cols, chunks, queries + q0 * 2 * rows, 2 * rows, M.T, dst,
                                               dst_qstride, n, s));
                 else
-                    IPB_CK(ipb::launch_matvec_tc(db, rows, cols, M.planes + 8 * q0 * rows, n, M.T, dst, dst_qstride,
+                    IPB_CK(ipb::launch_matvec_tc(db, rows, cols, M.planes + ipb::mv_tc_planes_offset(q0, rows), n, M.T, dst, dst_qstride,
                                                  M.err, M.tiles, sms, (int)kchunk, s));
                 if (chunks > 1)
                     IPB_CK(ipb::launch_mv_chunk_reduce(M.part, pq, chunks, cols, M.T, out + q0 * 2 * cols, 2 * cols, n,
