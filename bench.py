@@ -706,7 +706,7 @@ def run_matvec(args):
             ib.matvec_ex(db.data_ptr(), R, Cc, q.data_ptr(), B, out.data_ptr(), path, qpp, kc, sh, True)
             torch.cuda.synchronize()
             passes = -(-B // qpp)
-            ops = 2 * 16 * B * R * Cc           # 8 query planes x 2 DB bytes per (row, col), 2 ops per MAC
+            ops = 2 * 14 * B * R * Cc           # 7 CRT query planes x 2 DB bytes per (row, col), 2 ops per MAC
             d = {"ms": ms, "q_per_s": B * 1e3 / ms, "db_passes": passes,
                  "hbm_gbs": passes * db_bytes / (ms * 1e-3) / 1e9,
                  "hbm_frac": passes * db_bytes / (ms * 1e-3) / 1e9 / hbm_peak,
