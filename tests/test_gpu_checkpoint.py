@@ -62,3 +62,36 @@ def test_corrupted_sections_fail_the_checksum(tmp_path):
         with pytest.raises(ib.InspireError, match=f"checksum mismatch \\({label}\\)"):
             ib.Server.load(f, max_batch=1)
         os.remove(f)
+
+
+def test_checkpoint_as_next_generation(tmp_path):
+    """A database refreshed offline, saved, and restored from its checkpoint
+    replaces the live generation of a serving loop: after the swap every
+    response is the restored handle's, bit-identical to the handle that was
+    saved."""
+    import inspire_b200 as ib
+    c = get_case("medium")
+    live = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=2, crs_seed=c.seed)
+    fresh = ib.Server(c.n_entries, c.w, ib.fill_db(c.R * c.C, 91), db_rows=2048, max_batch=2, crs_seed=c.seed)
+    path = tmp_path / "next.ckpt"
+    qs = [c.query(i, 9200 + k)[0] for k, i in enumerate([3, 200000, 3])]
+    try:
+        fresh.save(path)
+        want_new = [fresh.answer(q) for q in qs]
+        want_old = [live.answer(q) for q in qs]
+    finally:
+        fresh.close()
+    restored = ib.Server.load(path, max_batch=2)
+    loop = ib.ServeLoop([live], max_batch=2, lanes_per_db=2, queue_slots=16, autotune=False)
+    try:
+        r = np.zeros(ib.response_u64s(live.params), np.uint64)
+        loop.wait(loop.submit(0, qs[0]), out=r)
+        assert (r == want_old[0]).all()
+        loop.replace_db(0, restored)
+        for q, w in zip(qs, want_new):
+            loop.wait(loop.submit(0, q), out=r)
+            assert (r == w).all()
+    finally:
+        loop.close()
+        restored.close()
+        live.close()
