@@ -202,15 +202,24 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                 for (int q0 = 0; q0 < P.nq; q0 += 8) {
                     // queries q0..q0+7: columns 7 q0 .. 7 q0 + 55, seven 8-column
                     // loads (those at or past N are not loaded: they hold no query)
+                    uint32_t t[kPlanes][8];
+#pragma unroll
+                    for (int c = 0; c < kPlanes; ++c) {
+                        const int col = kPlanes * q0 + 8 * c;
+                        if (col < P.npad) {
+                            tmem_ld8_issue(tmem_base + lane_base + (uint32_t)(as * 2 * P.npad + mb * P.npad + col),
+                                           t[c]);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) t[c][e] = 0;
+                        }
+                    }
                     uint32_t v[kPlanes * 8];
 #pragma unroll
                     for (int c = 0; c < kPlanes; ++c) {
-                        uint32_t t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                        const int col = kPlanes * q0 + 8 * c;
-                        if (col < P.npad)
-                            tmem_ld8(tmem_base + lane_base + (uint32_t)(as * 2 * P.npad + mb * P.npad + col), t);
+                        tmem_wait8(t[c]);  // one wait for all seven loads; the others are no-ops
 #pragma unroll
-                        for (int e = 0; e < 8; ++e) v[8 * c + e] = t[e];
+                        for (int e = 0; e < 8; ++e) v[8 * c + e] = t[c][e];
                     }
                     // per limb sum_k (256^k mod q) D[row][7 q + k] (< 2^61); lane
                     // 2j+1 holds the hi DB byte's sums, lane 2j the lo byte's:
