@@ -52,9 +52,10 @@ constexpr int kKChunk = 32768;    // rows per exact s32 accumulation
 constexpr int kRing = 8;          // published work items in flight
 constexpr int kPlanes = 7;        // CRT byte planes per query
 struct TcParams {
-    uint32_t* part;        // [q][chunk][limb][cols]
+    uint32_t* part;        // [q][chunk][limb][ld], first column of the range at part
     size_t part_qstride;
-    size_t cols;
+    size_t cols;           // columns in the range
+    size_t ld;             // columns per (chunk, limb) row of part
     int nq;                // queries in this pass (<= 32)
     int npad;              // N = 16 ceil(7 nq / 16) (<= 224)
     uint32_t c[2][kPlanes];  // 256^k mod q_l
@@ -237,9 +238,9 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                         const uint32_t p0 = __shfl_down_sync(0xffffffffu, h0, 1);
                         const uint32_t p1 = __shfl_down_sync(0xffffffffu, h1, 1);
                         if ((lane & 1) == 0 && q0 + e < P.nq) {
-                            uint32_t* dst = P.part + (size_t)(q0 + e) * P.part_qstride + (size_t)kc * 2 * P.cols + j;
+                            uint32_t* dst = P.part + (size_t)(q0 + e) * P.part_qstride + (size_t)kc * 2 * P.ld + j;
                             dst[0] = mod_u64(a0 + ((uint64_t)p0 << 8), cr0, kQ0);
-                            dst[P.cols] = mod_u64(a1 + ((uint64_t)p1 << 8), cr1, kQ1);
+                            dst[P.ld] = mod_u64(a1 + ((uint64_t)p1 << 8), cr1, kQ1);
                         }
                     }
                 }
@@ -350,7 +351,19 @@ int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms) {
 cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const uint8_t* planes, int nq,
                              const DevTables* T, uint32_t* part, size_t part_qstride, int* err, unsigned* tiles,
                              int num_sms, int kchunk_rows, cudaStream_t s) {
+    return launch_matvec_tc_range(db, rows, cols, 0, cols, planes, nq, T, part, part_qstride, err, tiles, num_sms,
+                                  kchunk_rows, s);
+}
+
+cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, size_t c0, size_t c1,
+                                   const uint8_t* planes, int nq, const DevTables* T, uint32_t* part,
+                                   size_t part_qstride, int* err, unsigned* tiles, int num_sms, int kchunk_rows,
+                                   cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
+    if (c1 <= c0 || c1 > ld || c0 % 128) return cudaErrorInvalidValue;
+    const size_t cols = c1 - c0;
+    db += c0;
+    part += c0;
     if (nq > 32 || rows % kKT || cols % 128 || !tiles) return cudaErrorInvalidValue;
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
@@ -360,7 +373,7 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     CUtensorMap ma, mb;
     {
         cuuint64_t dims[2] = {(cuuint64_t)(2 * cols), (cuuint64_t)rows};
-        cuuint64_t strides[1] = {(cuuint64_t)(2 * cols)};
+        cuuint64_t strides[1] = {(cuuint64_t)(2 * ld)};
         cuuint32_t box[2] = {128, (cuuint32_t)kKT};
         cuuint32_t es[2] = {1, 1};
         if (enc(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)db, dims, strides, box, es,
@@ -382,6 +395,7 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
     P.part = part;
     P.part_qstride = part_qstride;
     P.cols = cols;
+    P.ld = ld;
     P.nq = nq;
     P.npad = npad;
     {

@@ -155,11 +155,11 @@ __global__ void __launch_bounds__(256) matvec_kernel(const uint16_t* __restrict_
 // The tensor pass result is tp_out[l][i][q][g] (tensorpass_tc.cu).
 __global__ void __launch_bounds__(256) finalize_kernel(
     const uint32_t* __restrict__ mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
-    const uint32_t* __restrict__ tp_out, int nq_total, int groups,
+    const uint32_t* __restrict__ tp_out, int nq_total, int q_off, int groups, int g0,
     const uint32_t* __restrict__ df, const uint32_t* __restrict__ keys, size_t key_qstride,
     const DevTables* __restrict__ T, uint32_t* __restrict__ packed_b, size_t pb_qstride) {
     __shared__ __align__(16) uint32_t sbuf[2 * kN];
-    const int g = blockIdx.x, l = blockIdx.y, b = blockIdx.z;
+    const int g = g0 + (int)blockIdx.x, l = blockIdx.y, b = blockIdx.z;
     const uint32_t t = threadIdx.x;
     const LimbTables& L = T->limb[l];
     uint32_t r[8];
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(
     uint32_t cs[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e)
-        cs[e] = tp_out[(((size_t)l * kN + 8 * t + e) * nq_total + b) * groups + g];
+        cs[e] = tp_out[(((size_t)l * kN + 8 * t + e) * nq_total + q_off + b) * groups + g];
     uint32_t d0[8], d1[8], k0[8], k1[8];
     ld8(df + ((size_t)g * 2 + l) * kDeff * kN + 8 * t, d0);
     ld8(df + (((size_t)g * 2 + l) * kDeff + 1) * kN + 8 * t, d1);
@@ -729,10 +729,19 @@ cudaError_t launch_finalize(const uint32_t* mvpart, size_t mv_qstride, int mv_ch
                             const uint32_t* tp_out, const uint32_t* df, const uint32_t* keys, size_t key_qstride,
                             const DevTables* T, uint32_t* packed_b, size_t pb_qstride, size_t groups, int nq,
                             cudaStream_t s) {
+    return launch_finalize_range(mvpart, mv_qstride, mv_chunks, cols, tp_out, nq, 0, df, keys, key_qstride, T,
+                                 packed_b, pb_qstride, groups, 0, groups, nq, s);
+}
+
+cudaError_t launch_finalize_range(const uint32_t* mvpart, size_t mv_qstride, int mv_chunks, size_t cols,
+                                  const uint32_t* tp_out, int tp_nq_total, int tp_q0, const uint32_t* df,
+                                  const uint32_t* keys, size_t key_qstride, const DevTables* T, uint32_t* packed_b,
+                                  size_t pb_qstride, size_t groups, size_t g0, size_t gn, int nq, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    finalize_kernel<<<dim3((unsigned)groups, 2, nq), 256, 0, s>>>(mvpart, mv_qstride, mv_chunks, cols, tp_out, nq,
-                                                                  (int)groups, df, keys, key_qstride, T, packed_b,
-                                                                  pb_qstride);
+    if (gn == 0 || g0 + gn > groups || tp_q0 < 0 || tp_q0 + nq > tp_nq_total) return cudaErrorInvalidValue;
+    finalize_kernel<<<dim3((unsigned)gn, 2, nq), 256, 0, s>>>(mvpart, mv_qstride, mv_chunks, cols, tp_out,
+                                                              tp_nq_total, tp_q0, (int)groups, (int)g0, df, keys,
+                                                              key_qstride, T, packed_b, pb_qstride);
     return cudaGetLastError();
 }
 

@@ -33,6 +33,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "inspire_b200.h"
@@ -69,8 +70,51 @@ struct LaneRun {
     Engine* eng = nullptr;
 };
 
+// Cyclic shared scan (ipir_serve_config.scan_segments = ns > 1): a
+// database's DB and tensor passes run as ns segments (groups [k G/ns,
+// (k + 1) G/ns)) in rotation on one lane.  The requests waiting when a
+// segment is enqueued join the rotation there, as one group of contiguous
+// lane query slots; each segment's kernels serve every active query at once
+// (one DB read).  A group's packed ciphertexts are complete after ns
+// segments; its Horner chains and response copies then run on a
+// higher-priority stream while the rotation goes on.  A request waits for
+// the rest of the running segment instead of the rest of a whole DB pass.
+struct ScanGroup {
+    size_t s0 = 0, k = 0;        // lane query slots [s0, s0 + k)
+    int left = 0;                // segments still to run
+    std::vector<uint32_t> req;   // request slots, in lane-slot order
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
+    int* h_err = nullptr;        // pinned copy of the device error word after its Horner chains
+    int64_t t_issue0 = 0, t_issue1 = 0;
+};
+
+struct ScanState {
+    int ns = 0;
+    size_t gseg = 0;             // groups per segment
+    int next_seg = 0;
+    size_t cap = 0;              // lane query slots (<= 32: one pass per segment)
+    std::vector<char> used;
+    std::deque<ScanGroup> active, finishing;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_free;
+    std::vector<int*> err_free;
+    int* pinned_err = nullptr;
+    cudaEvent_t ev_next = nullptr;     // the last segment's mat-vec ran: time to enqueue the next one
+    cudaEvent_t ev_seg_end = nullptr;
+    cudaStream_t hst = nullptr;        // Horner chains and response copies
+    bool stepped = false;
+    uint32_t* keys_pos = nullptr;      // keys of the active queries in pass order (lane arena)
+    std::vector<cudaEvent_t> all_events;
+    ~ScanState() {
+        if (hst) cudaStreamSynchronize(hst);
+        for (auto e : all_events) cudaEventDestroy(e);
+        if (hst) cudaStreamDestroy(hst);
+        if (pinned_err) cudaFreeHost(pinned_err);
+    }
+};
+
 struct DbState {
     Server* S = nullptr;
+    std::unique_ptr<ScanState> scan;  // cyclic scan mode, else lane batches
     size_t max_batch = 0;
     std::vector<Sched> sched;
     std::vector<std::unique_ptr<LaneRun>> lanes;
@@ -110,6 +154,10 @@ struct Engine {
     void finish(DbState& d, LaneRun& r);
     void fail_all_locked(const std::string& why);
     void swap_locked(DbState& d, std::unique_lock<std::mutex>& lk);
+    void scan_step(DbState& d, std::unique_lock<std::mutex>& lk);
+    void scan_poll(DbState& d, bool& any_busy, std::string& poll_err);
+    void scan_finish(DbState& d, ScanGroup& g);
+    void scan_fail_locked(DbState& d);
 };
 
 void Engine::issue(DbState& d, LaneRun& r) {
@@ -181,6 +229,8 @@ void Engine::finish(DbState& d, LaneRun& r) {
 void Engine::fail_all_locked(const std::string& why) {
     failed = true;
     fail_text = why;
+    for (auto& d : dbs)
+        if (d->scan) scan_fail_locked(*d);
     for (auto& d : dbs) {
         for (uint32_t s : d->pending) slots[s].state = kFailed;
         n_failed += d->pending.size();
@@ -189,11 +239,198 @@ void Engine::fail_all_locked(const std::string& why) {
     cv_done.notify_all();
 }
 
+// Enqueue one segment of d's rotation (lock held on entry and exit):
+// admit the waiting requests as a new group, run the segment for every
+// active group, and start the Horner chains of the groups it completes.
+void Engine::scan_step(DbState& d, std::unique_lock<std::mutex>& lk) {
+    ScanState& sc = *d.scan;
+    LaneRun& r = *d.lanes[0];
+    size_t n_active = 0;
+    for (auto& g : sc.active) n_active += g.k;
+    bool admit = false;
+    if (!d.swap_to && !d.pending.empty() && n_active < sc.cap && !sc.ev_free.empty() && !sc.err_free.empty()) {
+        const size_t want = std::min(d.pending.size(), sc.cap - n_active);
+        size_t best_s = 0, best_k = 0;  // longest run of free lane slots (first that fits)
+        for (size_t i = 0; i < sc.cap && best_k < want;) {
+            if (sc.used[i]) {
+                ++i;
+                continue;
+            }
+            size_t j = i;
+            while (j < sc.cap && !sc.used[j]) ++j;
+            if (j - i > best_k) {
+                best_k = j - i;
+                best_s = i;
+            }
+            i = j;
+        }
+        const size_t k = std::min(want, best_k);
+        if (k > 0) {
+            ScanGroup g;
+            g.s0 = best_s;
+            g.k = k;
+            g.left = sc.ns;
+            std::tie(g.ev_start, g.ev_end) = sc.ev_free.back();
+            sc.ev_free.pop_back();
+            g.h_err = sc.err_free.back();
+            sc.err_free.pop_back();
+            *g.h_err = 0;
+            const auto now = Clock::now();
+            for (size_t i = 0; i < k; ++i) {
+                const uint32_t s = d.pending.front();
+                d.pending.pop_front();
+                slots[s].state = kRunning;
+                slots[s].t_issue = now;
+                g.req.push_back(s);
+                sc.used[best_s + i] = 1;
+            }
+            sc.active.push_back(std::move(g));
+            admit = true;
+        }
+    }
+    if (sc.active.empty()) return;
+    std::vector<SlotRun> runs;
+    for (auto& g : sc.active) runs.push_back(SlotRun{g.s0, g.k});
+    const int seg = sc.next_seg;
+    sc.next_seg = (seg + 1) % sc.ns;
+    for (auto& g : sc.active) --g.left;
+    std::vector<ScanGroup> done;  // groups this segment completes (oldest first)
+    while (!sc.active.empty() && sc.active.front().left == 0) {
+        done.push_back(std::move(sc.active.front()));
+        sc.active.pop_front();
+    }
+    ScanGroup* fresh = admit ? &sc.active.back() : nullptr;  // ns > 1: not completed yet
+    sc.stepped = true;
+    const Server& S = *d.S;
+    lk.unlock();
+    std::string err;
+    try {
+        Lane& L = r.lane;
+        IPB_CK(cudaSetDevice(S.device));
+        if (fresh) {
+            fresh->t_issue0 = Clock::now().time_since_epoch().count();
+            IPB_CK(cudaEventRecord(fresh->ev_start, r.st));
+            for (size_t i = 0; i < fresh->k; ++i)
+                IPB_CK(cudaMemcpyAsync(L.qraw + (fresh->s0 + i) * S.qstride, slots[fresh->req[i]].q, S.qstride * 8,
+                                       cudaMemcpyHostToDevice, r.st));
+            enqueue_qprep_slots(S, L, fresh->s0, fresh->k, r.st);
+        }
+        enqueue_scan_segment(S, L, sc.keys_pos, runs, (size_t)seg * sc.gseg, sc.gseg, r.st, sc.ev_next);
+        if (!done.empty()) {
+            IPB_CK(cudaEventRecord(sc.ev_seg_end, r.st));
+            IPB_CK(cudaStreamWaitEvent(sc.hst, sc.ev_seg_end, 0));
+            for (auto& g : done) {
+                enqueue_horner(S, d.sched[g.k], L.packed_b + g.s0 * S.pb_qstride, L.rgsw32 + g.s0 * kRgswStride,
+                               L.resp + g.s0 * S.resp_qstride, g.k, L.d_err, sc.hst);
+                for (size_t i = 0; i < g.k; ++i)
+                    IPB_CK(cudaMemcpyAsync(slots[g.req[i]].resp, L.resp + (g.s0 + i) * S.resp_qstride,
+                                           S.resp_qstride * 8, cudaMemcpyDeviceToHost, sc.hst));
+                IPB_CK(cudaMemcpyAsync(g.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost, sc.hst));
+                IPB_CK(cudaEventRecord(g.ev_end, sc.hst));
+                g.t_issue1 = Clock::now().time_since_epoch().count();
+            }
+        }
+    } catch (const std::exception& e) {
+        err = e.what();
+    }
+    lk.lock();
+    for (auto& g : done) sc.finishing.push_back(std::move(g));
+    if (!err.empty()) {
+        lk.unlock();
+        cudaStreamSynchronize(r.st);
+        cudaStreamSynchronize(sc.hst);
+        lk.lock();
+        fail_all_locked(err);
+    }
+}
+
+// Fails every request of d's rotation and returns its slots and events.
+void Engine::scan_fail_locked(DbState& d) {
+    ScanState& sc = *d.scan;
+    for (auto* q : {&sc.active, &sc.finishing}) {
+        for (auto& g : *q) {
+            for (uint32_t s : g.req) {
+                slots[s].state = kFailed;
+                slots[s].t_done = Clock::now();
+            }
+            n_failed += g.req.size();
+            for (size_t i = 0; i < g.k; ++i) sc.used[g.s0 + i] = 0;
+            sc.ev_free.emplace_back(g.ev_start, g.ev_end);
+            sc.err_free.push_back(g.h_err);
+        }
+        q->clear();
+    }
+    cv_done.notify_all();
+}
+
+// Groups complete in order on the Horner stream (lock held).
+void Engine::scan_poll(DbState& d, bool& any_busy, std::string& poll_err) {
+    ScanState& sc = *d.scan;
+    while (!sc.finishing.empty()) {
+        ScanGroup& g = sc.finishing.front();
+        const cudaError_t q = cudaEventQuery(g.ev_end);
+        if (q == cudaErrorNotReady) {
+            any_busy = true;
+            break;
+        }
+        if (q != cudaSuccess) {
+            poll_err = std::string("CUDA error while waiting for a batch: ") + cudaGetErrorString(q);
+            return;
+        }
+        scan_finish(d, g);
+        sc.finishing.pop_front();
+    }
+    if (!sc.active.empty()) any_busy = true;
+}
+
+void Engine::scan_finish(DbState& d, ScanGroup& g) {
+    ScanState& sc = *d.scan;
+    const int err = *g.h_err;
+    const auto now = Clock::now();
+    float dev_ms = 0.f;
+    if (cudaEventElapsedTime(&dev_ms, g.ev_start, g.ev_end) != cudaSuccess) dev_ms = -1.f;
+    const double notice = std::max(0.0, (now.time_since_epoch().count() - g.t_issue1) * 1e-6);
+    if (!trace.empty()) {
+        ipir_serve_batch_record& t = trace[trace_n++ % trace.size()];
+        t.t_issue_s = g.t_issue0 * 1e-9;
+        t.issue_ms = (float)((g.t_issue1 - g.t_issue0) * 1e-6);
+        t.device_ms = dev_ms;
+        t.notice_ms = (float)notice;
+        t.db = 0;
+        for (size_t i = 0; i < dbs.size(); ++i)
+            if (dbs[i].get() == &d) t.db = (uint16_t)i;
+        t.lane = 0;
+        t.count = (uint32_t)g.k;
+        t.failed = err != 0;
+    }
+    for (uint32_t s : g.req) {
+        slots[s].state = err ? kFailed : kDone;
+        slots[s].t_done = now;
+    }
+    if (err) {
+        n_failed += g.req.size();
+        fail_text = "device pipeline wait timed out (code " + std::to_string(err) + ")";
+    } else {
+        completed += g.req.size();
+    }
+    ++d.batches;
+    d.queries += g.req.size();
+    ++batches;
+    batched += g.req.size();
+    max_seen = std::max<uint64_t>(max_seen, g.req.size());
+    for (size_t i = 0; i < g.k; ++i) sc.used[g.s0 + i] = 0;
+    sc.ev_free.emplace_back(g.ev_start, g.ev_end);
+    sc.err_free.push_back(g.h_err);
+    cv_done.notify_all();
+}
+
 void Engine::run() {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         bool any_busy = false;
         std::string poll_err;
+        for (auto& dp : dbs)
+            if (dp->scan) scan_poll(*dp, any_busy, poll_err);
         for (auto& dp : dbs)
             for (auto& r : dp->lanes)
                 if (r->busy) {
@@ -215,13 +452,35 @@ void Engine::run() {
             if (!dp->swap_to) continue;
             bool idle = true;
             for (auto& r : dp->lanes) idle &= !r->busy;
+            if (dp->scan)
+                idle = dp->scan->active.empty() && dp->scan->finishing.empty() &&
+                       cudaStreamQuery(dp->lanes[0]->st) == cudaSuccess;
             if (idle) swap_locked(*dp, lk);
             else any_busy = true;
         }
+        // Scan rotations keep turning while they hold requests, also after
+        // stop (admitting none then: stop fails the waiting requests below).
+        if (!failed)
+            for (auto& dp : dbs) {
+                DbState& d = *dp;
+                if (!d.scan) continue;
+                ScanState& sc = *d.scan;
+                const bool work = !sc.active.empty() || (!stop && !d.pending.empty() && !d.swap_to);
+                if (work) {
+                    const cudaError_t q = sc.stepped ? cudaEventQuery(sc.ev_next) : cudaSuccess;
+                    if (q == cudaSuccess) {
+                        scan_step(d, lk);
+                    } else if (q != cudaErrorNotReady) {
+                        fail_all_locked(std::string("CUDA error in the scan rotation: ") + cudaGetErrorString(q));
+                    }
+                }
+                if (!sc.active.empty() || !sc.finishing.empty()) any_busy = true;
+            }
         if (stop && !any_busy) break;
         if (!stop && !failed) {
             for (auto& dp : dbs) {
                 DbState& d = *dp;
+                if (d.scan) continue;
                 if (d.pending.empty() || d.swap_to) continue;
                 if (!overlap_db && d.last_lane >= 0 && d.lanes[d.last_lane]->busy) {
                     const cudaError_t q = cudaEventQuery(d.lanes[d.last_lane]->ev_db);
@@ -291,6 +550,7 @@ Engine::~Engine() {
     for (auto& dp : dbs) {
         DbState& d = *dp;
         cudaSetDevice(d.S->device);
+        if (d.scan && d.scan->hst) cudaStreamSynchronize(d.scan->hst);
         for (auto& r : d.lanes) {
             if (r->st) cudaStreamSynchronize(r->st);
             if (r->ev_start) cudaEventDestroy(r->ev_start);
@@ -353,7 +613,7 @@ void Engine::swap_locked(DbState& d, std::unique_lock<std::mutex>& lk) {
     std::string err;
     try {
         IPB_CK(cudaSetDevice(next->device));
-        if (use_graphs)
+        if (use_graphs && !d.scan)
             for (auto& r : d.lanes) capture_graphs(d, *r, false);
     } catch (const std::exception& e) {
         err = e.what();
@@ -421,10 +681,24 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                 const size_t reserve = (size_t)2 << 30;
                 budget = fr > reserve ? fr - reserve : 0;
             }
+            // Cyclic scan for databases whose groups split into scan_segments
+            // parts of whole 128-row tensor-pass tiles (32 groups or more).
+            const size_t ns = cfg.scan_segments > 1 ? (size_t)cfg.scan_segments : 0;
+            auto scan_ok = [&](const ipb::Server& S) {
+                const size_t G = S.pp.n_packed;
+                return ns > 1 && G % ns == 0 && (G / ns) % 32 == 0;
+            };
             size_t mb = cfg.max_batch, lanes = cfg.lanes_per_db;
             auto need = [&](size_t b, size_t l) {
                 size_t t = 0;
-                for (auto& d : E->dbs) t += l * ipb::lane_bytes(*d->S, b, ipb::lane_gt_pass(*d->S, b));
+                for (auto& d : E->dbs) {
+                    if (scan_ok(*d->S)) {
+                        const size_t c = std::min<size_t>(b, 32);
+                        t += ipb::lane_bytes(*d->S, c, ipb::lane_gt_pass(*d->S, c)) + c * ipb::kKeyStride * 4;
+                    } else {
+                        t += l * ipb::lane_bytes(*d->S, b, ipb::lane_gt_pass(*d->S, b));
+                    }
+                }
                 return t;
             };
             while (need(mb, lanes) > budget) {
@@ -435,10 +709,11 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
             size_t q_words = 0, r_words = 0;
             for (auto& dp : E->dbs) {
                 ipb::DbState& d = *dp;
-                d.max_batch = mb;
+                const bool scan = scan_ok(*d.S);
+                d.max_batch = scan ? std::min<size_t>(mb, 32) : mb;
                 q_words = std::max(q_words, d.S->qstride);
                 r_words = std::max(r_words, d.S->resp_qstride);
-                for (size_t k = 0; k < lanes; ++k) {
+                for (size_t k = 0; k < (scan ? 1 : lanes); ++k) {
                     auto r = std::make_unique<ipb::LaneRun>();
                     r->eng = E.get();
                     r->db_index = (uint16_t)(&dp - &E->dbs[0]);
@@ -448,13 +723,38 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                     IPB_CK(cudaEventCreate(&r->ev_start));
                     IPB_CK(cudaEventCreate(&r->ev_end));
                     IPB_CK(cudaEventCreateWithFlags(&r->ev_db, cudaEventDisableTiming));
-                    ipb::alloc_lane(*d.S, r->lane, mb, ipb::lane_gt_pass(*d.S, mb));
+                    ipb::alloc_lane(*d.S, r->lane, d.max_batch, ipb::lane_gt_pass(*d.S, d.max_batch));
                     d.lanes.push_back(std::move(r));
                 }
                 d.sched = !cfg.disable_autotune ? ipb::autotune(*d.S, d.lanes[0]->lane, d.lanes[0]->st)
-                                       : ipb::default_sched(*d.S, mb, d.lanes[0]->lane.gt_pass);
-                if (E->use_graphs)
+                                       : ipb::default_sched(*d.S, d.max_batch, d.lanes[0]->lane.gt_pass);
+                if (scan) {
+                    auto sc = std::make_unique<ipb::ScanState>();
+                    sc->ns = (int)ns;
+                    sc->gseg = d.S->pp.n_packed / ns;
+                    sc->cap = d.max_batch;
+                    sc->used.assign(sc->cap, 0);
+                    sc->keys_pos = d.lanes[0]->lane.arena.alloc<uint32_t>(sc->cap * ipb::kKeyStride);
+                    int lo = 0, hi = 0;
+                    IPB_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+                    IPB_CK(cudaStreamCreateWithPriority(&sc->hst, cudaStreamNonBlocking, hi));
+                    auto mk = [&](unsigned flags) {
+                        cudaEvent_t e = nullptr;
+                        IPB_CK(cudaEventCreateWithFlags(&e, flags));
+                        sc->all_events.push_back(e);
+                        return e;
+                    };
+                    sc->ev_next = mk(cudaEventDisableTiming);
+                    sc->ev_seg_end = mk(cudaEventDisableTiming);
+                    IPB_CK(cudaMallocHost(&sc->pinned_err, sc->cap * sizeof(int)));
+                    for (size_t i = 0; i < sc->cap; ++i) {
+                        sc->ev_free.emplace_back(mk(cudaEventDefault), mk(cudaEventDefault));
+                        sc->err_free.push_back(sc->pinned_err + i);
+                    }
+                    d.scan = std::move(sc);
+                } else if (E->use_graphs) {
                     for (auto& r : d.lanes) ipb::capture_graphs(d, *r);
+                }
             }
             E->q_words = q_words;
             E->r_words = r_words;

@@ -430,22 +430,65 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
 
 static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st,
                             cudaEvent_t* ev) {
+    if (ev) IPB_CK(cudaEventRecord(ev[4], st));
+    enqueue_horner(S, sc, L.packed_b, L.rgsw32, L.resp, count, L.d_err, st);
+    if (ev) IPB_CK(cudaEventRecord(ev[5], st));
+    return 1;
+}
+
+void enqueue_horner(const Server& S, const Sched& sc, const uint32_t* packed_b, const uint32_t* rgsw32,
+                    uint64_t* resp, size_t count, int* err, cudaStream_t st) {
     const Params& pp = S.pp;
     const Precomp& P = *S.pre;
     const size_t G = pp.n_packed, d_act = std::min(pp.D, G);
     const int nq = (int)count;
-    if (ev) IPB_CK(cudaEventRecord(ev[4], st));
     if (sc.horner_cluster == 2)
-        IPB_CK(launch_horner_cluster8(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts,
-                                      L.resp, S.resp_qstride, nq, L.d_err, st));
+        IPB_CK(launch_horner_cluster8(P.pre_a, packed_b, S.pb_qstride, rgsw32, P.tables, G, d_act, pp.num_cts, resp,
+                                      S.resp_qstride, nq, err, st));
     else if (sc.horner_cluster)
-        IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts,
-                                     L.resp, S.resp_qstride, nq, L.d_err, st));
+        IPB_CK(launch_horner_cluster(P.pre_a, packed_b, S.pb_qstride, rgsw32, P.tables, G, d_act, pp.num_cts, resp,
+                                     S.resp_qstride, nq, err, st));
     else
-        IPB_CK(launch_horner(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, pp.num_cts, L.resp,
+        IPB_CK(launch_horner(P.pre_a, packed_b, S.pb_qstride, rgsw32, P.tables, G, d_act, pp.num_cts, resp,
                              S.resp_qstride, nq, st));
-    if (ev) IPB_CK(cudaEventRecord(ev[5], st));
-    return 1;
+}
+
+void enqueue_qprep_slots(const Server& S, Lane& L, size_t s0, size_t count, cudaStream_t st) {
+    IPB_CK(launch_qprep(L.qraw + s0 * S.qstride, S.qstride, S.pp.db_rows, S.pre->tables, L.keys + s0 * kKeyStride,
+                        L.rgsw32 + s0 * kRgswStride, (int)count, st));
+}
+
+void enqueue_scan_segment(const Server& S, Lane& L, uint32_t* keys_pos, const std::vector<SlotRun>& runs, size_t g0,
+                          size_t gn, cudaStream_t st, cudaEvent_t after_matvec) {
+    const Params& pp = S.pp;
+    const Precomp& P = *S.pre;
+    const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
+    size_t n = 0;
+    for (const SlotRun& r : runs) {
+        // positions n .. n + k - 1 of this segment's pass: query planes and keys
+        IPB_CK(launch_qplanes(L.qraw + r.s0 * S.qstride, S.qstride, R, P.tables, L.planes + mv_tc_planes_offset(n, R),
+                              (int)r.k, st));
+        IPB_CK(cudaMemcpyAsync(keys_pos + n * kKeyStride, L.keys + r.s0 * kKeyStride, r.k * kKeyStride * 4,
+                               cudaMemcpyDeviceToDevice, st));
+        n += r.k;
+    }
+    if (n == 0 || n > 32 || n > L.cap) throw std::invalid_argument("scan segment: 1..32 queries per pass");
+    const size_t c0 = g0 * kN, c1 = (g0 + gn) * kN;
+    IPB_CK(launch_matvec_tc_range(P.db, R, C, c0, c1, L.planes, (int)n, P.tables, L.mvpart, S.mv_qstride, L.d_err,
+                                  L.tiles, S.num_sms, S.tc_kchunk_rows, st));
+    if (after_matvec) IPB_CK(cudaEventRecord(after_matvec, st));
+    for (size_t q0 = 0; q0 < n; q0 += (size_t)L.gt_pass) {
+        const int k = (int)std::min<size_t>((size_t)L.gt_pass, n - q0);
+        IPB_CK(launch_tensor_pass_range(P.pre_dt, G, g0, gn, keys_pos + q0 * kKeyStride, kKeyStride, k, (int)n,
+                                        (int)q0, L.keyt, L.tp_out, L.d_err, L.tiles + 1, S.num_sms, st));
+    }
+    size_t p = 0;
+    for (const SlotRun& r : runs) {
+        IPB_CK(launch_finalize_range(L.mvpart + p * S.mv_qstride, S.mv_qstride, S.tc_kchunks, C, L.tp_out, (int)n,
+                                     (int)p, P.pre_df, keys_pos + p * kKeyStride, kKeyStride, P.tables,
+                                     L.packed_b + r.s0 * S.pb_qstride, S.pb_qstride, G, g0, gn, (int)r.k, st));
+        p += r.k;
+    }
 }
 
 int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,

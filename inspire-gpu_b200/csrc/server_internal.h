@@ -175,6 +175,26 @@ const Sched& sched_for(const Server& S, size_t c);
 // Queries per tensor-pass GEMM a lane of `cap` queries provisions Gt for.
 int lane_gt_pass(const Server& S, size_t cap);
 
+// Horner chains (variant sc.horner_cluster) of `count` queries whose
+// packed ciphertexts, RGSW parts and responses start at the given pointers
+// (per-query strides of S).
+void enqueue_horner(const Server& S, const Sched& sc, const uint32_t* packed_b, const uint32_t* rgsw32,
+                    uint64_t* resp, size_t count, int* err, cudaStream_t st);
+// Query prep (keys, RGSW parts) of the flat queries in lane slots [s0, s0 + count).
+void enqueue_qprep_slots(const Server& S, Lane& L, size_t s0, size_t count, cudaStream_t st);
+// Lane query slots [s0, s0 + k).
+struct SlotRun {
+    size_t s0, k;
+};
+// One segment of the cyclic scan: for the queries in `runs` (their positions
+// in this pass follow the order of runs), the tensor-core mat-vec over the
+// columns of groups [g0, g0 + gn), the tensor pass over those groups and the
+// finalize that writes their packed ciphertexts into the queries' own slots.
+// keys_pos: scratch for the queries' keys in pass order (<= 32 queries).
+// after_matvec (may be null) is recorded once the mat-vec is enqueued.
+void enqueue_scan_segment(const Server& S, Lane& L, uint32_t* keys_pos, const std::vector<SlotRun>& runs, size_t g0,
+                          size_t gn, cudaStream_t st, cudaEvent_t after_matvec);
+
 }  // namespace ipb
 
 // The C ABI handle (opaque in the public header).

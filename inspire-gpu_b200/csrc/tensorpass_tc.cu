@@ -177,8 +177,10 @@ struct TpParams {
     int nb;                // N = key rows per item, roundup16(spi * rq)
     int w8;                // 8-query groups per key-table position
     const uint32_t* keyt;  // Kt[l][j][p][8 * w8], 32-byte aligned rows
-    int G;                 // groups
-    int mti;               // M tiles (128 rows) per item (4G >= 128)
+    int G;                 // groups (Dt rows per slot: 4G)
+    int g0;                // first group of the range this launch covers
+    int gn;                // groups in the range
+    int mti;               // M tiles (128 rows) per item (4 gn >= 128)
     int n_mg;              // M-tile groups per (l, i)
     int spi;               // slots per item (4G < 128: several slots share one 128-row A tile)
     int rows_box;          // rows per A box
@@ -281,9 +283,10 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
             for (int bi = 0; bi < nblk; ++bi) {
                 const int mt = blk0 + bi;
                 const int li = li0 + (P.spi > 1 ? mt : 0);
-                const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;  // g*4 + a
-                const int g = grow >> 2, a = grow & 3;
-                const bool valid = grow >= 0 && grow < slot_rows;
+                // (g - g0) * 4 + a
+                const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;
+                const int g = P.g0 + (grow >> 2), a = grow & 3;
+                const bool valid = grow >= 0 && grow < 4 * P.gn;
                 // four queries (16 columns) per TMEM load where the block has
                 // them; the block's last columns one query at a time
                 const int lim = P.spi > 1 ? P.nb : (mt + 1) * P.nb;
@@ -330,7 +333,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                 mbar_arrive(&ifull[r]);
                 if (item < 0) break;
                 const int li = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
-                const int rowa = li * slot_rows + mg * P.mti * 128;
+                const int rowa = li * slot_rows + 4 * P.g0 + mg * P.mti * 128;
                 for (int kt = 0; kt < ktiles; ++kt) {
                     if (!mbar_wait(&empty[s], ph ^ 1, P.err, 11)) { abort_flag = 1; break; }
                     uint8_t* st = smem + (size_t)s * stage_bytes;
@@ -544,8 +547,17 @@ cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp
 cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
                                int nq_total, int q0, uint32_t* keyt, uint32_t* tp_out, int* err, unsigned* tiles,
                                int num_sms, cudaStream_t s) {
+    return launch_tensor_pass_range(Dt, G, 0, G, keys, key_qstride, nq, nq_total, q0, keyt, tp_out, err, tiles,
+                                    num_sms, s);
+}
+
+cudaError_t launch_tensor_pass_range(const uint8_t* Dt, size_t G, size_t g0, size_t gn, const uint32_t* keys,
+                                     size_t key_qstride, int nq, int nq_total, int q0, uint32_t* keyt,
+                                     uint32_t* tp_out, int* err, unsigned* tiles, int num_sms, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
     if (nq > 32 || !tiles) return cudaErrorInvalidValue;
+    // A part of the groups: whole 128-row M tiles of it (gn a multiple of 32)
+    if (gn == 0 || g0 + gn > G || (gn < G && gn % 32)) return cudaErrorInvalidValue;
     const int rq = 4 * nq;
     const int W = 8 * ((nq + 7) / 8);
     const size_t kt_n = (size_t)2 * kDeff * kN * W;
@@ -561,7 +573,9 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     P.w8 = W / 8;
     P.keyt = keyt;
     P.G = (int)G;
-    const int nmt = (int)std::max<size_t>(1, (4 * G + 127) / 128);
+    P.g0 = (int)g0;
+    P.gn = (int)gn;
+    const int nmt = (int)std::max<size_t>(1, (4 * gn + 127) / 128);
     P.mti = std::min(nmt, 4);
     P.n_mg = nmt / P.mti;
     // Small G: pack spi slots (each 4G rows) into one 128-row A tile.  G even
@@ -569,12 +583,12 @@ cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys
     // of two divides kN, so a packed item never straddles the two limbs.
     auto nb_of = [&](int sp) { return ((sp * rq + 15) / 16) * 16; };
     P.spi = 1;
-    if (4 * G < 128 && G % 2 == 0) {
+    if (4 * G < 128 && G % 2 == 0 && gn == G) {
         while (2 * P.spi * 4 * (int)G <= 128) P.spi *= 2;
         while (P.spi > 1 && (nb_of(P.spi) > 256 || 2 * nb_of(P.spi) > 512)) P.spi /= 2;
     }
     P.nb = nb_of(P.spi);
-    P.rows_box = (int)std::min<size_t>(128, 4 * G * (size_t)P.spi);
+    P.rows_box = (int)std::min<size_t>(128, 4 * gn * (size_t)P.spi);
     if (P.mti * P.nb > 512) return cudaErrorInvalidValue;
     P.acc_stages = (2 * P.mti * P.nb <= 512) ? 2 : 1;
     uint32_t need = (uint32_t)(P.acc_stages * P.mti * P.nb), tc = 32;

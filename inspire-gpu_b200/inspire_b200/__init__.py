@@ -103,7 +103,7 @@ class IpirSchedule(C.Structure):
 class IpirServeConfig(C.Structure):
     _fields_ = [("max_batch", C.c_size_t), ("lanes_per_db", C.c_size_t), ("queue_slots", C.c_size_t),
                 ("hbm_budget_bytes", C.c_size_t), ("disable_graphs", C.c_int), ("disable_autotune", C.c_int),
-                ("overlap_db_passes", C.c_int)]
+                ("overlap_db_passes", C.c_int), ("scan_segments", C.c_int)]
 
 
 class IpirServeCounters(C.Structure):
@@ -451,14 +451,17 @@ SERVE_DONE, SERVE_PENDING, SERVE_UNKNOWN, SERVE_FAILED, SERVE_TIMEOUT, SERVE_FUL
 class ServeLoop:
     """Continuous-batching serving loop over resident databases (the
     ipir_serve_* entry points): submit() returns a ticket at once; poll() /
-    wait() collect the response and its submit-to-response latency."""
+    wait() collect the response and its submit-to-response latency.
+    scan_segments > 1: cyclic scan (requests join the running rotation of
+    DB-pass segments) for the databases whose groups split that way."""
 
     def __init__(self, servers, max_batch=0, lanes_per_db=0, queue_slots=0, hbm_budget_bytes=0,
-                 graphs=True, autotune=True, overlap_db_passes=False):
+                 graphs=True, autotune=True, overlap_db_passes=False, scan_segments=0):
         self.servers = list(servers)
         hs = (C.c_void_p * len(self.servers))(*[s._h for s in self.servers])
         cfg = IpirServeConfig(max_batch, lanes_per_db, queue_slots, hbm_budget_bytes,
-                              0 if graphs else 1, 0 if autotune else 1, 1 if overlap_db_passes else 0)
+                              0 if graphs else 1, 0 if autotune else 1, 1 if overlap_db_passes else 0,
+                              scan_segments)
         h = _L.ipir_serve_create(hs, len(self.servers), C.byref(cfg))
         if not h:
             raise InspireError(f"ipir_serve_create failed: {last_error()}")

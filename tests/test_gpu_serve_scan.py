@@ -1,0 +1,87 @@
+"""Serving loop in cyclic-scan mode (ipir_serve_config.scan_segments): the
+DB and tensor passes run as segments of 32 or 64 groups in rotation, and
+requests join at the next segment.  Every response must be bit-identical to
+the plain single answer of the same query (tolerance 0) whichever segment
+it joined at and whatever shared its segments; responses decrypt through
+the reference client's extract() to the queried entry.  A segment count
+that does not split the groups into multiples of 32 leaves the database on
+lane batches."""
+import random
+import time
+
+import numpy as np
+import pytest
+
+from cases import get_case
+
+pytestmark = pytest.mark.gpu
+
+N_REQ = 20
+
+
+@pytest.fixture(scope="module")
+def env():
+    import inspire_b200 as ib
+    c = get_case("g128")
+    assert c.G == 128
+    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=8, crs_seed=c.seed)
+    rng = np.random.default_rng(31)
+    idxs = [int(x) for x in rng.integers(0, c.n_entries, N_REQ)]
+    idxs[3] = idxs[4]   # the same entry twice, fresh keys
+    qs, sts = [], []
+    for k, idx in enumerate(idxs):
+        q, st = c.query(idx, 9100 + k)
+        qs.append(q)
+        sts.append(st)
+    singles = [srv.answer(q) for q in qs]
+    yield ib, c, srv, idxs, qs, sts, singles
+    srv.close()
+
+
+def _serve(ib, srv, qs, rng, gaps, **cfg):
+    loop = ib.ServeLoop([srv], **cfg)
+    try:
+        tickets = []
+        for q in qs:
+            tickets.append(loop.submit(0, q))
+            if gaps and rng.random() < 0.5:   # later requests join at later segments
+                time.sleep(rng.uniform(0.0, 0.003))
+        out = []
+        for t in tickets:
+            r = np.zeros(ib.response_u64s(srv.params), np.uint64)
+            assert loop.wait(t, out=r, timeout=60.0) >= 0.0
+            out.append(r)
+        stats = loop.stats()
+        info = loop.db_info(0)
+        trace = loop.trace()
+    finally:
+        loop.close()
+    return out, stats, info, trace
+
+
+@pytest.mark.parametrize("segments,gaps", [(4, True), (2, True), (4, False)])
+def test_scan_equals_singles(env, segments, gaps):
+    ib, c, srv, idxs, qs, sts, singles = env
+    out, stats, info, trace = _serve(ib, srv, qs, random.Random(segments), gaps, max_batch=8, queue_slots=64,
+                                     autotune=False, scan_segments=segments)
+    for i in range(N_REQ):
+        assert (out[i] == singles[i]).all(), (segments, i)
+    assert stats["completed"] == N_REQ and stats["failed"] == 0 and stats["queued"] == 0
+    assert stats["batched_queries"] == N_REQ and stats["free_slots"] == 64
+    assert 1 <= stats["max_batch_seen"] <= 8      # a group holds at most the lane's 8 slots
+    assert info["lanes"] == 1 and info["max_batch"] == 8
+    assert sum(t["count"] for t in trace) == N_REQ and not any(t["failed"] for t in trace)
+    if not gaps:
+        assert stats["batches"] >= 3               # 20 requests at once: groups of <= 8 slots
+    for i in (0, 3, 4, N_REQ - 1):
+        assert (sts[i].extract(out[i]) == c.expected_slots(idxs[i])).all(), i
+    assert not (out[3] == out[4]).all()
+
+
+def test_segments_that_do_not_split_fall_back_to_lanes(env):
+    ib, c, srv, idxs, qs, sts, singles = env
+    out, stats, info, _ = _serve(ib, srv, qs[:6], random.Random(5), True, max_batch=4, lanes_per_db=2,
+                                 queue_slots=16, autotune=False, scan_segments=3)
+    assert info["lanes"] == 2
+    for i in range(6):
+        assert (out[i] == singles[i]).all(), i
