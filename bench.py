@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--serve-max-batch", type=int, default=64)
     ap.add_argument("--serve-overlap", action="store_true",
                     help="admit batches while the previous DB pass of their database still runs")
+    ap.add_argument("--serve-scan", type=int, default=0,
+                    help="cyclic scan: DB passes as this many group segments in rotation, requests join at "
+                         "the next segment (databases whose groups split into multiples of 32)")
     return ap.parse_args()
 
 
@@ -508,7 +511,7 @@ def run_serve(args):
         rates = [float(x) for x in args.serve_rates.split(",")]
     t0 = time.perf_counter()
     loop = ib.ServeLoop(servers, max_batch=args.serve_max_batch, lanes_per_db=args.serve_lanes, queue_slots=512,
-                        overlap_db_passes=args.serve_overlap)
+                        overlap_db_passes=args.serve_overlap, scan_segments=args.serve_scan)
     t_create = time.perf_counter() - t0
     views = [[ib.query_view_from_flat(servers[k].params, pools[k][i]) for i in range(pool_n)]
              for k in range(len(dbs))]
@@ -614,7 +617,8 @@ def run_serve(args):
             "mode": "serve", "config": {"workload": args.serve_config, "databases": [p["workload"] for p in plain],
                                         "split": split, "seconds_per_rate": args.serve_seconds,
                                         "max_batch": args.serve_max_batch, "lanes_per_db": args.serve_lanes,
-                                        "overlap_db_passes": args.serve_overlap},
+                                        "overlap_db_passes": args.serve_overlap,
+                                        "scan_segments": args.serve_scan},
             "n_gpus": 1, "unit": "ms", "data": "synthetic queries (pool of 32 per database)",
             "plain": plain, "rates": results, "create_s": t_create,
             "lanes": [{"lanes": i["lanes"], "max_batch": i["max_batch"]} for i in infos],

@@ -297,9 +297,9 @@ typedef struct {
     int overlap_db_passes;   /* 1: admit a batch on any free lane at once, even while the previous
                                 batch of its database still streams the DB (default 0: wait for
                                 that pass to end, overlapping only its Horner chains) */
-    int scan_segments;       /* > 1: cyclic scan for each database whose n_packed groups split into
-                                this many parts of a multiple of 32 groups: its DB and tensor passes
-                                run as that many segments in rotation on one lane of up to 32
+    int scan_segments;       /* > 1 (a power of two <= 128): cyclic scan for each database whose
+                                columns split into this many multiples of 128: its DB and tensor
+                                passes run as that many segments in rotation on one lane of up to 32
                                 queries, and waiting requests join at the next segment instead of
                                 the next whole pass (default 0: lane batches) */
 } ipir_serve_config;

@@ -40,12 +40,13 @@ cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const
                              const DevTables* T, uint32_t* part, size_t part_qstride, int* err, unsigned* tiles,
                              int num_sms, int kchunk_rows, cudaStream_t s);
 // The same over the DB columns [c0, c1) of a DB with ld columns per row
-// (c0 a multiple of 128): writes part[q][chunk][limb][c] for c in [c0, c1)
-// of the full-width layout (ld columns per chunk and limb).
+// (c0 a multiple of 128): writes part[q'][chunk][limb][c] for c in [c0, c1)
+// of the full-width layout (ld columns per chunk and limb); q' = qmap[q]
+// for pass query q when qmap (nq entries) is given, else q.
 cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, size_t c0, size_t c1,
                                    const uint8_t* planes, int nq, const DevTables* T, uint32_t* part,
-                                   size_t part_qstride, int* err, unsigned* tiles, int num_sms, int kchunk_rows,
-                                   cudaStream_t s);
+                                   size_t part_qstride, const uint8_t* qmap, int* err, unsigned* tiles, int num_sms,
+                                   int kchunk_rows, cudaStream_t s);
 
 // out[q][limb][cols] = sum over chunks of part[q][chunk][limb][cols] mod q.
 cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, int chunks, size_t cols,
@@ -64,11 +65,14 @@ cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp
 cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
                                int nq_total, int q0, uint32_t* keyt, uint32_t* tp_out, int* err, unsigned* tiles,
                                int num_sms, cudaStream_t s);
-// The same for the groups [g0, g0 + gn) only (gn = G, or a multiple of 32):
-// writes tp_out[l][i][q][g] for g in that range.
-cudaError_t launch_tensor_pass_range(const uint8_t* Dt, size_t G, size_t g0, size_t gn, const uint32_t* keys,
-                                     size_t key_qstride, int nq, int nq_total, int q0, uint32_t* keyt,
-                                     uint32_t* tp_out, int* err, unsigned* tiles, int num_sms, cudaStream_t s);
+// The same for the (limb, slot) indices l * N + i in [li0, li0 + n_li) only
+// (multiples of 32), all groups: writes tp_out[l][i][q'][g] for those
+// indices, q' = qmap[q0 + p] for pass query p when qmap (the output rows of
+// queries 0 .. q0 + nq - 1 of the pass, < nq_total) is given, else q0 + p.
+cudaError_t launch_tensor_pass_slots(const uint8_t* Dt, size_t G, int li0, int n_li, const uint32_t* keys,
+                                     size_t key_qstride, int nq, int nq_total, int q0, const uint8_t* qmap,
+                                     uint32_t* keyt, uint32_t* tp_out, int* err, unsigned* tiles, int num_sms,
+                                     cudaStream_t s);
 
 // packed_b[q][g][limb][N] = NTT(sum_y mvpart) - tp_out - Dfinal (.) Kn1.
 cudaError_t launch_finalize(const uint32_t* mvpart, size_t mv_qstride, int mv_chunks, size_t cols,

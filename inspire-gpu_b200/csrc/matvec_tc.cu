@@ -68,6 +68,8 @@ struct TcParams {
     int* err;
     unsigned* tiles;       // work-item counter, zero at launch
     const DevTables* T;
+    int has_qmap;          // output row of pass query q: qmap[q] (else q)
+    uint8_t qmap[32];
 };
 
 __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ CUtensorMap map_a,
@@ -238,7 +240,8 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                         const uint32_t p0 = __shfl_down_sync(0xffffffffu, h0, 1);
                         const uint32_t p1 = __shfl_down_sync(0xffffffffu, h1, 1);
                         if ((lane & 1) == 0 && q0 + e < P.nq) {
-                            uint32_t* dst = P.part + (size_t)(q0 + e) * P.part_qstride + (size_t)kc * 2 * P.ld + j;
+                            const int qo = P.has_qmap ? P.qmap[q0 + e] : q0 + e;
+                            uint32_t* dst = P.part + (size_t)qo * P.part_qstride + (size_t)kc * 2 * P.ld + j;
                             dst[0] = mod_u64(a0 + ((uint64_t)p0 << 8), cr0, kQ0);
                             dst[P.ld] = mod_u64(a1 + ((uint64_t)p1 << 8), cr1, kQ1);
                         }
@@ -351,14 +354,14 @@ int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms) {
 cudaError_t launch_matvec_tc(const uint16_t* db, size_t rows, size_t cols, const uint8_t* planes, int nq,
                              const DevTables* T, uint32_t* part, size_t part_qstride, int* err, unsigned* tiles,
                              int num_sms, int kchunk_rows, cudaStream_t s) {
-    return launch_matvec_tc_range(db, rows, cols, 0, cols, planes, nq, T, part, part_qstride, err, tiles, num_sms,
-                                  kchunk_rows, s);
+    return launch_matvec_tc_range(db, rows, cols, 0, cols, planes, nq, T, part, part_qstride, nullptr, err, tiles,
+                                  num_sms, kchunk_rows, s);
 }
 
 cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, size_t c0, size_t c1,
                                    const uint8_t* planes, int nq, const DevTables* T, uint32_t* part,
-                                   size_t part_qstride, int* err, unsigned* tiles, int num_sms, int kchunk_rows,
-                                   cudaStream_t s) {
+                                   size_t part_qstride, const uint8_t* qmap, int* err, unsigned* tiles, int num_sms,
+                                   int kchunk_rows, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
     if (c1 <= c0 || c1 > ld || c0 % 128) return cudaErrorInvalidValue;
     const size_t cols = c1 - c0;
@@ -396,6 +399,9 @@ cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, s
     P.part_qstride = part_qstride;
     P.cols = cols;
     P.ld = ld;
+    P.has_qmap = qmap != nullptr;
+    if (qmap)
+        for (int q = 0; q < nq; ++q) P.qmap[q] = qmap[q];
     P.nq = nq;
     P.npad = npad;
     {

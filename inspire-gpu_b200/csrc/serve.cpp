@@ -71,14 +71,16 @@ struct LaneRun {
 };
 
 // Cyclic shared scan (ipir_serve_config.scan_segments = ns > 1): a
-// database's DB and tensor passes run as ns segments (groups [k G/ns,
-// (k + 1) G/ns)) in rotation on one lane.  The requests waiting when a
-// segment is enqueued join the rotation there, as one group of contiguous
-// lane query slots; each segment's kernels serve every active query at once
-// (one DB read).  A group's packed ciphertexts are complete after ns
-// segments; its Horner chains and response copies then run on a
-// higher-priority stream while the rotation goes on.  A request waits for
-// the rest of the running segment instead of the rest of a whole DB pass.
+// database's DB and tensor passes run as ns segments in rotation on one lane
+// (segment k: DB columns [k C/ns, (k + 1) C/ns) and the tensor pass's
+// (limb, slot) indices [k 2N/ns, (k + 1) 2N/ns), all groups).  The requests
+// waiting when a segment is enqueued join the rotation there, as one group
+// of contiguous lane query slots; each segment's kernels serve every active
+// query at once (one read of that part of the DB and tensors), writing
+// per-slot partial results.  After a group's ns-th segment its finalize
+// runs, then its Horner chains and response copies on a higher-priority
+// stream while the rotation goes on.  A request waits for the rest of the
+// running segment instead of the rest of a whole DB pass.
 struct ScanGroup {
     size_t s0 = 0, k = 0;        // lane query slots [s0, s0 + k)
     int left = 0;                // segments still to run
@@ -90,7 +92,6 @@ struct ScanGroup {
 
 struct ScanState {
     int ns = 0;
-    size_t gseg = 0;             // groups per segment
     int next_seg = 0;
     size_t cap = 0;              // lane query slots (<= 32: one pass per segment)
     std::vector<char> used;
@@ -315,8 +316,9 @@ void Engine::scan_step(DbState& d, std::unique_lock<std::mutex>& lk) {
                                        cudaMemcpyHostToDevice, r.st));
             enqueue_qprep_slots(S, L, fresh->s0, fresh->k, r.st);
         }
-        enqueue_scan_segment(S, L, sc.keys_pos, runs, (size_t)seg * sc.gseg, sc.gseg, r.st, sc.ev_next);
+        enqueue_scan_segment(S, L, sc.keys_pos, runs, seg, sc.ns, r.st, sc.ev_next);
         if (!done.empty()) {
+            for (auto& g : done) enqueue_scan_finalize(S, L, SlotRun{g.s0, g.k}, r.st);
             IPB_CK(cudaEventRecord(sc.ev_seg_end, r.st));
             IPB_CK(cudaStreamWaitEvent(sc.hst, sc.ev_seg_end, 0));
             for (auto& g : done) {
@@ -681,12 +683,12 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                 const size_t reserve = (size_t)2 << 30;
                 budget = fr > reserve ? fr - reserve : 0;
             }
-            // Cyclic scan for databases whose groups split into scan_segments
-            // parts of whole 128-row tensor-pass tiles (32 groups or more).
+            // Cyclic scan for databases whose columns split into scan_segments
+            // parts of whole 128-column tiles (the tensor pass splits its
+            // 2N (limb, slot) indices the same way, in multiples of 32).
             const size_t ns = cfg.scan_segments > 1 ? (size_t)cfg.scan_segments : 0;
             auto scan_ok = [&](const ipb::Server& S) {
-                const size_t G = S.pp.n_packed;
-                return ns > 1 && G % ns == 0 && (G / ns) % 32 == 0;
+                return ns > 1 && S.pp.db_cols % (128 * ns) == 0 && (2 * ipb::kN) % (32 * ns) == 0;
             };
             size_t mb = cfg.max_batch, lanes = cfg.lanes_per_db;
             auto need = [&](size_t b, size_t l) {
@@ -731,7 +733,6 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                 if (scan) {
                     auto sc = std::make_unique<ipb::ScanState>();
                     sc->ns = (int)ns;
-                    sc->gseg = d.S->pp.n_packed / ns;
                     sc->cap = d.max_batch;
                     sc->used.assign(sc->cap, 0);
                     sc->keys_pos = d.lanes[0]->lane.arena.alloc<uint32_t>(sc->cap * ipb::kKeyStride);

@@ -458,37 +458,45 @@ void enqueue_qprep_slots(const Server& S, Lane& L, size_t s0, size_t count, cuda
                         L.rgsw32 + s0 * kRgswStride, (int)count, st));
 }
 
-void enqueue_scan_segment(const Server& S, Lane& L, uint32_t* keys_pos, const std::vector<SlotRun>& runs, size_t g0,
-                          size_t gn, cudaStream_t st, cudaEvent_t after_matvec) {
+void enqueue_scan_segment(const Server& S, Lane& L, uint32_t* keys_pos, const std::vector<SlotRun>& runs, int seg,
+                          int ns, cudaStream_t st, cudaEvent_t after_matvec) {
     const Params& pp = S.pp;
     const Precomp& P = *S.pre;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
+    uint8_t qmap[32];
     size_t n = 0;
     for (const SlotRun& r : runs) {
+        if (n + r.k > 32 || r.s0 + r.k > L.cap) throw std::invalid_argument("scan segment: 1..32 queries per pass");
         // positions n .. n + k - 1 of this segment's pass: query planes and keys
         IPB_CK(launch_qplanes(L.qraw + r.s0 * S.qstride, S.qstride, R, P.tables, L.planes + mv_tc_planes_offset(n, R),
                               (int)r.k, st));
         IPB_CK(cudaMemcpyAsync(keys_pos + n * kKeyStride, L.keys + r.s0 * kKeyStride, r.k * kKeyStride * 4,
                                cudaMemcpyDeviceToDevice, st));
+        for (size_t i = 0; i < r.k; ++i) qmap[n + i] = (uint8_t)(r.s0 + i);
         n += r.k;
     }
-    if (n == 0 || n > 32 || n > L.cap) throw std::invalid_argument("scan segment: 1..32 queries per pass");
-    const size_t c0 = g0 * kN, c1 = (g0 + gn) * kN;
-    IPB_CK(launch_matvec_tc_range(P.db, R, C, c0, c1, L.planes, (int)n, P.tables, L.mvpart, S.mv_qstride, L.d_err,
-                                  L.tiles, S.num_sms, S.tc_kchunk_rows, st));
+    if (n == 0) throw std::invalid_argument("scan segment: no queries");
+    if (ns < 1 || C % (128 * (size_t)ns) || (2 * kN) % (32 * ns)) throw std::invalid_argument("scan segment: bad split");
+    const size_t c0 = C / ns * seg, c1 = c0 + C / ns;
+    IPB_CK(launch_matvec_tc_range(P.db, R, C, c0, c1, L.planes, (int)n, P.tables, L.mvpart, S.mv_qstride, qmap,
+                                  L.d_err, L.tiles, S.num_sms, S.tc_kchunk_rows, st));
     if (after_matvec) IPB_CK(cudaEventRecord(after_matvec, st));
+    const int n_li = (int)(2 * kN) / ns, li0 = n_li * seg;
     for (size_t q0 = 0; q0 < n; q0 += (size_t)L.gt_pass) {
         const int k = (int)std::min<size_t>((size_t)L.gt_pass, n - q0);
-        IPB_CK(launch_tensor_pass_range(P.pre_dt, G, g0, gn, keys_pos + q0 * kKeyStride, kKeyStride, k, (int)n,
-                                        (int)q0, L.keyt, L.tp_out, L.d_err, L.tiles + 1, S.num_sms, st));
+        IPB_CK(launch_tensor_pass_slots(P.pre_dt, G, li0, n_li, keys_pos + q0 * kKeyStride, kKeyStride, k,
+                                        (int)L.cap, (int)q0, qmap, L.keyt, L.tp_out, L.d_err, L.tiles + 1, S.num_sms,
+                                        st));
     }
-    size_t p = 0;
-    for (const SlotRun& r : runs) {
-        IPB_CK(launch_finalize_range(L.mvpart + p * S.mv_qstride, S.mv_qstride, S.tc_kchunks, C, L.tp_out, (int)n,
-                                     (int)p, P.pre_df, keys_pos + p * kKeyStride, kKeyStride, P.tables,
-                                     L.packed_b + r.s0 * S.pb_qstride, S.pb_qstride, G, g0, gn, (int)r.k, st));
-        p += r.k;
-    }
+}
+
+void enqueue_scan_finalize(const Server& S, Lane& L, const SlotRun& r, cudaStream_t st) {
+    const Params& pp = S.pp;
+    const Precomp& P = *S.pre;
+    const size_t C = pp.db_cols, G = pp.n_packed;
+    IPB_CK(launch_finalize_range(L.mvpart + r.s0 * S.mv_qstride, S.mv_qstride, S.tc_kchunks, C, L.tp_out, (int)L.cap,
+                                 (int)r.s0, P.pre_df, L.keys + r.s0 * kKeyStride, kKeyStride, P.tables,
+                                 L.packed_b + r.s0 * S.pb_qstride, S.pb_qstride, G, 0, G, (int)r.k, st));
 }
 
 int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,

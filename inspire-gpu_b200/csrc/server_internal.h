@@ -186,14 +186,18 @@ void enqueue_qprep_slots(const Server& S, Lane& L, size_t s0, size_t count, cuda
 struct SlotRun {
     size_t s0, k;
 };
-// One segment of the cyclic scan: for the queries in `runs` (their positions
-// in this pass follow the order of runs), the tensor-core mat-vec over the
-// columns of groups [g0, g0 + gn), the tensor pass over those groups and the
-// finalize that writes their packed ciphertexts into the queries' own slots.
-// keys_pos: scratch for the queries' keys in pass order (<= 32 queries).
+// One segment (seg of ns) of the cyclic scan for the queries in `runs`
+// (their positions in this pass follow the order of runs): the tensor-core
+// mat-vec over DB columns [seg C/ns, (seg + 1) C/ns) and the tensor pass
+// over the (limb, slot) indices [seg 2N/ns, (seg + 1) 2N/ns), all groups,
+// writing each query's mat-vec partials and tensor-pass rows under its own
+// lane slot.  keys_pos: scratch for the keys in pass order (<= 32 queries).
 // after_matvec (may be null) is recorded once the mat-vec is enqueued.
-void enqueue_scan_segment(const Server& S, Lane& L, uint32_t* keys_pos, const std::vector<SlotRun>& runs, size_t g0,
-                          size_t gn, cudaStream_t st, cudaEvent_t after_matvec);
+void enqueue_scan_segment(const Server& S, Lane& L, uint32_t* keys_pos, const std::vector<SlotRun>& runs, int seg,
+                          int ns, cudaStream_t st, cudaEvent_t after_matvec);
+// Finalize (all groups) of lane slots r after their ns segments: packed
+// ciphertexts from the slots' mat-vec partials and tensor-pass rows.
+void enqueue_scan_finalize(const Server& S, Lane& L, const SlotRun& r, cudaStream_t st);
 
 }  // namespace ipb
 

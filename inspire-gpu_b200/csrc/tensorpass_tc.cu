@@ -178,9 +178,9 @@ struct TpParams {
     int w8;                // 8-query groups per key-table position
     const uint32_t* keyt;  // Kt[l][j][p][8 * w8], 32-byte aligned rows
     int G;                 // groups (Dt rows per slot: 4G)
-    int g0;                // first group of the range this launch covers
-    int gn;                // groups in the range
-    int mti;               // M tiles (128 rows) per item (4 gn >= 128)
+    int li0;               // first (limb, slot) index l * N + i of this launch
+    int n_li;              // (limb, slot) indices it covers
+    int mti;               // M tiles (128 rows) per item (4G >= 128)
     int n_mg;              // M-tile groups per (l, i)
     int spi;               // slots per item (4G < 128: several slots share one 128-row A tile)
     int rows_box;          // rows per A box
@@ -189,6 +189,8 @@ struct TpParams {
     uint32_t tmem_cols;
     int* err;
     unsigned* tiles;       // work-item counter, zero at launch
+    int has_qmap;          // output row of pass query p: qmap[p] (else q0 + p)
+    uint8_t qmap[32];
     uint32_t c[2][7];      // 256^k mod q_l
     uint64_t cr[2];
     uint32_t q[2];
@@ -246,7 +248,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int n_items = (2 * kN / P.spi) * P.n_mg;
+    const int n_items = (P.n_li / P.spi) * P.n_mg;
     constexpr int ktiles = kUPad / 128;
     const int acc_cols = P.mti * P.nb;
     const int slot_rows = 4 * P.G;  // A rows of one slot
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
             if (item < 0) break;
             if (!mbar_wait(&tfull[as], aph, P.err, 15)) { abort_flag = 1; break; }
             tc_fence_after();
-            const int li0 = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
+            const int li0 = P.li0 + (item / P.n_mg) * P.spi, mg = item % P.n_mg;
             const int l = li0 / kN;
             const uint32_t* c = P.c[l];
             // spi == 1: TMEM block mt (columns mt * nb) holds M-tile mt of the
@@ -283,10 +285,9 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
             for (int bi = 0; bi < nblk; ++bi) {
                 const int mt = blk0 + bi;
                 const int li = li0 + (P.spi > 1 ? mt : 0);
-                // (g - g0) * 4 + a
-                const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;
-                const int g = P.g0 + (grow >> 2), a = grow & 3;
-                const bool valid = grow >= 0 && grow < 4 * P.gn;
+                const int grow = P.spi > 1 ? row - mt * slot_rows : (mg * P.mti + mt) * 128 + row;  // g*4 + a
+                const int g = grow >> 2, a = grow & 3;
+                const bool valid = grow >= 0 && grow < slot_rows;
                 // four queries (16 columns) per TMEM load where the block has
                 // them; the block's last columns one query at a time
                 const int lim = P.spi > 1 ? P.nb : (mt + 1) * P.nb;
@@ -307,8 +308,10 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                         }
                     }
                     const uint64_t tot = tp_reduce4(v, c, a);
-                    if (valid && q + a < P.nq)
-                        P.out[((size_t)li * P.nq_total + P.q0 + q + a) * P.G + g] = mod_u64(tot, P.cr[l], P.q[l]);
+                    if (valid && q + a < P.nq) {
+                        const int qo = P.has_qmap ? P.qmap[P.q0 + q + a] : P.q0 + q + a;
+                        P.out[((size_t)li * P.nq_total + qo) * P.G + g] = mod_u64(tot, P.cr[l], P.q[l]);
+                    }
                 }
             }
             tc_fence_before();
@@ -332,8 +335,8 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                 item_ring[r] = item;
                 mbar_arrive(&ifull[r]);
                 if (item < 0) break;
-                const int li = (item / P.n_mg) * P.spi, mg = item % P.n_mg;
-                const int rowa = li * slot_rows + 4 * P.g0 + mg * P.mti * 128;
+                const int li = P.li0 + (item / P.n_mg) * P.spi, mg = item % P.n_mg;
+                const int rowa = li * slot_rows + mg * P.mti * 128;
                 for (int kt = 0; kt < ktiles; ++kt) {
                     if (!mbar_wait(&empty[s], ph ^ 1, P.err, 11)) { abort_flag = 1; break; }
                     uint8_t* st = smem + (size_t)s * stage_bytes;
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                 const int item = item_ring[r];
                 mbar_arrive(&iempty[r]);
                 if (item < 0) break;
-                const int li0 = (item / P.n_mg) * P.spi;
+                const int li0 = P.li0 + (item / P.n_mg) * P.spi;
                 const int l = li0 / kN;
                 const uint32_t* kl = P.keyt + (size_t)l * kDeff * kN * W;  // [j][p][W]
                 for (int kt = grp; grp < ngrp && kt < ktiles; kt += ngrp) {
@@ -547,17 +550,17 @@ cudaError_t launch_dt_export(const uint8_t* Dt, size_t g, size_t G, uint32_t* dp
 cudaError_t launch_tensor_pass(const uint8_t* Dt, size_t G, const uint32_t* keys, size_t key_qstride, int nq,
                                int nq_total, int q0, uint32_t* keyt, uint32_t* tp_out, int* err, unsigned* tiles,
                                int num_sms, cudaStream_t s) {
-    return launch_tensor_pass_range(Dt, G, 0, G, keys, key_qstride, nq, nq_total, q0, keyt, tp_out, err, tiles,
-                                    num_sms, s);
+    return launch_tensor_pass_slots(Dt, G, 0, 2 * kN, keys, key_qstride, nq, nq_total, q0, nullptr, keyt, tp_out, err,
+                                    tiles, num_sms, s);
 }
 
-cudaError_t launch_tensor_pass_range(const uint8_t* Dt, size_t G, size_t g0, size_t gn, const uint32_t* keys,
-                                     size_t key_qstride, int nq, int nq_total, int q0, uint32_t* keyt,
-                                     uint32_t* tp_out, int* err, unsigned* tiles, int num_sms, cudaStream_t s) {
+cudaError_t launch_tensor_pass_slots(const uint8_t* Dt, size_t G, int li0, int n_li, const uint32_t* keys,
+                                     size_t key_qstride, int nq, int nq_total, int q0, const uint8_t* qmap,
+                                     uint32_t* keyt, uint32_t* tp_out, int* err, unsigned* tiles, int num_sms,
+                                     cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    if (nq > 32 || !tiles) return cudaErrorInvalidValue;
-    // A part of the groups: whole 128-row M tiles of it (gn a multiple of 32)
-    if (gn == 0 || g0 + gn > G || (gn < G && gn % 32)) return cudaErrorInvalidValue;
+    if (nq > 32 || !tiles || (qmap && q0 + nq > 32)) return cudaErrorInvalidValue;
+    if (n_li <= 0 || li0 < 0 || li0 + n_li > 2 * kN || li0 % 32 || n_li % 32) return cudaErrorInvalidValue;
     const int rq = 4 * nq;
     const int W = 8 * ((nq + 7) / 8);
     const size_t kt_n = (size_t)2 * kDeff * kN * W;
@@ -573,9 +576,12 @@ cudaError_t launch_tensor_pass_range(const uint8_t* Dt, size_t G, size_t g0, siz
     P.w8 = W / 8;
     P.keyt = keyt;
     P.G = (int)G;
-    P.g0 = (int)g0;
-    P.gn = (int)gn;
-    const int nmt = (int)std::max<size_t>(1, (4 * gn + 127) / 128);
+    P.li0 = li0;
+    P.n_li = n_li;
+    P.has_qmap = qmap != nullptr;
+    if (qmap)
+        for (int p = 0; p < q0 + nq; ++p) P.qmap[p] = qmap[p];
+    const int nmt = (int)std::max<size_t>(1, (4 * G + 127) / 128);
     P.mti = std::min(nmt, 4);
     P.n_mg = nmt / P.mti;
     // Small G: pack spi slots (each 4G rows) into one 128-row A tile.  G even
@@ -583,12 +589,12 @@ cudaError_t launch_tensor_pass_range(const uint8_t* Dt, size_t G, size_t g0, siz
     // of two divides kN, so a packed item never straddles the two limbs.
     auto nb_of = [&](int sp) { return ((sp * rq + 15) / 16) * 16; };
     P.spi = 1;
-    if (4 * G < 128 && G % 2 == 0 && gn == G) {
+    if (4 * G < 128 && G % 2 == 0) {
         while (2 * P.spi * 4 * (int)G <= 128) P.spi *= 2;
         while (P.spi > 1 && (nb_of(P.spi) > 256 || 2 * nb_of(P.spi) > 512)) P.spi /= 2;
     }
     P.nb = nb_of(P.spi);
-    P.rows_box = (int)std::min<size_t>(128, 4 * gn * (size_t)P.spi);
+    P.rows_box = (int)std::min<size_t>(128, 4 * G * (size_t)P.spi);
     if (P.mti * P.nb > 512) return cudaErrorInvalidValue;
     P.acc_stages = (2 * P.mti * P.nb <= 512) ? 2 : 1;
     uint32_t need = (uint32_t)(P.acc_stages * P.mti * P.nb), tc = 32;
@@ -614,7 +620,7 @@ cudaError_t launch_tensor_pass_range(const uint8_t* Dt, size_t G, size_t g0, siz
     CUtensorMap ma;
     if (!make_map(&ma, Dt, (uint64_t)2 * kN * 4 * G, (uint32_t)P.rows_box)) return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
-    const int items = (2 * kN / P.spi) * P.n_mg;
+    const int items = (n_li / P.spi) * P.n_mg;
     if ((e = cudaMemsetAsync(tiles, 0, sizeof(unsigned), s))) return e;
     tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), kTpThreads, smem, s>>>(ma, P);
     return cudaGetLastError();

@@ -1,11 +1,12 @@
 """Serving loop in cyclic-scan mode (ipir_serve_config.scan_segments): the
-DB and tensor passes run as segments of 32 or 64 groups in rotation, and
-requests join at the next segment.  Every response must be bit-identical to
-the plain single answer of the same query (tolerance 0) whichever segment
-it joined at and whatever shared its segments; responses decrypt through
-the reference client's extract() to the queried entry.  A segment count
-that does not split the groups into multiples of 32 leaves the database on
-lane batches."""
+DB pass runs as column segments and the tensor pass as (limb, slot)
+segments in rotation, requests join at the next segment, and a query's
+partial results stay under its lane slot until its last segment.  Every
+response must be bit-identical to the plain single answer of the same query
+(tolerance 0) whichever segment it joined at and whatever shared its
+segments; responses decrypt through the reference client's extract() to the
+queried entry.  A segment count that does not split the columns into
+multiples of 128 leaves the database on lane batches."""
 import random
 import time
 
