@@ -275,7 +275,10 @@ int ipir_b200_answer_wire(ipir_server* srv, const uint8_t* packed, size_t count,
  * streaming the database and precomputed tensors, overlapping that batch's
  * Horner chains; requests that arrive meanwhile join it.  Lanes of
  * different databases run concurrently.  A lane batch replays the CUDA
- * graphs captured for its batch size at create.  All device and pinned memory is allocated at create,
+ * graphs captured for its batch size at create.  With scan_segments > 1 a
+ * database instead runs its DB and tensor passes as that many segments in
+ * rotation, and waiting requests join at the next segment (the config
+ * field says more).  All device and pinned memory is allocated at create,
  * with lanes sized to the HBM budget; submit, poll and wait allocate
  * nothing.  Each response is bit-identical to ipir_answer_batch on the same
  * query, whatever else shares its batch.
