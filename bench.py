@@ -511,7 +511,8 @@ def run_serve(args):
         rates = [float(x) for x in args.serve_rates.split(",")]
     t0 = time.perf_counter()
     loop = ib.ServeLoop(servers, max_batch=args.serve_max_batch, lanes_per_db=args.serve_lanes, queue_slots=512,
-                        overlap_db_passes=args.serve_overlap, scan_segments=args.serve_scan)
+                        overlap_db_passes=args.serve_overlap, scan_segments=args.serve_scan,
+                        autotune=not args.no_autotune)
     t_create = time.perf_counter() - t0
     views = [[ib.query_view_from_flat(servers[k].params, pools[k][i]) for i in range(pool_n)]
              for k in range(len(dbs))]
@@ -618,7 +619,7 @@ def run_serve(args):
                                         "split": split, "seconds_per_rate": args.serve_seconds,
                                         "max_batch": args.serve_max_batch, "lanes_per_db": args.serve_lanes,
                                         "overlap_db_passes": args.serve_overlap,
-                                        "scan_segments": args.serve_scan},
+                                        "scan_segments": args.serve_scan, "autotune": not args.no_autotune},
             "n_gpus": 1, "unit": "ms", "data": "synthetic queries (pool of 32 per database)",
             "plain": plain, "rates": results, "create_s": t_create,
             "lanes": [{"lanes": i["lanes"], "max_batch": i["max_batch"]} for i in infos],

@@ -86,3 +86,40 @@ def test_segments_that_do_not_split_fall_back_to_lanes(env):
     assert info["lanes"] == 2
     for i in range(6):
         assert (out[i] == singles[i]).all(), i
+
+
+def test_scan_packed_slots_and_generation_swap():
+    """G = 4: the tensor pass packs eight (limb, slot) items into one 128-row
+    tile, so each segment's slot range is whole packed items.  Scan responses
+    equal single answers, a duplicate index with fresh keys stays distinct,
+    and a generation swap replaces the database between rotations: after it
+    every response is the new handle's."""
+    import inspire_b200 as ib
+    c = get_case("medium")
+    live = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=4, crs_seed=c.seed)
+    nxt = ib.Server(c.n_entries, c.w, ib.fill_db(c.R * c.C, 91), db_rows=2048, max_batch=4, crs_seed=c.seed)
+    idx = [3, 200000, 3, 77, 262143, 1000]
+    qs = [c.query(i, 9300 + k) for k, i in enumerate(idx)]
+    try:
+        old = [live.answer(q) for q, _ in qs]
+        new = [nxt.answer(q) for q, _ in qs]
+        loop = ib.ServeLoop([live], max_batch=4, queue_slots=16, autotune=False, scan_segments=4)
+        try:
+            assert loop.db_info(0)["lanes"] == 1
+            r = np.zeros(ib.response_u64s(live.params), np.uint64)
+            for want in (old, new):
+                ts = [loop.submit(0, q) for q, _ in qs]
+                for k, t in enumerate(ts):
+                    loop.wait(t, out=r, timeout=60.0)
+                    assert (r == want[k]).all(), k
+                    if want is old and k in (0, 2):
+                        assert (qs[k][1].extract(r) == c.expected_slots(idx[k])).all(), k
+                if want is old:
+                    loop.replace_db(0, nxt)
+            assert loop.stats()["completed"] == 2 * len(qs)
+        finally:
+            loop.close()
+        assert not (old[0] == old[2]).all()
+    finally:
+        live.close()
+        nxt.close()
