@@ -74,8 +74,8 @@ def parse():
     ap.add_argument("--serve-overlap", action="store_true",
                     help="admit batches while the previous DB pass of their database still runs")
     ap.add_argument("--serve-scan", type=int, default=0,
-                    help="cyclic scan: DB passes as this many group segments in rotation, requests join at "
-                         "the next segment (databases whose groups split into multiples of 32)")
+                    help="cyclic scan: DB and tensor passes as this many segments in rotation, requests join "
+                         "at the next segment (databases whose columns split into multiples of 128)")
     return ap.parse_args()
 
 

@@ -16,6 +16,9 @@ struct DevTables;
 // qprep: keys [q][key(2)][limb][digit][N] NTT form, rgsw32 [q][4][digit][limb][N].
 cudaError_t launch_qprep(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
                          uint32_t* keys, uint32_t* rgsw32, int nq, cudaStream_t s);
+// Only some of it: parts 1 = the keys, 2 = the RGSW parts, 3 = both.
+cudaError_t launch_qprep_parts(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
+                               uint32_t* keys, uint32_t* rgsw32, int nq, int parts, cudaStream_t s);
 
 // Mat-vec row-split partials part[q][chunk][limb][cols] for nq <= 4 queries
 // sharing one DB stream.  chunks must divide rows.

@@ -50,9 +50,9 @@ __device__ __forceinline__ void st8(uint32_t* p, const uint32_t (&v)[8]) {
 __global__ void __launch_bounds__(256) qprep_kernel(const uint64_t* __restrict__ qraw, size_t qstride,
                                                     size_t rows, const DevTables* __restrict__ T,
                                                     uint32_t* __restrict__ keys,
-                                                    uint32_t* __restrict__ rgsw32) {
+                                                    uint32_t* __restrict__ rgsw32, int y0) {
     __shared__ __align__(16) uint32_t sbuf[2 * kN];
-    const int b = blockIdx.x, y = blockIdx.y;
+    const int b = blockIdx.x, y = y0 + (int)blockIdx.y;
     const uint32_t t = threadIdx.x;
     const uint64_t* qr = qraw + (size_t)b * qstride;
     const size_t blk = (size_t)kDeff * 2 * kN;
@@ -691,8 +691,15 @@ cudaError_t launch_fill_db(uint16_t* out, size_t count, uint64_t seed, cudaStrea
 // ==================================================================== wrappers
 cudaError_t launch_qprep(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
                          uint32_t* keys, uint32_t* rgsw32, int nq, cudaStream_t s) {
+    return launch_qprep_parts(qraw, qstride, rows, T, keys, rgsw32, nq, 3, s);
+}
+
+cudaError_t launch_qprep_parts(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
+                               uint32_t* keys, uint32_t* rgsw32, int nq, int parts, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    qprep_kernel<<<dim3(nq, 12), 256, 0, s>>>(qraw, qstride, rows, T, keys, rgsw32);
+    if (parts < 1 || parts > 3) return cudaErrorInvalidValue;
+    const int y0 = (parts & 1) ? 0 : 8, y1 = (parts & 2) ? 12 : 8;  // rows 0-7: key NTTs, 8-11: RGSW
+    qprep_kernel<<<dim3(nq, y1 - y0), 256, 0, s>>>(qraw, qstride, rows, T, keys, rgsw32, y0);
     return cudaGetLastError();
 }
 

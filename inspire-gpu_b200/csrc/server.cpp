@@ -216,6 +216,7 @@ void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
     IPB_CK(cudaStreamCreateWithFlags(&L.aux, cudaStreamNonBlocking));
     IPB_CK(cudaEventCreateWithFlags(&L.fork, cudaEventDisableTiming));
     IPB_CK(cudaEventCreateWithFlags(&L.join, cudaEventDisableTiming));
+    IPB_CK(cudaEventCreateWithFlags(&L.rgsw_ready, cudaEventDisableTiming));
     // Defined contents before any pipeline run (the autotuner runs on them).
     IPB_CK(cudaMemset(L.qraw, 0, cap * S.qstride * 8));
     IPB_CK(cudaMemset(L.planes, 0, mv_tc_planes_bytes(R, (int)cap)));
@@ -364,6 +365,7 @@ std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
 // lwe_ready (optional): the queries' LWE vectors arrive later than their
 // key parts (copied on another stream, this event marks them); the key side
 // (query prep, tensor pass) then runs first and the mat-vec after the event.
+// The RGSW parts are then prepared on that other stream as well.
 static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
                         cudaEvent_t lwe_ready = nullptr) {
     const Params& pp = S.pp;
@@ -372,7 +374,7 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
     const int nq = (int)count;
     int launches = 0;
     if (ev) IPB_CK(cudaEventRecord(ev[0], st));
-    IPB_CK(launch_qprep(L.qraw, S.qstride, R, P.tables, L.keys, L.rgsw32, nq, st));
+    IPB_CK(launch_qprep_parts(L.qraw, S.qstride, R, P.tables, L.keys, L.rgsw32, nq, lwe_ready ? 1 : 3, st));
     ++launches;
     if (ev) IPB_CK(cudaEventRecord(ev[1], st));
     // Beside: the tensor pass (keys only) on sc.tp_sms SMs from the lane's
@@ -517,11 +519,12 @@ static void run_pipeline(Server* S, size_t count) {
                                                     S->timing ? S->ev : nullptr);
 }
 
-// The blocking answer from host views: the key parts are copied first and
+// The blocking answer from host views: the KSK parts are copied first and
 // the query prep and tensor pass (which need only them) start while the
-// LWE vectors are still crossing PCIe on the lane's second stream; the
-// mat-vec waits for those.  Schedules that already run the tensor pass on
-// the second stream stage everything first instead.
+// LWE vectors and then the RGSW parts cross PCIe on the lane's second
+// stream; the mat-vec waits for the LWE vectors, the Horner chains for the
+// RGSW parts (prepared on that stream).  Schedules that already run the
+// tensor pass on the second stream stage everything first instead.
 static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
     IPB_CK(cudaSetDevice(S->device));
     const Sched& sc = sched_for(*S, count);
@@ -533,11 +536,16 @@ static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
     Lane& L = S->lane;
     IPB_CK(cudaEventRecord(L.fork, S->stream));  // the lane's buffers are free from here on
     IPB_CK(cudaStreamWaitEvent(L.aux, L.fork, 0));
-    stage_parts(*S, qs, count, 2, 3, S->stream);  // keys and RGSW: needed first
-    stage_parts(*S, qs, count, 0, 2, L.aux);      // LWE vectors: needed by the mat-vec only
+    stage_parts(*S, qs, count, 2, 2, S->stream);  // KSK parts: needed first
+    stage_parts(*S, qs, count, 0, 2, L.aux);      // LWE vectors: needed by the mat-vec
     IPB_CK(cudaEventRecord(L.join, L.aux));
+    stage_parts(*S, qs, count, 4, 1, L.aux);      // RGSW parts: needed by the Horner chains
+    IPB_CK(launch_qprep_parts(L.qraw, S->qstride, S->pp.db_rows, S->pre->tables, L.keys, L.rgsw32, (int)count, 2,
+                              L.aux));
+    IPB_CK(cudaEventRecord(L.rgsw_ready, L.aux));
     S->staged = count;
-    S->launches += (unsigned long long)run_db_phase(*S, L, sc, count, S->stream, nullptr, L.join);
+    S->launches += 1 + (unsigned long long)run_db_phase(*S, L, sc, count, S->stream, nullptr, L.join);
+    IPB_CK(cudaStreamWaitEvent(S->stream, L.rgsw_ready, 0));
     S->launches += (unsigned long long)run_horner_phase(*S, L, sc, count, S->stream, nullptr);
 }
 

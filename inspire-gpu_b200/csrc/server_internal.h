@@ -111,7 +111,9 @@ struct Lane {
     uint32_t* codec_tmp = nullptr;  // coefficient-form responses for compression
     cudaStream_t aux = nullptr;     // second stream: the tensor pass beside the mat-vec
     cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t rgsw_ready = nullptr;  // RGSW parts staged and prepared on aux
     ~Lane() {
+        if (rgsw_ready) cudaEventDestroy(rgsw_ready);
         if (join) cudaEventDestroy(join);
         if (fork) cudaEventDestroy(fork);
         if (aux) cudaStreamDestroy(aux);
