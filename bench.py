@@ -22,8 +22,9 @@ Poisson arrivals over resident databases and reports p50/p95/p99 latency and
 sustained q/s per offered rate, every response checked bit-exact against
 the plain single answer of the same query.  ``--serve-config mixed``: a
 1 GB database (setup(2^25, 30)) and a 4 GB one (setup(2^22, 960)), 70/30
-split, 50/100/200/400 q/s.  ``--serve-config 16gb``: the default workload at
-1, 3 and 5 times the plain per-query rate.
+split, 50/100/200/400 q/s, lane batches.  ``--serve-config 16gb``: the
+default workload at 1, 3 and 5 times the plain per-query rate, cyclic scan
+with 4 segments (``--serve-scan`` overrides either).
 
 ``--impl reference`` times the CPU restatement of the reference's server
 path (the reference has no CPU server of its own) on a bounded sample of
@@ -73,9 +74,10 @@ def parse():
     ap.add_argument("--serve-max-batch", type=int, default=64)
     ap.add_argument("--serve-overlap", action="store_true",
                     help="admit batches while the previous DB pass of their database still runs")
-    ap.add_argument("--serve-scan", type=int, default=0,
+    ap.add_argument("--serve-scan", type=int, default=None,
                     help="cyclic scan: DB and tensor passes as this many segments in rotation, requests join "
-                         "at the next segment (databases whose columns split into multiples of 128)")
+                         "at the next segment (databases whose columns split into multiples of 128); 0: lane "
+                         "batches; default 4 for --serve-config 16gb, 0 for mixed (the faster of each)")
     return ap.parse_args()
 
 
@@ -507,6 +509,8 @@ def run_serve(args):
     if rates is None:
         r1 = plain[0]["q_per_s"]
         rates = [r1, 3 * r1, 5 * r1]
+    if args.serve_scan is None:
+        args.serve_scan = 4 if args.serve_config == "16gb" else 0
     if args.serve_rates:
         rates = [float(x) for x in args.serve_rates.split(",")]
     t0 = time.perf_counter()
