@@ -123,3 +123,26 @@ def test_scan_packed_slots_and_generation_swap():
     finally:
         live.close()
         nxt.close()
+
+
+def test_close_with_requests_in_the_rotation(env):
+    """Destroying the loop right after submitting: the rotation runs its
+    admitted requests to the end (requests still waiting fail), and destroy
+    returns.  A watchdog thread bounds the wait so a regression fails the
+    test instead of hanging the run."""
+    import threading
+    ib, c, srv, idxs, qs, sts, singles = env
+    loop = ib.ServeLoop([srv], max_batch=8, queue_slots=64, autotune=False, scan_segments=4)
+    for q in qs:
+        loop.submit(0, q)
+    done = threading.Event()
+
+    def close():
+        loop.close()
+        done.set()
+
+    th = threading.Thread(target=close, daemon=True)
+    th.start()
+    assert done.wait(60.0), "ipir_serve_destroy did not return"
+    # the handle still answers on its own afterwards
+    assert (srv.answer(qs[0]) == singles[0]).all()
