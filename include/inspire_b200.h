@@ -350,11 +350,13 @@ int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_bat
  * failed, 6 another swap of db is in progress. */
 int ipir_serve_replace_db(ipir_serve* sv, size_t db, ipir_server* next);
 
-/* One lane batch, for tracing. */
+/* One lane batch (in cyclic-scan mode: one group of requests admitted at
+ * the same segment), for tracing. */
 typedef struct {
     double t_issue_s;  /* steady (CLOCK_MONOTONIC) seconds when the batch was issued */
-    float issue_ms;    /* host time to enqueue copies + graph replay */
-    float device_ms;   /* device time of the batch, copies included (CUDA events) */
+    float issue_ms;    /* host time to enqueue copies + graph replay (scan: admission, Horner and copies) */
+    float device_ms;   /* device time of the batch, copies included (CUDA events; scan: admission to
+                          response copy, the whole rotation) */
     float notice_ms;   /* bound on the delay from the batch's end to the worker handling it */
     uint16_t db, lane;
     uint32_t count;    /* queries in the batch */

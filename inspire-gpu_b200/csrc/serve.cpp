@@ -87,7 +87,8 @@ struct ScanGroup {
     std::vector<uint32_t> req;   // request slots, in lane-slot order
     cudaEvent_t ev_start = nullptr, ev_end = nullptr;
     int* h_err = nullptr;        // pinned copy of the device error word after its Horner chains
-    int64_t t_issue0 = 0, t_issue1 = 0;
+    int64_t t_issue0 = 0;        // steady-clock ns when its admission was enqueued
+    int64_t issue_ns = 0;        // host time spent enqueueing its admission, Horner chains and copies
 };
 
 struct ScanState {
@@ -315,6 +316,7 @@ void Engine::scan_step(DbState& d, std::unique_lock<std::mutex>& lk) {
                 IPB_CK(cudaMemcpyAsync(L.qraw + (fresh->s0 + i) * S.qstride, slots[fresh->req[i]].q, S.qstride * 8,
                                        cudaMemcpyHostToDevice, r.st));
             enqueue_qprep_slots(S, L, fresh->s0, fresh->k, r.st);
+            fresh->issue_ns = Clock::now().time_since_epoch().count() - fresh->t_issue0;
         }
         enqueue_scan_segment(S, L, sc.keys_pos, runs, seg, sc.ns, r.st, sc.ev_next);
         if (!done.empty()) {
@@ -322,6 +324,7 @@ void Engine::scan_step(DbState& d, std::unique_lock<std::mutex>& lk) {
             IPB_CK(cudaEventRecord(sc.ev_seg_end, r.st));
             IPB_CK(cudaStreamWaitEvent(sc.hst, sc.ev_seg_end, 0));
             for (auto& g : done) {
+                const int64_t t0 = Clock::now().time_since_epoch().count();
                 enqueue_horner(S, d.sched[g.k], L.packed_b + g.s0 * S.pb_qstride, L.rgsw32 + g.s0 * kRgswStride,
                                L.resp + g.s0 * S.resp_qstride, g.k, L.d_err, sc.hst);
                 for (size_t i = 0; i < g.k; ++i)
@@ -329,7 +332,7 @@ void Engine::scan_step(DbState& d, std::unique_lock<std::mutex>& lk) {
                                            S.resp_qstride * 8, cudaMemcpyDeviceToHost, sc.hst));
                 IPB_CK(cudaMemcpyAsync(g.h_err, L.d_err, sizeof(int), cudaMemcpyDeviceToHost, sc.hst));
                 IPB_CK(cudaEventRecord(g.ev_end, sc.hst));
-                g.t_issue1 = Clock::now().time_since_epoch().count();
+                g.issue_ns += Clock::now().time_since_epoch().count() - t0;
             }
         }
     } catch (const std::exception& e) {
@@ -391,11 +394,14 @@ void Engine::scan_finish(DbState& d, ScanGroup& g) {
     const auto now = Clock::now();
     float dev_ms = 0.f;
     if (cudaEventElapsedTime(&dev_ms, g.ev_start, g.ev_end) != cudaSuccess) dev_ms = -1.f;
-    const double notice = std::max(0.0, (now.time_since_epoch().count() - g.t_issue1) * 1e-6);
+    // Upper bound on the delay between the group's end and this call: wall
+    // time since its admission was enqueued, less its device time.
+    const double notice = std::max(0.0, (now.time_since_epoch().count() - g.t_issue0) * 1e-6 - dev_ms);
+    max_notice_ms = std::max(max_notice_ms, notice);
     if (!trace.empty()) {
         ipir_serve_batch_record& t = trace[trace_n++ % trace.size()];
         t.t_issue_s = g.t_issue0 * 1e-9;
-        t.issue_ms = (float)((g.t_issue1 - g.t_issue0) * 1e-6);
+        t.issue_ms = (float)(g.issue_ns * 1e-6);
         t.device_ms = dev_ms;
         t.notice_ms = (float)notice;
         t.db = 0;
