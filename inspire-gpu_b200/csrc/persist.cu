@@ -15,9 +15,16 @@
 // mix64(w_i + i * 0x9E3779B97F4A7C15) mod 2^64 (mix64: the splitmix64
 // finalizer), computed on the device, so a flipped, missing or moved word
 // changes it.
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "server_internal.h"
 
@@ -28,7 +35,7 @@ namespace {
 constexpr char kMagic[8] = {'I', 'P', 'I', 'R', 'B', '2', '0', '0'};
 constexpr uint32_t kVersion = 1;
 constexpr uint32_t kHeaderBytes = 256;
-constexpr size_t kChunk = (size_t)64 << 20;  // pinned staging per copy
+constexpr size_t kChunk = (size_t)64 << 20;  // pinned staging per copy (two, alternating)
 const char* const kSectionName[4] = {"DB", "a", "D byte planes", "D_final"};
 
 struct Header {
@@ -86,7 +93,7 @@ uint64_t device_checksum(const void* d, size_t bytes, unsigned long long* scratc
     return h;
 }
 
-// RAII holders for the host file, the pinned staging buffer, a stream.
+// RAII holders for the host file, a pinned staging buffer, a stream.
 struct File {
     FILE* f = nullptr;
     ~File() {
@@ -107,6 +114,59 @@ struct Stream {
         if (s) cudaStreamDestroy(s);
     }
 };
+// Waits for the stream when it leaves scope, so that no copy into or out of
+// the staging buffers (declared before it, destroyed after it) is in flight
+// when an error unwinds them.
+struct StreamDrain {
+    cudaStream_t s;
+    ~StreamDrain() { cudaStreamSynchronize(s); }
+};
+struct Events2 {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    Events2() {
+        for (auto& x : e) IPB_CK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    }
+    ~Events2() {
+        for (auto x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
+// n bytes between buf and the file at offset off (positional I/O).  Reads
+// are split over up to 8 host threads, so the page-cache copies run in
+// parallel (1 GB checkpoint: 0.29 -> 0.16 s to load; 4 GB: 1.0-1.7 ->
+// 0.3-0.6 s).  Writes use one thread: parallel writers to one new file were
+// slower.  write: buf -> file, else file -> buf.  False on a short transfer
+// or an error.
+bool file_io(int fd, void* buf, size_t n, off_t off, bool write) {
+    const size_t slice = (size_t)4 << 20;
+    const size_t parts = (n + slice - 1) / slice;
+    const size_t nt =
+        write ? 1 : std::min<size_t>(parts, std::max(1u, std::min(8u, std::thread::hardware_concurrency())));
+    std::atomic<bool> ok{true};
+    auto run = [&](size_t t) {
+        for (size_t pi = t; pi < parts && ok; pi += nt) {
+            size_t done = pi * slice;
+            const size_t end = std::min(n, done + slice);
+            while (done < end) {
+                char* b = static_cast<char*>(buf) + done;
+                const ssize_t r = write ? ::pwrite(fd, b, end - done, off + (off_t)done)
+                                        : ::pread(fd, b, end - done, off + (off_t)done);
+                if (r < 0 && errno == EINTR) continue;
+                if (r <= 0) {
+                    ok = false;
+                    return;
+                }
+                done += (size_t)r;
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nt; ++t) th.emplace_back(run, t);
+    run(0);
+    for (auto& x : th) x.join();
+    return ok;
+}
 
 void save(const Server& S, const char* path) {
     IPB_CK(cudaSetDevice(S.device));
@@ -138,16 +198,39 @@ void save(const Server& S, const char* path) {
     if (!f.f) throw IoError(std::string("cannot create ") + path);
     unsigned char head[kHeaderBytes] = {};
     std::memcpy(head, &h, sizeof h);
-    if (std::fwrite(head, 1, kHeaderBytes, f.f) != kHeaderBytes) throw IoError("write failed (header)");
-    Pinned buf(kChunk);
-    for (int k = 0; k < 4; ++k) {
-        const uint8_t* d = static_cast<const uint8_t*>(sec.dev[k]);
-        for (size_t off = 0; off < sec.bytes[k]; off += kChunk) {
-            const size_t n = std::min(kChunk, sec.bytes[k] - off);
-            IPB_CK(cudaMemcpyAsync(buf.p, d + off, n, cudaMemcpyDeviceToHost, st.s));
-            IPB_CK(cudaStreamSynchronize(st.s));
-            if (std::fwrite(buf.p, 1, n, f.f) != n)
-                throw IoError(std::string("write failed (") + kSectionName[k] + ")");
+    if (std::fwrite(head, 1, kHeaderBytes, f.f) != kHeaderBytes || std::fflush(f.f) != 0)
+        throw IoError("write failed (header)");
+    {
+        // Chunk c goes device -> staging buffer c % 2 while chunk c - 1 is
+        // written from the other buffer.
+        Pinned b0(kChunk), b1(kChunk);
+        void* buf[2] = {b0.p, b1.p};
+        Events2 ev;
+        StreamDrain drain{st.s};
+        const int fd = fileno(f.f);
+        off_t fpos = kHeaderBytes;
+        size_t c = 0, prev_n = 0;
+        int prev_k = 0;
+        for (int k = 0; k < 4; ++k) {
+            const uint8_t* d = static_cast<const uint8_t*>(sec.dev[k]);
+            for (size_t off = 0; off < sec.bytes[k]; off += kChunk, ++c) {
+                const size_t n = std::min(kChunk, sec.bytes[k] - off);
+                IPB_CK(cudaMemcpyAsync(buf[c & 1], d + off, n, cudaMemcpyDeviceToHost, st.s));
+                IPB_CK(cudaEventRecord(ev.e[c & 1], st.s));
+                if (c > 0) {
+                    IPB_CK(cudaEventSynchronize(ev.e[(c - 1) & 1]));
+                    if (!file_io(fd, buf[(c - 1) & 1], prev_n, fpos, true))
+                        throw IoError(std::string("write failed (") + kSectionName[prev_k] + ")");
+                    fpos += (off_t)prev_n;
+                }
+                prev_n = n;
+                prev_k = k;
+            }
+        }
+        if (c > 0) {
+            IPB_CK(cudaEventSynchronize(ev.e[(c - 1) & 1]));
+            if (!file_io(fd, buf[(c - 1) & 1], prev_n, fpos, true))
+                throw IoError(std::string("write failed (") + kSectionName[prev_k] + ")");
         }
     }
     const int c = std::fclose(f.f);
@@ -200,17 +283,28 @@ Server* load(const char* path, size_t max_batch) {
     alloc_precomp(*P, st.s);
     const Sections sec = sections_of(*P);
     {
-        Pinned buf(kChunk);
+        // Chunk c is read into staging buffer c % 2 while chunk c - 1
+        // crosses PCIe from the other one.
+        Pinned b0(kChunk), b1(kChunk);
+        void* buf[2] = {b0.p, b1.p};
+        Events2 ev;
+        StreamDrain drain{st.s};
+        const int fd = fileno(f.f);
+        off_t fpos = kHeaderBytes;
+        size_t c = 0;
         for (int k = 0; k < 4; ++k) {
             uint8_t* d = static_cast<uint8_t*>(sec.dev[k]);
-            for (size_t off = 0; off < sec.bytes[k]; off += kChunk) {
+            for (size_t off = 0; off < sec.bytes[k]; off += kChunk, ++c) {
                 const size_t n = std::min(kChunk, sec.bytes[k] - off);
-                if (std::fread(buf.p, 1, n, f.f) != n)
+                if (c >= 2) IPB_CK(cudaEventSynchronize(ev.e[c & 1]));  // the copy out of this buffer is done
+                if (!file_io(fd, buf[c & 1], n, fpos, false))
                     throw IoError(std::string("read failed (") + kSectionName[k] + ")");
-                IPB_CK(cudaMemcpyAsync(d + off, buf.p, n, cudaMemcpyHostToDevice, st.s));
-                IPB_CK(cudaStreamSynchronize(st.s));
+                fpos += (off_t)n;
+                IPB_CK(cudaMemcpyAsync(d + off, buf[c & 1], n, cudaMemcpyHostToDevice, st.s));
+                IPB_CK(cudaEventRecord(ev.e[c & 1], st.s));
             }
         }
+        IPB_CK(cudaStreamSynchronize(st.s));
     }
     int num_sms = 0;
     IPB_CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, P->device));
