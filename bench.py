@@ -15,7 +15,9 @@ through ipir_answer_batch with pinned host queries/responses (H2D + kernels +
 D2H inside the timed region); plus the plain batch-1 q/s, p50/p99 latency of
 the plain path, a batch sweep (B = 1, 8, 32, 64) with per-stage times, the
 DB-pass GB/s, the roofline of the mat-vec kernel, the kernel schedule the
-autotuner picked, and the CPU baseline (the oracle port on the host cores).
+autotuner picked, the CPU baseline (the oracle port on the host cores), and
+``serving``: the serving loop (cyclic scan) on the same database at 3x and
+5x the plain rate, p99 over the plain p50, every response checked.
 
 ``--mode serve`` drives the continuous-batching serving loop with open-loop
 Poisson arrivals over resident databases and reports p50/p95/p99 latency and
@@ -67,6 +69,8 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve-check", action="store_true",
+                    help="skip the serving-loop check (cyclic scan at 3x and 5x the plain rate) of the default run")
     ap.add_argument("--serve-config", default="mixed", choices=["mixed", "16gb"])
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-rates", default="")
@@ -283,6 +287,35 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ our arm
+def serve_check(ib, srv, params, qbuf, plain_lat_ms, seconds=8.0):
+    """The serving form on the benchmark's own database: a serving loop in
+    cyclic-scan mode (4 segments) under open-loop Poisson arrivals at 3x and
+    5x the plain per-query rate; p99 latency over the plain answer's p50,
+    every response compared with the plain answer of its query."""
+    pool_n = min(32, len(qbuf))
+    alone = [np.stack([srv.answer(qbuf[i]) for i in range(pool_n)])]
+    views = [[ib.query_view_from_flat(params, qbuf[i]) for i in range(pool_n)]]
+    r1 = 1000.0 / statistics.mean(plain_lat_ms)
+    p50_plain = sorted(plain_lat_ms)[len(plain_lat_ms) // 2]
+    loop = ib.ServeLoop([srv], max_batch=32, queue_slots=256, scan_segments=4)
+    try:
+        scan = loop.db_info(0)["lanes"] == 1
+        rng = random.Random(7)
+        rates = []
+        for x in (3, 5):
+            r = serve_rate(ib, loop, [srv], views, alone, [1.0], x * r1, seconds, rng)
+            rates.append({"x_plain_rate": x, "offered_q_per_s": r["offered_q_per_s"],
+                          "sustained_q_per_s": r["sustained_q_per_s"], "requests": r["requests"],
+                          "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+                          "p99_over_plain_p50": r["p99_ms"] / p50_plain if r["p99_ms"] else None,
+                          "mismatches": r["mismatches"], "failed": r["failed"]})
+    finally:
+        loop.close()
+    return {"mode": "cyclic scan, 4 segments" if scan else "lane batches", "plain_p50_ms": p50_plain,
+            "plain_q_per_s": r1, "seconds_per_rate": seconds, "rates": rates,
+            "bit_exact": all(r["mismatches"] == 0 and r["failed"] == 0 for r in rates)}
+
+
 def run_ours(args):
     import torch
     rank, local_rank, world = dist_env()
@@ -421,6 +454,9 @@ def run_ours(args):
     lat.sort()
     p50 = lat[len(lat) // 2]
     p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve_check:
+        serving = serve_check(ib, srv, params, qbuf, lat)
 
     mv1 = st1["matvec"]
     db_bytes = R * Ccols * 2
@@ -462,6 +498,8 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if serving:
+        line["serving"] = serving
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(params)
     srv.close()
@@ -472,6 +510,104 @@ def run_ours(args):
 
 
 # ------------------------------------------------------------------ serving loop
+def serve_rate(ib, loop, servers, views, alone, split, rate, seconds, rng):
+    """Open-loop Poisson arrivals at `rate` q/s for `seconds` on a serving
+    loop; every response is compared with the plain answer of its query
+    (alone[db][pool index])."""
+    pool_n = len(views[0])
+    s0 = loop.stats()
+    tickets = []          # (ticket, db, pool index)
+    lock = threading.Lock()
+    done = {"lat": [], "queue": [], "slow": [], "bad": 0, "n": 0, "failed": 0}
+    t_start = time.perf_counter()
+    finished = threading.Event()
+
+    def collector():
+        outs = [np.zeros(ib.response_u64s(s.params), np.uint64) for s in servers]
+        i = 0
+        while True:
+            with lock:
+                item = tickets[i] if i < len(tickets) else None
+            if item is None:
+                if finished.is_set():
+                    with lock:
+                        if i >= len(tickets):
+                            return
+                    continue
+                time.sleep(0.0002)
+                continue
+            t, k, qi, t_arr = item
+            lq = C_wait(loop, t, outs[k])
+            if lq is None:
+                done["failed"] += 1
+            else:
+                done["lat"].append(lq[0])
+                done["queue"].append(lq[1])
+                if lq[0] > 10.0:
+                    done["slow"].append((round(t_arr - t_start, 3), round(lq[0], 2), round(lq[1], 2), k))
+                if not np.array_equal(outs[k], alone[k][qi]):
+                    done["bad"] += 1
+            done["n"] += 1
+            i += 1
+
+    th = threading.Thread(target=collector)
+    th.start()
+    t_next = t_start
+    full = 0
+    late = 0.0
+    while True:
+        t_next += rng.expovariate(rate)
+        if t_next - t_start > seconds:
+            break
+        while True:
+            d = t_next - time.perf_counter()
+            if d <= 0:
+                break
+            time.sleep(min(d, 0.001) if d > 0.0015 else 0)
+        k = 0 if rng.random() < split[0] else 1 if len(servers) > 1 else 0
+        qi = rng.randrange(pool_n)
+        while True:
+            rc, t = loop.submit_view(k, views[k][qi])
+            if rc != ib.SERVE_FULL:
+                break
+            full += 1
+            time.sleep(0.0005)
+        assert rc == 0, (rc, ib.last_error())
+        late = max(late, time.perf_counter() - t_next)
+        with lock:
+            tickets.append((t, k, qi, t_next))
+    finished.set()
+    th.join()
+    wall = time.perf_counter() - t_start
+    s1 = loop.stats()
+    lat = sorted(done["lat"])
+
+    def pct(p):
+        return lat[min(len(lat) - 1, int(round(p * (len(lat) - 1))))] if lat else None
+
+    qs = sorted(done["queue"])
+
+    def qpct(p):
+        return qs[min(len(qs) - 1, int(round(p * (len(qs) - 1))))] if qs else None
+
+    tr = [r for r in loop.trace() if r["t_issue_s"] >= t_start]
+    slow_batches = sorted(([round(r["t_issue_s"] - t_start, 3), round(r["issue_ms"], 2), round(r["device_ms"], 2),
+                            round(r["notice_ms"], 3), r["db"], r["lane"], r["count"]]
+                           for r in tr if r["device_ms"] > 5.0 or r["issue_ms"] > 2.0), key=lambda x: x[0])
+    dev = sorted(r["device_ms"] for r in tr)
+    nb = s1["batches"] - s0["batches"]
+    return {"offered_q_per_s": rate, "sustained_q_per_s": done["n"] / wall,
+            "requests": done["n"], "p50_ms": pct(0.50), "p95_ms": pct(0.95), "p99_ms": pct(0.99),
+            "max_ms": lat[-1] if lat else None, "mismatches": done["bad"], "failed": done["failed"],
+            "batches": nb, "mean_batch": (s1["batched_queries"] - s0["batched_queries"]) / max(1, nb),
+            "queue_full_retries": full, "queue_p50_ms": qpct(0.5), "queue_p99_ms": qpct(0.99),
+            "slow_over_10ms": done["slow"][:20], "max_notice_ms": s1["max_notice_ms"],
+            "batch_device_ms_p50": dev[len(dev) // 2] if dev else None,
+            "batch_device_ms_max": dev[-1] if dev else None,
+            "slow_batches_t_issue_dev_notice_db_lane_n": slow_batches[:20],
+            "generator_max_late_ms": late * 1e3}
+
+
 def run_serve(args):
     """Open-loop Poisson load on the continuous-batching serving loop."""
     import torch
@@ -523,97 +659,7 @@ def run_serve(args):
     results = []
     rng = random.Random(6)
     for rate in rates:
-        s0 = loop.stats()
-        tickets = []          # (ticket, db, pool index)
-        lock = threading.Lock()
-        done = {"lat": [], "queue": [], "slow": [], "bad": 0, "n": 0, "failed": 0}
-        t_start = time.perf_counter()
-        finished = threading.Event()
-
-        def collector():
-            outs = [np.zeros(ib.response_u64s(s.params), np.uint64) for s in servers]
-            i = 0
-            while True:
-                with lock:
-                    item = tickets[i] if i < len(tickets) else None
-                if item is None:
-                    if finished.is_set():
-                        with lock:
-                            if i >= len(tickets):
-                                return
-                        continue
-                    time.sleep(0.0002)
-                    continue
-                t, k, qi, t_arr = item
-                lq = C_wait(loop, t, outs[k])
-                if lq is None:
-                    done["failed"] += 1
-                else:
-                    done["lat"].append(lq[0])
-                    done["queue"].append(lq[1])
-                    if lq[0] > 10.0:
-                        done["slow"].append((round(t_arr - t_start, 3), round(lq[0], 2), round(lq[1], 2), k))
-                    if not np.array_equal(outs[k], alone[k][qi]):
-                        done["bad"] += 1
-                done["n"] += 1
-                i += 1
-
-        th = threading.Thread(target=collector)
-        th.start()
-        t_next = t_start
-        full = 0
-        late = 0.0
-        while True:
-            t_next += rng.expovariate(rate)
-            if t_next - t_start > args.serve_seconds:
-                break
-            while True:
-                d = t_next - time.perf_counter()
-                if d <= 0:
-                    break
-                time.sleep(min(d, 0.001) if d > 0.0015 else 0)
-            k = 0 if rng.random() < split[0] else 1 if len(dbs) > 1 else 0
-            qi = rng.randrange(pool_n)
-            while True:
-                rc, t = loop.submit_view(k, views[k][qi])
-                if rc != ib.SERVE_FULL:
-                    break
-                full += 1
-                time.sleep(0.0005)
-            assert rc == 0, (rc, ib.last_error())
-            late = max(late, time.perf_counter() - t_next)
-            with lock:
-                tickets.append((t, k, qi, t_next))
-        finished.set()
-        th.join()
-        wall = time.perf_counter() - t_start
-        s1 = loop.stats()
-        lat = sorted(done["lat"])
-
-        def pct(p):
-            return lat[min(len(lat) - 1, int(round(p * (len(lat) - 1))))] if lat else None
-
-        qs = sorted(done["queue"])
-
-        def qpct(p):
-            return qs[min(len(qs) - 1, int(round(p * (len(qs) - 1))))] if qs else None
-
-        tr = [r for r in loop.trace() if r["t_issue_s"] >= t_start]
-        slow_batches = sorted(([round(r["t_issue_s"] - t_start, 3), round(r["issue_ms"], 2), round(r["device_ms"], 2),
-                                round(r["notice_ms"], 3), r["db"], r["lane"], r["count"]]
-                               for r in tr if r["device_ms"] > 5.0 or r["issue_ms"] > 2.0), key=lambda x: x[0])
-        dev = sorted(r["device_ms"] for r in tr)
-        nb = s1["batches"] - s0["batches"]
-        results.append({"offered_q_per_s": rate, "sustained_q_per_s": done["n"] / wall,
-                        "requests": done["n"], "p50_ms": pct(0.50), "p95_ms": pct(0.95), "p99_ms": pct(0.99),
-                        "max_ms": lat[-1] if lat else None, "mismatches": done["bad"], "failed": done["failed"],
-                        "batches": nb, "mean_batch": (s1["batched_queries"] - s0["batched_queries"]) / max(1, nb),
-                        "queue_full_retries": full, "queue_p50_ms": qpct(0.5), "queue_p99_ms": qpct(0.99),
-                        "slow_over_10ms": done["slow"][:20], "max_notice_ms": s1["max_notice_ms"],
-                        "batch_device_ms_p50": dev[len(dev) // 2] if dev else None,
-                        "batch_device_ms_max": dev[-1] if dev else None,
-                        "slow_batches_t_issue_dev_notice_db_lane_n": slow_batches[:20],
-                        "generator_max_late_ms": late * 1e3})
+        results.append(serve_rate(ib, loop, servers, views, alone, split, rate, args.serve_seconds, rng))
     infos = [loop.db_info(k) for k in range(len(dbs))]
     loop.close()
     for s in servers:
