@@ -29,8 +29,8 @@ default workload at 1, 3 and 5 times the plain per-query rate, cyclic scan
 with 4 segments (``--serve-scan`` overrides either).
 
 ``--impl reference`` times the CPU restatement of the reference's server
-path (the reference has no CPU server of its own) on a bounded sample of
-the same workload.  Multi-GPU: every rank serves an independent replica.
+path (the reference has no CPU server of its own) answering one full query
+per step, unsampled, on all host threads; it loads nothing of this build.  Multi-GPU: every rank serves an independent replica.
 """
 import argparse
 import json
@@ -205,83 +205,131 @@ def measured_peaks():
 
 
 # ------------------------------------------------------------------ CPU leg
-def cpu_sample(params, seconds_hint=15.0):
-    """Time the oracle port (CPU restatement of the server path) on a bounded
-    sample of the workload and scale to q/s: mat-vec over a column slice,
-    the tensor pass of a few groups, and the full Horner chain; the DB,
-    precomp and query are synthetic (the work does not depend on values)."""
-    sys.path.insert(0, os.path.join(REPO, "tests"))
-    import ctypes as C
-    from oracle_lib import Oracle, ptr, u16p, u32p, u64p
-    o = Oracle()
-    threads = o.L.orc_num_threads()
-    R, Ccols, G = params["db_rows"], params["db_cols"], params["n_packed"]
-    D = min(params["interp_d"], G)
-    rng = np.random.default_rng(5)
-    # mat-vec on a slice of columns (all rows)
-    cs = 2048
-    db = rng.integers(0, 65535, R * cs, dtype=np.uint16)
-    b = np.concatenate([rng.integers(0, Q[0], R, dtype=np.uint64), rng.integers(0, Q[1], R, dtype=np.uint64)])
-    out = np.zeros(2 * cs, np.uint64)
-    t0 = time.perf_counter()
-    o.L.orc_matvec(ptr(db, u16p), R, cs, ptr(b, u64p), 0, cs, ptr(out, u64p))
-    t_mv = (time.perf_counter() - t0) * (Ccols / cs)
-    # tensor pass of sample groups (one at a time, as the CPU loop would)
-    ng = 2
-    dp = rng.integers(0, Q[0], 2 * NSTEPS * 2 * N, dtype=np.uint32)
-    dm = rng.integers(0, Q[0], 2 * NSTEPS * 2 * N, dtype=np.uint32)
-    df = rng.integers(0, Q[0], 2 * 2 * N, dtype=np.uint32)
-    k5 = rng.integers(0, Q[0], 2 * 2 * N, dtype=np.uint64)
-    kn = rng.integers(0, Q[0], 2 * 2 * N, dtype=np.uint64)
-    r = rng.integers(0, Q[0], 2 * N, dtype=np.uint64)
-    ob = np.zeros(2 * N, np.uint64)
-    t0 = time.perf_counter()
-    for _ in range(ng):
-        o.L.orc_pack_group(ptr(r, u64p), N, 0, ptr(dp, u32p), ptr(dm, u32p), ptr(df, u32p),
-                           ptr(k5, u64p), ptr(kn, u64p), ptr(ob, u64p))
-    t_pack_1 = (time.perf_counter() - t0) / ng
-    # groups run in parallel on the host threads
-    t_pack = t_pack_1 * G / max(1, min(threads, G))
-    # Horner chain of D cts (serial)
-    L = min(D, 8)
-    rg = np.concatenate([rng.integers(0, Q[(x // N) & 1], N, dtype=np.uint64) for x in range(0, 16 * N, N)])
-    pk = np.concatenate([rng.integers(0, Q[(x // N) & 1], N, dtype=np.uint64) for x in range(0, 4 * N * L, N)])
-    oh = np.zeros(4 * N, np.uint64)
-    t0 = time.perf_counter()
-    o.L.orc_horner(ptr(rg, u64p), ptr(pk, u64p), L, ptr(oh, u64p))
-    t_h = (time.perf_counter() - t0) / max(1, L - 1) * max(0, D - 1) * params["num_cts"]
-    per_query = t_mv + t_pack + t_h
-    return {"value": 1.0 / per_query, "unit": "q/s", "cores": threads, "kind": "port",
-            "sample": (f"oracle port on {threads} host threads: mat-vec over {cs} of {Ccols} columns x all "
-                       f"{R} rows scaled by {Ccols // cs}; tensor pass of {ng} of {G} groups scaled to {G} "
-                       f"groups over the threads; Horner {L - 1} of {D - 1} ExtProd steps scaled; "
-                       f"per-query {per_query:.2f} s = mat-vec {t_mv:.2f} + tensor {t_pack:.2f} + Horner {t_h:.2f}")}
+def host_mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
 
+
+class CpuQuery:
+    """The CPU restatement of the reference's server path (the oracle port:
+    orc_answer = mat-vec over every DB column, the tensor pass of every group
+    in parallel on all host threads, the full Horner chain) answering one
+    whole query, unsampled.  Geometry comes from the reference's own setup()
+    (its CPU library built from its sources); the DB, the precomputed
+    tensors and the query are synthetic residues (the work does not depend
+    on their values).  If the host cannot hold the DB and the tensors, the
+    1 GB geometry setup(2^25, 30) is used instead and the sample says so."""
+
+    def __init__(self, n_entries, w):
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        from oracle_lib import PRE_A, PRE_D, PRE_F, Oracle, RefLib
+        self.o = Oracle()
+        self.threads = self.o.L.orc_num_threads()
+        ref = RefLib()
+        geom = ref.setup(n_entries, w)
+        need = lambda g: g[2] * g[3] * 2 + g[4] * (PRE_A + 2 * PRE_D + PRE_F) * 4
+        avail = host_mem_available()
+        self.note = ""
+        if avail is not None and need(geom) > 0.7 * avail:
+            self.note = (f"; host MemAvailable {avail / 1e9:.0f} GB cannot hold the {need(geom) / 1e9:.1f} GB "
+                         f"geometry, so the 1 GB geometry setup(2^25, 30) is timed instead")
+            geom = ref.setup(1 << 25, 30)
+        self.geom = geom
+        _, _, R, Cc, G, D, ncts = geom
+        self.R, self.C, self.D = R, Cc, D
+        t0 = time.perf_counter()
+        self.db = self.o.fill_db(R * Cc, 0)
+        self.pa = self.o.fill_u32_mod(G * PRE_A, 1, Q[0])
+        self.pdp = self.o.fill_u32_mod(G * PRE_D, 2, Q[0])
+        self.pdm = self.o.fill_u32_mod(G * PRE_D, 3, Q[0])
+        self.pdf = self.o.fill_u32_mod(G * PRE_F, 4, Q[0])
+        self.fill_s = time.perf_counter() - t0
+        rng = np.random.default_rng(5)
+        qn = 2 * R + 6 * 2 * 2 * N
+        q = np.empty(qn, np.uint64)
+        q[:R] = rng.integers(0, Q[0], R, dtype=np.uint64)
+        q[R:2 * R] = rng.integers(0, Q[1], R, dtype=np.uint64)
+        rest = q[2 * R:].reshape(-1, N)
+        for r in range(rest.shape[0]):
+            rest[r] = rng.integers(0, Q[r & 1], N, dtype=np.uint64)
+        self.q = q
+        self.resp = np.zeros(ncts * 4 * N, np.uint64)
+
+    def answer_s(self):
+        from oracle_lib import ptr, u16p, u32p, u64p
+        args = (ptr(self.db, u16p), self.R, self.C, self.D, ptr(self.pa, u32p), ptr(self.pdp, u32p),
+                ptr(self.pdm, u32p), ptr(self.pdf, u32p), ptr(self.q, u64p), ptr(self.resp, u64p))
+        t0 = time.perf_counter()
+        rc = self.o.L.orc_answer(*args)
+        t = time.perf_counter() - t0
+        assert rc == 0
+        return t
+
+    def sample(self, n_timed):
+        _, _, R, Cc, G, D, ncts = self.geom
+        return (f"oracle port (CPU restatement of the reference's server path), one full query per step, "
+                f"unsampled and measured: mat-vec over all {R} x {Cc} DB entries, the tensor pass of all {G} "
+                f"groups, {ncts} Horner chain(s) of {min(D, G) - 1} ExtProd steps; {self.threads} host threads "
+                f"(OpenMP over columns and groups; the Horner chain is serial); {n_timed} timed queries; "
+                f"synthetic DB, tensors and query{self.note}")
+
+
+def cpu_baseline(n_entries, w, timed=2):
+    """cpu_baseline of our arm's line: the same full CPU query, median of
+    `timed` runs after one untimed run."""
+    cq = CpuQuery(n_entries, w)
+    cq.answer_s()
+    ts = [cq.answer_s() for _ in range(timed)]
+    t = statistics.median(ts)
+    return {"value": 1.0 / t, "unit": "q/s", "cores": cq.threads, "kind": "port", "ms_per_query": t * 1e3,
+            "sample": cq.sample(timed)}
+
+
+def line_config(params, B, world):
+    """The `config` both arms report (the same workload)."""
+    db_bytes = params["db_rows"] * params["db_cols"] * 2
+    return {"workload": describe(params) + f"; batch {B}",
+            "model": "InsPIRe PIR server", "global_batch": B * world, "seq_len": 0,
+            "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 ({db_bytes / 1e9:.1f} GB DB read per step)"}
+
+
+METRIC = "q/s at 16 GB DB (plain batch-1 vs served batch-32), p50/p99 latency, DB-pass GB/s"
 
 
 # ------------------------------------------------------------------ reference arm
 def run_reference(args):
+    """The reference has no CPU server of its own (docs/ARCHITECTURE.md:378-380),
+    so its CPU path is the oracle port: one full query per step on all host
+    threads.  Nothing of this build's library is loaded here: the geometry
+    comes from the reference's own setup()."""
     rank, _, world = dist_env()
     if rank != 0:
         return
-    import inspire_b200 as ib
-    params = ib.setup(args.n_entries, args.entry_bytes)
-    vals = []
-    for _ in range(max(1, args.warmup)):
-        cpu_sample(params)
-    for _ in range(args.steps):
-        vals.append(cpu_sample(params)["value"])
-    last = cpu_sample(params)
-    v = statistics.median(vals)
-    line = {"impl": "reference",
-            "metric": "q/s at 16 GB DB (plain batch-1 vs served batch-32), p50/p99 latency, DB-pass GB/s",
+    cq = CpuQuery(args.n_entries, args.entry_bytes)
+    _, _, R, Cc, G, D, ncts = cq.geom
+    params = {"n_entries": cq.geom[0], "entry_bytes": cq.geom[1], "db_rows": R, "db_cols": Cc, "n_packed": G,
+              "interp_d": D, "num_cts": ncts}
+    for _ in range(args.warmup):
+        cq.answer_s()
+    ts = [cq.answer_s() for _ in range(args.steps)]
+    t = sum(ts) / len(ts)
+    v = 1.0 / t
+    line = {"impl": "reference", "metric": METRIC,
             "value": v, "unit": "q/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64 modular",
-            "data": "synthetic",
-            "config": {"workload": describe(params) + "; CPU restatement, one query at a time",
-                       "model": "InsPIRe PIR server", "global_batch": 1, "seq_len": 0, "parallelism": "replicas"},
-            "cpu_baseline": {"value": v, "unit": "q/s", "cores": last["cores"], "kind": last["kind"],
-                             "sample": last["sample"]},
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32/u64 modular (exact)", "data": "synthetic",
+            "config": line_config(params, args.batch, 1),
+            "queries_per_step": 1,
+            "ms_per_step_p50": statistics.median(ts) * 1e3, "fill_s": cq.fill_s,
+            "cpu_baseline": {"value": v, "unit": "q/s", "cores": cq.threads, "kind": "port",
+                             "sample": cq.sample(args.steps)},
             "e2e": {"value": v, "unit": "q/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -467,14 +515,11 @@ def run_ours(args):
     sched1 = srv.schedule(1)
 
     line = {
-        "metric": "q/s at 16 GB DB (plain batch-1 vs served batch-32), p50/p99 latency, DB-pass GB/s",
+        "metric": METRIC,
         "value": value, "unit": "q/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": msB, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32/u64 modular (exact)", "data": "synthetic",
-        "config": {"workload": describe(params) + f"; batch {B}",
-                   "model": "InsPIRe PIR server", "global_batch": B * world, "seq_len": 0,
-                   "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2 ({db_bytes / 1e9:.1f} GB DB read per step)"},
+        "config": line_config(params, B, world),
         "plain_b1": {"q_per_s": 1000.0 / ms1, "ms": ms1, "p50_ms_e2e": p50, "p99_ms_e2e": p99},
         "served": {"batch": B, "ms_per_batch": msB, "q_per_s": value / world},
         "batch_sweep": sweep_out,
@@ -501,7 +546,7 @@ def run_ours(args):
     if serving:
         line["serving"] = serving
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(params)
+        line["cpu_baseline"] = cpu_baseline(args.n_entries, args.entry_bytes)
     srv.close()
     if world > 1:
         torch.distributed.destroy_process_group()

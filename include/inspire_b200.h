@@ -195,14 +195,22 @@ int ipir_b200_matvec_ex(const uint16_t* db, size_t rows, size_t cols, const uint
  * library keeps until the process exits.  Limits: rows a multiple of 1024
  * and <= 32768, count <= 8, cols a multiple of 128; larger shapes return 2
  * with the reason in ipir_b200_last_error().  The first call on a device
- * resolves the array's device address and writes the NTT tables into it:
- * make that first call before any stream capture.  All calls share the one
- * array, so calls whose GPU work overlaps (other streams, other threads)
- * race; serialise them.  The call synchronises `stream` and returns 0, 1
- * null argument, 2 shape beyond the limits, 4 CUDA error, 5 device wait
- * timeout. */
+ * (and the first after a device reset, which gives the device a new
+ * context) resolves the array's device address and writes the NTT tables
+ * into it with a copy on `stream` that it waits for: make that first call
+ * before any stream capture.  All calls share the one array, so calls whose
+ * GPU work overlaps (other streams, other threads) race; serialise them.
+ * The call synchronises `stream` only (the error word is read back on it)
+ * and returns 0, 1 null argument, 2 shape beyond the limits, 4 CUDA error,
+ * 5 device wait timeout. */
 int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries,
                              size_t count, uint32_t* out, void* stream);
+
+/* Target of the library's device code as the CUDA runtime loaded it:
+ * *out = cudaFuncAttributes.binaryVersion of its tensor-core mat-vec kernel
+ * (100 for the sm_100a cubins this library is built from).  Returns 0, 1
+ * null argument, 4 CUDA error.  No counterpart in the reference. */
+int ipir_b200_kernel_binary_version(int* out);
 
 /* Synthetic database for benchmarks and tests: out[k] = splitmix64(seed ^ k)
  * mod 65535 for k < count, filled on all host threads. */
@@ -216,13 +224,16 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
  * 8-CTA cluster (2) or one CTA per chain (0); tp_sms > 0 runs the tensor
  * pass on that many SMs at the same time as the tensor-core mat-vec on the
  * others (the two read disjoint data: the tensor pass is DRAM-bound, the
- * batched mat-vec tensor-core-bound), 0 runs them one after the other.
+ * batched mat-vec tensor-core-bound), 0 runs them one after the other;
+ * slice = 32 runs a batch of more than 32 queries as consecutive 32-query
+ * pipelines (query prep to Horner), 0 as one pipeline.
  * Every schedule gives the same responses. */
 typedef struct {
     int matvec_tc;
     int tp_pass;
     int horner_cluster;
     int tp_sms;
+    int slice;
 } ipir_serve_schedule;
 
 /* Time the candidate schedules on this handle for batch sizes 1, 2, 4, ...

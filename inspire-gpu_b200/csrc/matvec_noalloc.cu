@@ -31,26 +31,65 @@ constexpr size_t kNoAllocScratchBytes = kNoAllocPlanesOff + kNoAllocPlanesBytes;
 __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
 std::mutex g_noalloc_mu;
-uint8_t* g_noalloc_addr[64];  // device address of g_noalloc_scratch, per device
+struct NoAllocDevice {
+    unsigned long long ctx_id;  // CUDA context the tables were written in (0: none yet)
+    uint8_t* addr;              // device address of g_noalloc_scratch in that context
+};
+NoAllocDevice g_noalloc_dev[64];
 
-// Once per device, with that device current: resolve the array's device
-// address (the host symbol is only a stand-in) and write the NTT tables into
-// it.  No allocation.
-cudaError_t noalloc_setup(int dev, uint8_t** out) {
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+// Unique id of the calling thread's current CUDA context (driver entry points
+// through the runtime, so the library needs no -lcuda).  A device reset
+// destroys the context and the module with it; a new context gets a new id,
+// which makes the next call write the tables again.
+cudaError_t current_context_id(unsigned long long* id) {
+    typedef int (*get_current_t)(void**);
+    typedef int (*get_id_t)(void*, unsigned long long*);
+    static get_current_t get_current = nullptr;
+    static get_id_t get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &qr) == cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<get_current_t>(p);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &qr) == cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<get_id_t>(p);
+    });
+    if (!get_current || !get_id) return cudaErrorNotSupported;
+    void* ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
+}
+
+// Per device and context, with that device current: resolve the array's
+// device address (the host symbol is only a stand-in) and write the NTT
+// tables into it.  The copy is enqueued on the caller's stream and waited for
+// under the lock, so neither this call's kernels (same stream) nor another
+// thread's call on another stream can read the tables before they land.  No
+// allocation.
+cudaError_t noalloc_setup(int dev, cudaStream_t s, uint8_t** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // also makes the context current
+    if (e != cudaSuccess) return e;
+    unsigned long long ctx = 0;
+    e = current_context_id(&ctx);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (d.ctx_id != ctx || d.addr != p) {
         static DevTables host_T;
         static std::once_flag once;
         std::call_once(once, [] { build_tables(host_T); });
-        e = cudaMemcpy(static_cast<uint8_t*>(p) + kNoAllocTablesOff, &host_T, sizeof(DevTables),
-                       cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(static_cast<uint8_t*>(p) + kNoAllocTablesOff, &host_T, sizeof(DevTables),
+                            cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return e;
-        g_noalloc_addr[dev] = static_cast<uint8_t*>(p);
+        d.ctx_id = ctx;
+        d.addr = static_cast<uint8_t*>(p);
     }
-    *out = g_noalloc_addr[dev];
+    *out = d.addr;
     return cudaSuccess;
 }
 }  // namespace
@@ -74,13 +113,13 @@ extern "C" int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t 
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess && (dev < 0 || dev >= 64)) e = cudaErrorInvalidDevice;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     uint8_t* base = nullptr;
-    if (e == cudaSuccess) e = noalloc_setup(dev, &base);
+    if (e == cudaSuccess) e = noalloc_setup(dev, s, &base);
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));
         return 4;
     }
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const DevTables* T = reinterpret_cast<const DevTables*>(base + kNoAllocTablesOff);
     int* err = reinterpret_cast<int*>(base + kNoAllocErrOff);
     unsigned* tiles = reinterpret_cast<unsigned*>(base + kNoAllocErrOff + 128);  // same 256-byte slot
@@ -90,9 +129,9 @@ extern "C" int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t 
     // rows <= 32768: one exact K-chunk, so the kernel writes the result directly.
     if (e == cudaSuccess)
         e = launch_matvec_tc(db, rows, cols, planes, (int)count, T, out, 2 * cols, err, tiles, sms, (int)rows, s);
+    int h_err = 0;  // read back on the caller's stream: no device-wide synchronisation
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    int h_err = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
         set_last_error(cudaGetErrorString(e));
         return 4;

@@ -438,3 +438,19 @@ cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, s
 
 }  // namespace ipb
 
+// Target of the device code this library carries, read back from the loaded
+// module (cudaFuncGetAttributes on the tensor-core mat-vec kernel):
+// binaryVersion is 100 for sm_100a cubins.  No counterpart in the reference.
+extern "C" int ipir_b200_kernel_binary_version(int* out) {
+    if (!out) return 1;
+    cudaFuncAttributes a{};
+    cudaError_t e = cudaFuncGetAttributes(&a, ipb::mv_tc_kernel);
+    if (e != cudaSuccess) {
+        ipb::set_last_error(cudaGetErrorString(e));
+        return 4;
+    }
+    *out = a.binaryVersion;
+    return 0;
+}
+
+

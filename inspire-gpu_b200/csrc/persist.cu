@@ -332,6 +332,7 @@ int ipir_b200_save_server(const ipir_server* srv, const char* path) {
         ipb::set_last_error("ipir_b200_save_server: null argument");
         return 1;
     }
+    ipb::DeviceRestore keep_device;  // save() switches to the handle's device
     try {
         ipb::save(*srv->s, path);
         return 0;
@@ -349,6 +350,7 @@ ipir_server* ipir_b200_load_server(const char* path, size_t max_batch, ipir_para
         ipb::set_last_error("ipir_b200_load_server: null argument or max_batch == 0");
         return nullptr;
     }
+    ipb::DeviceRestore keep_device;
     try {
         ipb::Server* S = ipb::load(path, max_batch);
         ipb::fill_params(S->pp, out_params);

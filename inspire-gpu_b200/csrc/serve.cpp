@@ -644,6 +644,7 @@ struct ipir_serve {
 namespace {
 template <class F>
 int serve_guarded(F&& f, int fail_code) {
+    ipb::DeviceRestore keep_device;
     try {
         return f();
     } catch (const std::exception& e) {
@@ -924,6 +925,7 @@ int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_bat
             sched[c].tp_pass = d.sched[c].tp_pass;
             sched[c].horner_cluster = d.sched[c].horner_cluster;
             sched[c].tp_sms = d.sched[c].tp_sms;
+            sched[c].slice = d.sched[c].slice;
         }
     return 0;
 }
@@ -977,6 +979,7 @@ size_t ipir_serve_trace(ipir_serve* sv, ipir_serve_batch_record* out, size_t max
 
 void ipir_serve_destroy(ipir_serve* sv) {
     if (!sv) return;
+    ipb::DeviceRestore keep_device;  // the engine's destructor switches to its device
     ipb::Engine* E = sv->e;
     {
         std::lock_guard<std::mutex> lk(E->mu);

@@ -255,6 +255,7 @@ Server* make_server(const Params& pp, std::shared_ptr<Precomp> pre, size_t max_b
     const int gt_pass = lane_gt_pass(*S, max_batch);
     S->sched = default_sched(*S, max_batch, gt_pass);
     alloc_lane(*S, S->lane, max_batch, gt_pass);
+    S->ev.assign(6 * ((max_batch + kSliceQueries - 1) / kSliceQueries), nullptr);
     for (auto& e : S->ev) IPB_CK(cudaEventCreate(&e));
     pre->adopted = true;
     S->resident_bytes = pre->arena.bytes + S->lane.arena.bytes;
@@ -366,15 +367,25 @@ std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
 // key parts (copied on another stream, this event marks them); the key side
 // (query prep, tensor pass) then runs first and the mat-vec after the event.
 // The RGSW parts are then prepared on that other stream as well.
-static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
-                        cudaEvent_t lwe_ready = nullptr) {
+// q_off: the batch's first lane slot (slices of a batch larger than one DB
+// pass run the whole phase on slots [q_off, q_off + count)); the tensor-pass
+// rows (tp_out) and key table are shared by slices run one after the other.
+// qprep_parts: 3 prepares keys and RGSW parts here, 1 the keys only (the
+// RGSW parts are prepared elsewhere).
+static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t q_off, size_t count, cudaStream_t st,
+                        cudaEvent_t* ev, cudaEvent_t lwe_ready = nullptr, int qprep_parts = 3) {
     const Params& pp = S.pp;
     const Precomp& P = *S.pre;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
     const int nq = (int)count;
+    uint64_t* const qraw = L.qraw + q_off * S.qstride;
+    uint32_t* const keys = L.keys + q_off * kKeyStride;
+    uint32_t* const mvpart = L.mvpart + q_off * S.mv_qstride;
+    uint8_t* const planes = L.planes + mv_tc_planes_offset(q_off, R);
     int launches = 0;
     if (ev) IPB_CK(cudaEventRecord(ev[0], st));
-    IPB_CK(launch_qprep_parts(L.qraw, S.qstride, R, P.tables, L.keys, L.rgsw32, nq, lwe_ready ? 1 : 3, st));
+    IPB_CK(launch_qprep_parts(qraw, S.qstride, R, P.tables, keys, L.rgsw32 + q_off * kRgswStride, nq, qprep_parts,
+                              st));
     ++launches;
     if (ev) IPB_CK(cudaEventRecord(ev[1], st));
     // Beside: the tensor pass (keys only) on sc.tp_sms SMs from the lane's
@@ -384,7 +395,7 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
     auto tensor_pass = [&](cudaStream_t ts, int sms) {
         for (size_t c0 = 0; c0 < count; c0 += (size_t)sc.tp_pass) {
             const int n = (int)std::min<size_t>((size_t)sc.tp_pass, count - c0);
-            IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.keyt,
+            IPB_CK(launch_tensor_pass(P.pre_dt, G, keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.keyt,
                                       L.tp_out, L.d_err, L.tiles + 1, sms, ts));
             launches += 2;  // key table + GEMM
         }
@@ -401,21 +412,21 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
     }
     int mv_parts;
     if (sc.matvec_tc) {
-        IPB_CK(launch_qplanes(L.qraw, S.qstride, R, P.tables, L.planes, nq, st));
+        IPB_CK(launch_qplanes(qraw, S.qstride, R, P.tables, planes, nq, st));
         ++launches;
         for (size_t c0 = 0; c0 < count; c0 += 32) {
             const int n = (int)std::min<size_t>(32, count - c0);
-            IPB_CK(launch_matvec_tc(P.db, R, C, L.planes + mv_tc_planes_offset(c0, R), n, P.tables, L.mvpart + c0 * S.mv_qstride,
-                                    S.mv_qstride, L.d_err, L.tiles, beside ? S.num_sms - sc.tp_sms : S.num_sms,
-                                    S.tc_kchunk_rows, st));
+            IPB_CK(launch_matvec_tc(P.db, R, C, planes + mv_tc_planes_offset(c0, R), n, P.tables,
+                                    mvpart + c0 * S.mv_qstride, S.mv_qstride, L.d_err, L.tiles,
+                                    beside ? S.num_sms - sc.tp_sms : S.num_sms, S.tc_kchunk_rows, st));
             ++launches;
         }
         mv_parts = S.tc_kchunks;
     } else {
         for (size_t c0 = 0; c0 < count; c0 += 4) {
             const int n = (int)std::min<size_t>(4, count - c0);
-            IPB_CK(launch_matvec(P.db, R, C, S.mv_chunks, L.qraw + c0 * S.qstride, S.qstride, P.tables,
-                                 L.mvpart + c0 * S.mv_qstride, S.mv_qstride, n, st));
+            IPB_CK(launch_matvec(P.db, R, C, S.mv_chunks, qraw + c0 * S.qstride, S.qstride, P.tables,
+                                 mvpart + c0 * S.mv_qstride, S.mv_qstride, n, st));
             ++launches;
         }
         mv_parts = S.mv_chunks;
@@ -425,15 +436,16 @@ static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t count,
     if (ev) IPB_CK(cudaEventRecord(ev[2], st));
     if (!beside && !lwe_ready) tensor_pass(st, S.num_sms);
     if (ev) IPB_CK(cudaEventRecord(ev[3], st));
-    IPB_CK(launch_finalize(L.mvpart, S.mv_qstride, mv_parts, C, L.tp_out, P.pre_df, L.keys, kKeyStride, P.tables,
-                           L.packed_b, S.pb_qstride, G, nq, st));
+    IPB_CK(launch_finalize(mvpart, S.mv_qstride, mv_parts, C, L.tp_out, P.pre_df, keys, kKeyStride, P.tables,
+                           L.packed_b + q_off * S.pb_qstride, S.pb_qstride, G, nq, st));
     return launches + 1;
 }
 
-static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st,
+static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t q_off, size_t count, cudaStream_t st,
                             cudaEvent_t* ev) {
     if (ev) IPB_CK(cudaEventRecord(ev[4], st));
-    enqueue_horner(S, sc, L.packed_b, L.rgsw32, L.resp, count, L.d_err, st);
+    enqueue_horner(S, sc, L.packed_b + q_off * S.pb_qstride, L.rgsw32 + q_off * kRgswStride,
+                   L.resp + q_off * S.resp_qstride, count, L.d_err, st);
     if (ev) IPB_CK(cudaEventRecord(ev[5], st));
     return 1;
 }
@@ -502,21 +514,38 @@ void enqueue_scan_finalize(const Server& S, Lane& L, const SlotRun& r, cudaStrea
 }
 
 int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
-                 int phases) {
+                 int phases, size_t n_ev) {
     if (count == 0) return 0;
     if (count > L.cap || sc.tp_pass < 1 || sc.tp_pass > L.gt_pass)
         throw std::invalid_argument("run_pipeline: batch exceeds the lane or its tensor-pass buffer");
-    if (phases != kPhaseAll) ev = nullptr;
+    const size_t ns = slices_of(count, sc), slice = sc.slice > 0 ? (size_t)sc.slice : count;
+    if (phases != kPhaseAll || 6 * ns > n_ev) ev = nullptr;
     int launches = 0;
-    if (phases & kPhaseDb) launches += run_db_phase(S, L, sc, count, st, ev);
-    if (phases & kPhaseHorner) launches += run_horner_phase(S, L, sc, count, st, ev);
+    // Slices run one after the other, each its own pipeline on its lane
+    // slots: the DB and the tensors are read once per slice either way (one
+    // mat-vec pass serves at most 32 queries), and a slice's Horner chains fit
+    // the SMs in one wave.
+    if (phases & kPhaseDb)
+        for (size_t k = 0; k < ns; ++k) {
+            const size_t q0 = k * slice;
+            launches += run_db_phase(S, L, sc, q0, std::min(slice, count - q0), st, ev ? ev + 6 * k : nullptr);
+            if ((phases & kPhaseHorner) && ns > 1)
+                launches += run_horner_phase(S, L, sc, q0, std::min(slice, count - q0), st, ev ? ev + 6 * k : nullptr);
+        }
+    if ((phases & kPhaseHorner) && !((phases & kPhaseDb) && ns > 1))
+        for (size_t k = 0; k < ns; ++k) {
+            const size_t q0 = k * slice;
+            launches += run_horner_phase(S, L, sc, q0, std::min(slice, count - q0), st, ev ? ev + 6 * k : nullptr);
+        }
     return launches;
 }
 
 static void run_pipeline(Server* S, size_t count) {
     IPB_CK(cudaSetDevice(S->device));
-    S->launches += (unsigned long long)run_pipeline(*S, S->lane, sched_for(*S, count), count, S->stream,
-                                                    S->timing ? S->ev : nullptr);
+    const Sched& sc = sched_for(*S, count);
+    S->timed_slices = S->timing ? slices_of(count, sc) : 0;
+    S->launches += (unsigned long long)run_pipeline(*S, S->lane, sc, count, S->stream,
+                                                    S->timing ? S->ev.data() : nullptr, kPhaseAll, S->ev.size());
 }
 
 // The blocking answer from host views: the KSK parts are copied first and
@@ -530,7 +559,9 @@ static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
     const Sched& sc = sched_for(*S, count);
     if (sc.tp_sms > 0 || S->timing) {
         stage_queries(S, qs, count);
-        S->launches += (unsigned long long)run_pipeline(*S, S->lane, sc, count, S->stream, S->timing ? S->ev : nullptr);
+        S->timed_slices = S->timing ? slices_of(count, sc) : 0;
+        S->launches += (unsigned long long)run_pipeline(*S, S->lane, sc, count, S->stream,
+                                                        S->timing ? S->ev.data() : nullptr, kPhaseAll, S->ev.size());
         return;
     }
     Lane& L = S->lane;
@@ -544,9 +575,17 @@ static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
                               L.aux));
     IPB_CK(cudaEventRecord(L.rgsw_ready, L.aux));
     S->staged = count;
-    S->launches += 1 + (unsigned long long)run_db_phase(*S, L, sc, count, S->stream, nullptr, L.join);
-    IPB_CK(cudaStreamWaitEvent(S->stream, L.rgsw_ready, 0));
-    S->launches += (unsigned long long)run_horner_phase(*S, L, sc, count, S->stream, nullptr);
+    S->launches += 1;
+    // The first slice's key side starts before the LWE vectors land; every
+    // slice's RGSW parts were prepared on the second stream above.
+    const size_t ns = slices_of(count, sc), slice = sc.slice > 0 ? (size_t)sc.slice : count;
+    for (size_t k = 0; k < ns; ++k) {
+        const size_t q0 = k * slice, n = std::min(slice, count - q0);
+        S->launches += (unsigned long long)run_db_phase(*S, L, sc, q0, n, S->stream, nullptr,
+                                                        k == 0 ? L.join : nullptr, 1);
+        if (k == 0) IPB_CK(cudaStreamWaitEvent(S->stream, L.rgsw_ready, 0));
+        S->launches += (unsigned long long)run_horner_phase(*S, L, sc, q0, n, S->stream, nullptr);
+    }
 }
 
 // A kernel whose pipeline wait ran out of iterations leaves a code in the
@@ -565,8 +604,15 @@ static void fetch(Server* S, size_t count, uint64_t* out) {
     IPB_CK(cudaMemcpyAsync(out, S->lane.resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, S->stream));
     IPB_CK(cudaStreamSynchronize(S->stream));
     check_device_error(S->lane);
-    if (S->timing)
-        for (int i = 0; i < 5; ++i) IPB_CK(cudaEventElapsedTime(&S->stage_ms[i], S->ev[i], S->ev[i + 1]));
+    if (S->timing && S->timed_slices)  // stage times summed over the batch's slices
+        for (int i = 0; i < 5; ++i) {
+            S->stage_ms[i] = 0.f;
+            for (size_t k = 0; k < S->timed_slices; ++k) {
+                float t = 0.f;
+                IPB_CK(cudaEventElapsedTime(&t, S->ev[6 * k + i], S->ev[6 * k + i + 1]));
+                S->stage_ms[i] += t;
+            }
+        }
 }
 
 // ------------------------------------------------------------ schedule autotuner
@@ -579,7 +625,9 @@ static void fetch(Server* S, size_t count, uint64_t* out) {
 // cluster, 8-CTA cluster, single CTA) -- and keep the fastest; then, for the
 // tensor-core mat-vec, the number of SMs (1/18 .. 8/18 of them) that run the
 // tensor pass at the same time as the mat-vec, if that is faster still.
-// Sizes between two measured ones use the smaller's.
+// Batches larger than 32 queries also try one pipeline for the whole batch
+// against consecutive 32-query slices.  Sizes between two measured ones use
+// the smaller's.
 std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
     IPB_CK(cudaSetDevice(S.device));
     std::vector<size_t> sizes;
@@ -599,6 +647,14 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
                 for (int p : passes)
                     for (int h : {1, 2, 0}) cands.push_back(Sched{mv, p, h});
             }
+            // Batches larger than one slice: also the whole batch in one
+            // pipeline (one query prep, finalize and Horner launch for all).
+            if (b > kSliceQueries)
+                for (size_t i = 0, n = cands.size(); i < n; ++i) {
+                    Sched w = cands[i];
+                    w.slice = 0;
+                    cands.push_back(w);
+                }
             auto time_of = [&](const Sched& c) {
                 run_pipeline(S, L, c, b, st, nullptr);  // warm
                 float ms = 1e30f;
@@ -800,6 +856,7 @@ GpuServerCtx* gpu_setup_server(const PublicParams& pp, const PreprocessData& pre
     // Ownership of the device buffers moves to the context, as in the
     // reference (src/gpu_protocol.cu:856-885).
     std::shared_ptr<ipb::Precomp> p = std::move(precomp.state->p);
+    ipb::DeviceRestore keep_device;
     auto* ctx = new GpuServerCtx{ipb::make_server(to_ipb(pp), std::move(p), cfg.max_batch)};
     return ctx;
 }
@@ -811,6 +868,7 @@ GpuServerCaps gpu_server_caps(const GpuServerCtx* ctx) {
     c.resident_bytes = ctx->s->resident_bytes;
     c.num_cts = ctx->s->pp.num_cts;
     size_t fr = 0, tot = 0;
+    ipb::DeviceRestore keep_device;
     cudaSetDevice(ctx->s->device);
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) c.device_free_bytes = fr;
     return c;
@@ -822,6 +880,7 @@ void gpu_answer_batch(GpuServerCtx* ctx, const ipir_query_view* queries, size_t 
     if (rc == 2) throw std::invalid_argument("gpu_answer_batch: count exceeds max_batch");
     if (rc) throw std::invalid_argument("gpu_answer_batch: null argument");
     if (count == 0) return;
+    ipb::DeviceRestore keep_device;
     ipb::stage_and_run(ctx->s, queries, count);
     ipb::fetch(ctx->s, count, out);
 }
@@ -830,6 +889,7 @@ void gpu_answer(GpuServerCtx* ctx, const ipir_query_view& q, uint64_t* out) { gp
 
 void gpu_free_server(GpuServerCtx* ctx) {
     if (!ctx) return;
+    ipb::DeviceRestore keep_device;
     delete ctx->s;
     delete ctx;
 }
@@ -841,6 +901,7 @@ void gpu_free_server(GpuServerCtx* ctx) {
 namespace {
 template <class F>
 int guarded(F&& f, int fail_code) {
+    ipb::DeviceRestore keep_device;
     try {
         return f();
     } catch (const std::exception& e) {
@@ -940,6 +1001,7 @@ int ipir_answer_batch(ipir_server* srv, const ipir_query_view* queries, size_t c
 
 void ipir_server_destroy(ipir_server* srv) {
     if (!srv) return;
+    ipb::DeviceRestore keep_device;
     delete srv->s;
     delete srv;
 }
@@ -1025,6 +1087,7 @@ int ipir_b200_get_schedule(const ipir_server* srv, size_t count, ipir_serve_sche
     out->tp_pass = sc.tp_pass;
     out->horner_cluster = sc.horner_cluster;
     out->tp_sms = sc.tp_sms;
+    out->slice = sc.slice;
     return 0;
 }
 
@@ -1034,13 +1097,13 @@ int ipir_b200_set_schedule(ipir_server* srv, size_t count, const ipir_serve_sche
     if (count == 0 || count > S->max_batch) return 2;
     if (sc->matvec_tc < 0 || sc->matvec_tc > 1 || sc->horner_cluster < 0 || sc->horner_cluster > 2 ||
         sc->tp_pass < 1 || sc->tp_pass > S->lane.gt_pass || sc->tp_sms < 0 || sc->tp_sms >= S->num_sms ||
-        (sc->tp_sms > 0 && !sc->matvec_tc)) {
+        (sc->tp_sms > 0 && !sc->matvec_tc) || (sc->slice != 0 && sc->slice != (int)ipb::kSliceQueries)) {
         ipb::g_last_error =
             "ipir_b200_set_schedule: matvec_tc 0/1, horner_cluster 0/1/2, tp_pass 1..capacity, "
-            "tp_sms 0..SMs-1 (0 with the CUDA-core mat-vec)";
+            "tp_sms 0..SMs-1 (0 with the CUDA-core mat-vec), slice 0/32";
         return 2;
     }
-    S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster, sc->tp_sms};
+    S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster, sc->tp_sms, sc->slice};
     return 0;
 }
 

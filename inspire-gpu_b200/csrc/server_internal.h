@@ -32,6 +32,22 @@ struct CudaFailure : std::runtime_error {
         if (e_ != cudaSuccess) ::ipb::cuda_fail(e_, #call, __FILE__, __LINE__); \
     } while (0)
 
+// Puts the calling thread's current device back on scope exit.  Entry points
+// switch to their handle's device; a caller in a multi-GPU process keeps the
+// device it had chosen, on error paths too.
+struct DeviceRestore {
+    int dev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    }
+    ~DeviceRestore() {
+        int cur = -1;
+        if (dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev) cudaSetDevice(dev);
+    }
+    DeviceRestore(const DeviceRestore&) = delete;
+    DeviceRestore& operator=(const DeviceRestore&) = delete;
+};
+
 // Device allocations freed together.
 struct DevArena {
     std::vector<void*> ptrs;
@@ -88,7 +104,17 @@ struct Sched {
     int horner_cluster = 1;  // 1: 4-CTA cluster per chain, 2: 8-CTA cluster, 0: one CTA per chain
     int tp_sms = 0;          // > 0: tensor pass on this many SMs beside the tcgen05 mat-vec on the
                              // others (the lane's second stream); 0: tensor pass after the mat-vec
+    int slice = 32;          // > 0: a batch larger than this runs as consecutive slices of this many
+                             // queries, each its own pipeline (query prep .. Horner) on the lane's slots;
+                             // 0: the whole batch in one pipeline
 };
+
+// Queries per slice a batch is cut into (one DB pass of the tensor-core
+// mat-vec serves at most this many) and the slices a batch of c needs.
+constexpr size_t kSliceQueries = 32;
+inline size_t slices_of(size_t c, const Sched& sc) {
+    return sc.slice > 0 ? (c + (size_t)sc.slice - 1) / (size_t)sc.slice : 1;
+}
 
 // Per-batch device scratch for up to `cap` queries.
 struct Lane {
@@ -140,7 +166,8 @@ struct Server {
     bool tuned = false;
     size_t staged = 0;
     bool timing = false;
-    cudaEvent_t ev[6] = {};
+    std::vector<cudaEvent_t> ev;  // 6 stage events per slice of the largest batch
+    size_t timed_slices = 0;      // slices of the last batch run with stage timing
     float stage_ms[5] = {};
     size_t resident_bytes = 0;
     unsigned long long launches = 0;  // kernels launched through this handle's pipeline
@@ -163,8 +190,10 @@ constexpr int kPhaseDb = 1, kPhaseHorner = 2, kPhaseAll = 3;
 // Enqueues the answer pipeline (the given phases) for `count` staged
 // queries of lane L on stream st; returns the number of kernels launched.
 // ev (6 stage events, used when all phases run) or null.
+// ev holds n_ev events: 6 per slice (fewer than the batch's slices need: no
+// stage events are recorded).
 int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
-                 int phases = kPhaseAll);
+                 int phases = kPhaseAll, size_t n_ev = 6);
 // H2D of one flat query into query slot i of lane L.
 void stage_query_flat(const Server& S, Lane& L, size_t i, const uint64_t* flat, cudaStream_t st);
 // Schedule table (index = batch size, 0 unused) for a lane of `cap` queries

@@ -94,7 +94,8 @@ _L.ipir_b200_matvec_noalloc.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_
 
 
 class IpirSchedule(C.Structure):
-    _fields_ = [("matvec_tc", C.c_int), ("tp_pass", C.c_int), ("horner_cluster", C.c_int), ("tp_sms", C.c_int)]
+    _fields_ = [("matvec_tc", C.c_int), ("tp_pass", C.c_int), ("horner_cluster", C.c_int), ("tp_sms", C.c_int),
+                ("slice", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -119,6 +120,8 @@ class IpirMatvecOpts(C.Structure):
 _L.ipir_b200_matvec_ex.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                    C.c_void_p, C.c_int, C.POINTER(IpirMatvecOpts)]
 _L.ipir_b200_fill_db_device.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, C.c_void_p]
+_L.ipir_b200_kernel_binary_version.argtypes = [C.POINTER(C.c_int)]
+_L.ipir_b200_kernel_binary_version.restype = C.c_int
 _L.ipir_b200_autotune.argtypes = [C.c_void_p]
 _L.ipir_b200_get_schedule.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(IpirSchedule)]
 _L.ipir_b200_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_ulonglong)]
@@ -164,6 +167,7 @@ EXPORTED = [
     "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy", "ipir_b200_matvec_ex",
     "ipir_b200_fill_db_device", "ipir_b200_set_schedule", "ipir_b200_wire_sizes", "ipir_b200_answer_wire",
     "ipir_serve_replace_db", "ipir_b200_save_server", "ipir_b200_load_server",
+    "ipir_b200_kernel_binary_version",
 ]
 
 
@@ -410,12 +414,13 @@ class Server:
             raise InspireError(f"get_schedule rc={rc}")
         return s.as_dict()
 
-    def set_schedule(self, count, matvec_tc=1, tp_pass=None, horner_cluster=1, tp_sms=0):
+    def set_schedule(self, count, matvec_tc=1, tp_pass=None, horner_cluster=1, tp_sms=0, slice=32):
         """Pin the kernel schedule for batches of `count` queries (tp_sms > 0:
-        tensor pass on that many SMs beside the mat-vec)."""
+        tensor pass on that many SMs beside the mat-vec; slice 32: batches of
+        more than 32 run as consecutive 32-query pipelines, 0: one pipeline)."""
         self._check()
         s = IpirSchedule(matvec_tc, tp_pass if tp_pass is not None else self.schedule(count)["tp_pass"],
-                         horner_cluster, tp_sms)
+                         horner_cluster, tp_sms, slice)
         rc = _L.ipir_b200_set_schedule(self._h, count, C.byref(s))
         if rc:
             raise InspireError(f"set_schedule rc={rc}: {last_error()}")
@@ -611,6 +616,16 @@ def fill_db_device(ptr, count, seed, stream=0):
     rc = _L.ipir_b200_fill_db_device(C.c_void_p(ptr), count, seed, C.c_void_p(stream or 0))
     if rc:
         raise InspireError(f"fill_db_device rc={rc}: {last_error()}")
+
+
+def kernel_binary_version():
+    """cudaFuncAttributes.binaryVersion of the library's kernels as loaded
+    (100 for sm_100a)."""
+    v = C.c_int(0)
+    rc = _L.ipir_b200_kernel_binary_version(C.byref(v))
+    if rc:
+        raise InspireError(f"ipir_b200_kernel_binary_version rc={rc}: {last_error()}")
+    return v.value
 
 
 def matvec_noalloc_rc(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0):

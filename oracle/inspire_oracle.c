@@ -730,6 +730,13 @@ void orc_fill_db(uint16_t* db, size_t count, uint64_t seed) {
     for (size_t k = 0; k < count; k++) db[k] = (uint16_t)(splitmix64(seed ^ k) % ORC_P);
 }
 
+/* Synthetic residues: p[k] = splitmix64(seed ^ k) mod q (q < 2^32), for
+ * precomputed tensors whose values the timed CPU path does not depend on. */
+void orc_fill_u32_mod(uint32_t* p, size_t count, uint64_t seed, uint32_t q) {
+#pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < count; k++) p[k] = (uint32_t)(splitmix64(seed ^ k) % q);
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -70,6 +70,7 @@ class Oracle:
                                  u64p, u64p]
         L.orc_answer.restype = C.c_int
         L.orc_fill_db.argtypes = [u16p, C.c_size_t, C.c_uint64]
+        L.orc_fill_u32_mod.argtypes = [u32p, C.c_size_t, C.c_uint64, C.c_uint32]
         L.orc_num_threads.restype = C.c_int
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_init()
@@ -112,6 +113,11 @@ class Oracle:
         db = np.empty(count, np.uint16)
         self.L.orc_fill_db(ptr(db, u16p), count, seed)
         return db
+
+    def fill_u32_mod(self, count, seed, q):
+        out = np.empty(count, np.uint32)
+        self.L.orc_fill_u32_mod(ptr(out, u32p), count, seed, q)
+        return out
 
     def preprocess(self, seed, db, rows, cols, D, group_lo=0, group_hi=None, encode=True):
         G = cols // N

@@ -144,3 +144,34 @@ def test_views_contiguous_or_scattered(batch_env):
     out2 = np.zeros((n, rn), np.uint64)
     assert srv.answer_batch_rc(scattered, n, out2) == 0
     assert (out2 == want).all()
+
+
+def test_batches_beyond_one_slice(batch_env):
+    """Batches of more than 32 queries run as consecutive 32-query slices
+    (slice = 32) or as one pipeline (slice = 0); both, through the blocking
+    answer, the staged path with stage timing, and the tensor pass beside
+    the mat-vec, give every query's single answer (70 = 32 + 32 + 6 and
+    40 = 32 + 8 queries, each of the 10 module queries repeated)."""
+    import inspire_b200 as ib
+    c, srv1, qs, sts = batch_env
+    singles = np.stack([srv1.answer(q) for q in qs])
+    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=70, crs_seed=c.seed)
+    try:
+        for n in (70, 40):
+            batch = [qs[k % len(qs)] for k in range(n)]
+            want = np.stack([singles[k % len(qs)] for k in range(n)])
+            for sl in (32, 0):
+                srv.set_schedule(n, matvec_tc=1, horner_cluster=1, slice=sl)
+                assert srv.schedule(n)["slice"] == sl
+                assert (srv.answer_batch(batch) == want).all(), (n, sl)
+                srv.enable_stage_timing(True)
+                assert (srv.answer_batch(batch) == want).all(), (n, sl, "timed")
+                st = srv.stage_times()
+                srv.enable_stage_timing(False)
+                assert all(v > 0 for v in st.values()), st
+                srv.set_schedule(n, matvec_tc=1, horner_cluster=1, tp_sms=40, slice=sl)
+                assert (srv.answer_batch(batch) == want).all(), (n, sl, "beside")
+        with pytest.raises(Exception):
+            srv.set_schedule(40, matvec_tc=1, horner_cluster=1, slice=16)
+    finally:
+        srv.close()

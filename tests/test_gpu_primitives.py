@@ -61,3 +61,9 @@ def test_decomp_matches_reference(ref):
     got = ib.decomp(f).reshape(n, 2 * 2 * N)
     for i in range(n):
         assert (got[i].astype(np.uint64) == ref.decomp(f[i].reshape(-1).astype(np.uint64))).all(), i
+
+
+def test_kernels_loaded_as_sm100():
+    """The CUDA runtime loaded the library's sm_100a cubin (binaryVersion 100)."""
+    import inspire_b200 as ib
+    assert ib.kernel_binary_version() == 100
