@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
     __shared__ volatile int abort_flag;
     __shared__ volatile int item_ring[kRing];
     __shared__ uint64_t ifull[kRing], iempty[kRing];
+    __shared__ uint64_t mma_done;  // the MMA issuer's final commit: all its MMAs have completed
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
         for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128); }
         for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 128); }
+        mbar_init(&mma_done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
         if (lane == 0) {
             int s = 0;
             uint32_t ph = 0;
+            unsigned issued = 0;  // stage loads issued
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
                 int item = -1;
@@ -137,13 +140,17 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                     tma_load_2d(st, &map_a, &full[s], m0, k0);
                     tma_load_2d(st + a_bytes, &map_a, &full[s], m0 + 128, k0);
                     tma_load_2d(st + 2 * a_bytes, &map_b, &full[s], k0, 0);
+                    ++issued;
                     if (++s == S) { s = 0; ph ^= 1; }
                 }
             }
-            // drain: every issued stage must be consumed before the CTA exits
-            for (int i = 0; i < S; ++i) {
-                mbar_wait(&empty[s], ph ^ 1, P.err, 2);
-                if (++s == S) { s = 0; ph ^= 1; }
+            // Drain: every issued load has landed in shared memory before the
+            // CTA exits, also when the MMA issuer stopped early (a timeout) and
+            // never consumed them.  Load n went to stage n % S with phase
+            // (n / S) & 1; no later load reuses a stage, so each wait is exact.
+            for (unsigned i = 0; i < (unsigned)S && i < issued; ++i) {
+                const unsigned n = issued - 1 - i;
+                mbar_wait(&full[n % S], (n / S) & 1u, P.err, 2);
             }
         }
     } else if (warp == 1) {
@@ -152,6 +159,7 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
             const uint32_t idesc = idesc_i8(P.npad);
             int s = 0, as = 0;
             uint32_t ph = 0, aph = 0;
+            bool it_mma = false;  // any MMA issued
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
                 if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 7)) { abort_flag = 1; break; }
@@ -177,11 +185,18 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                         mma_i8(d0, a0, b, idesc, acc);
                         mma_i8(d0 + (uint32_t)P.npad, a1, b, idesc, acc);
                     }
+                    it_mma = true;
                     mma_commit(&empty[s]);
                     if (++s == S) { s = 0; ph ^= 1; }
                 }
                 mma_commit(&tfull[as]);
                 if (++as == P.acc_stages) { as = 0; aph ^= 1; }
+            }
+            // Every MMA this thread issued has completed (also after an early
+            // stop) before TMEM is deallocated and shared memory released.
+            if (it_mma) {
+                mma_commit(&mma_done);
+                mbar_wait(&mma_done, 0, P.err, 9);
             }
         }
     } else if (warp >= 4) {

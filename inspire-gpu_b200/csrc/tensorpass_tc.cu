@@ -206,14 +206,16 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
     const uint32_t stage_bytes = a_region + b_bytes;
     const uint32_t tx_bytes = (uint32_t)P.mti * P.rows_box * 128;  // A only; B is written by the key warps
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
-    uint64_t* full = bars;
+    uint64_t* full = bars;               // the stage's A tiles have landed (TMA bytes)
     uint64_t* empty = bars + S;
     uint64_t* tfull = bars + 2 * S;
     uint64_t* tempty = bars + 2 * S + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 4);
+    uint64_t* bfull = bars + 2 * S + 4;  // the stage's B tile is written (the key group's arrivals)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * S + 4);
     __shared__ volatile int abort_flag;
     __shared__ volatile int item_ring[kRing];
     __shared__ uint64_t ifull[kRing], iempty[kRing];
+    __shared__ uint64_t mma_done;  // the MMA issuer's final commit: all its MMAs have completed
     // tw[w] for w = dir * 1023 + s: t = 5^(1022 - s), or 2N - t when dir = 1;
     // the two w of a 4-u group are one aligned 64-bit read.
     __shared__ __align__(8) uint32_t tw[2 * kSteps + 2];
@@ -230,8 +232,15 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
     }
     if (threadIdx.x == 0) {
         abort_flag = 0;
-        // full: the producer's expect_tx arrival (A bytes) + the key group of the stage
-        for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1 + kKeyGroup); mbar_init(&empty[s], 1); }
+        // full: the producer's expect_tx arrival (A bytes); bfull: the key
+        // group of the stage.  Kept apart so that the producer can wait for
+        // its own loads alone before the CTA exits.
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&bfull[s], kKeyGroup);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&mma_done, 1);
         // tempty: 128 epilogue threads per share (warps 4..7 and each key
         // group that fills no stages)
         const int shares = 1 + kKeyGroups - (S < kKeyGroups ? S : kKeyGroups);
@@ -323,6 +332,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
         if (lane == 0) {
             int s = 0;
             uint32_t ph = 0;
+            unsigned issued = 0;  // stage loads issued
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
                 int item = -1;
@@ -343,12 +353,17 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                     mbar_expect_tx(&full[s], tx_bytes);
                     for (int mt = 0; mt < P.mti; ++mt)
                         tma_load_2d(st + mt * a_tile, &map_a, &full[s], kt * 128, rowa + mt * 128);
+                    ++issued;
                     if (++s == S) { s = 0; ph ^= 1; }
                 }
             }
-            for (int i = 0; i < S; ++i) {
-                mbar_wait(&empty[s], ph ^ 1, P.err, 12);
-                if (++s == S) { s = 0; ph ^= 1; }
+            // Drain: every issued load has landed before the CTA exits, also
+            // when the MMA issuer stopped early and never consumed them.  Load n
+            // went to stage n % S with phase (n / S) & 1; no later load reuses
+            // a stage, so each wait is exact.
+            for (unsigned i = 0; i < (unsigned)S && i < issued; ++i) {
+                const unsigned n = issued - 1 - i;
+                mbar_wait(&full[n % S], (n / S) & 1u, P.err, 12);
             }
         }
     } else if (warp == 1) {
@@ -359,6 +374,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
             const uint32_t idesc = idesc_i8_kk(P.nb);
             int s = 0, as = 0;
             uint32_t ph = 0, aph = 0;
+            bool any_mma = false;
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
                 if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 17)) { abort_flag = 1; break; }
@@ -369,7 +385,10 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                 tc_fence_after();
                 const uint32_t d0 = tmem_base + (uint32_t)(as * acc_cols);
                 for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&full[s], ph, P.err, 14)) { abort_flag = 1; break; }
+                    if (!mbar_wait(&full[s], ph, P.err, 14) || !mbar_wait(&bfull[s], ph, P.err, 21)) {
+                        abort_flag = 1;
+                        break;
+                    }
                     tc_fence_after();
                     const uint8_t* st = smem + (size_t)s * stage_bytes;
                     const uint8_t* bt = st + a_region;
@@ -387,10 +406,17 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                         }
                     }
                     mma_commit(&empty[s]);
+                    any_mma = true;
                     if (++s == S) { s = 0; ph ^= 1; }
                 }
                 mma_commit(&tfull[as]);
                 if (++as == P.acc_stages) { as = 0; aph ^= 1; }
+            }
+            // Every MMA this thread issued has completed (also after an early
+            // stop) before TMEM is deallocated and shared memory released.
+            if (any_mma) {
+                mma_commit(&mma_done);
+                mbar_wait(&mma_done, 0, P.err, 22);
             }
         }
     } else if (warp >= 8) {
@@ -468,7 +494,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                     }
                     // generic-proxy stores -> visible to the tensor core's async proxy
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    mbar_arrive(&full[s]);
+                    mbar_arrive(&bfull[s]);
                 }
             }
         }
@@ -619,7 +645,7 @@ cudaError_t launch_tensor_pass_slots(const uint8_t* Dt, size_t G, int li0, int n
     if (P.stages < 2) return cudaErrorInvalidValue;
     CUtensorMap ma;
     if (!make_map(&ma, Dt, (uint64_t)2 * kN * 4 * G, (uint32_t)P.rows_box)) return cudaErrorInvalidValue;
-    const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
+    const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (3 * P.stages + 4) * 8 + 16;
     const int items = (n_li / P.spi) * P.n_mg;
     if ((e = cudaMemsetAsync(tiles, 0, sizeof(unsigned), s))) return e;
     tp_tc_kernel<<<std::min(items, std::max(1, num_sms)), kTpThreads, smem, s>>>(ma, P);
