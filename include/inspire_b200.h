@@ -11,7 +11,8 @@
  * does not have: explicit streams, a device-resident staged pipeline, stage
  * timers, precomp export, schedule autotuning, and the GPU primitives for
  * parity checks.  Part 3 (prefix ipir_serve_) is the continuous-batching
- * serving loop.
+ * serving loop.  Part 4 splits one database over several GPUs by group
+ * ranges (shards and a Horner owner).
  *
  * Values are residues mod the two 27-bit primes q0 = 94519297 and
  * q1 = 95293441 carried in u64 (u32 for GPU-side primitives).  One server
@@ -379,6 +380,52 @@ size_t ipir_serve_trace(ipir_serve* sv, ipir_serve_batch_record* out, size_t max
 /* Waits for the batches on the device, fails requests not yet admitted,
  * frees everything. */
 void ipir_serve_destroy(ipir_serve* sv);
+
+/* ===================================================== part 4: group shards
+ * One database split over several GPUs by contiguous group ranges (no
+ * counterpart in the reference, which runs on one GPU: docs/ARCHITECTURE.md:32).
+ * Each GPU holds a shard: its column slab of the encoded DB and its groups'
+ * tensors; per batch it computes the b parts of its groups' packed
+ * ciphertexts.  The caller gathers them (one collective, 2 N u32 per group
+ * and query) to one GPU, whose Horner owner runs the chains.  The responses
+ * equal ipir_answer_batch's on the whole database. */
+typedef struct ipir_shard ipir_shard;
+typedef struct ipir_horner ipir_horner;
+
+/* Preprocesses groups [group_lo, group_hi) of the database
+ * setup(n_entries, entry_bytes, db_rows_or_zero) on the current device; db is
+ * the whole host DB (the encode mixes columns of several groups per row, so
+ * it runs over full rows, chunk by chunk, and keeps the slab), crs_seed the
+ * 64-byte CRS seed every shard shares (required).  out_params receives the
+ * whole database's parameters.  NULL on failure (ipir_b200_last_error()). */
+ipir_shard* ipir_b200_shard_create(size_t n_entries, size_t entry_bytes, size_t db_rows_or_zero, size_t max_batch,
+                                   const uint16_t* db, const uint8_t* crs_seed, size_t group_lo, size_t group_hi,
+                                   ipir_params* out_params);
+/* The a parts of the shard's groups, host out[(group_hi - group_lo) * 2 * N]
+ * u32 ([group][limb][coeff], NTT form), for the Horner owner's set-up. */
+int ipir_b200_shard_export_a(const ipir_shard* shard, uint32_t* out);
+/* The shard's part of a batch: mat-vec over its slab, tensor pass and
+ * finalize of its groups for count <= max_batch queries (their LWE and KSK
+ * parts are read, not their RGSW parts); writes the DEVICE buffer
+ * out_packed_b[count][group_hi - group_lo][limb][N] u32 (b parts, NTT form).
+ * Blocking.  Returns 0, 1 null argument, 2 count > max_batch, 3 null view
+ * field, 4 CUDA error or device wait timeout. */
+int ipir_b200_shard_pack(ipir_shard* shard, const ipir_query_view* queries, size_t count, uint32_t* out_packed_b);
+void ipir_b200_shard_destroy(ipir_shard* shard);
+
+/* The Horner owner of a sharded database (params as ipir_b200_shard_create
+ * returned them) on the current device; a_all: host [n_packed][limb][N] u32,
+ * the shards' exported a parts in group order. */
+ipir_horner* ipir_b200_horner_create(const ipir_params* params, const uint32_t* a_all, size_t max_batch);
+/* Responses of count <= max_batch queries from the gathered b parts, DEVICE
+ * packed_b[count][n_packed][limb][N] u32, and the queries' RGSW parts (only
+ * those are read); out_resp as ipir_answer_batch's.  The work waits for what
+ * `stream` (0: the legacy default stream) has enqueued, so packed_b may come
+ * from a collective on that stream.  Blocking; returns 0, 1, 2, 3, 4 as
+ * ipir_b200_shard_pack. */
+int ipir_b200_horner_answer(ipir_horner* h, const uint32_t* packed_b, const ipir_query_view* queries, size_t count,
+                            uint64_t* out_resp, void* stream);
+void ipir_b200_horner_destroy(ipir_horner* h);
 
 #ifdef __cplusplus
 }

@@ -51,6 +51,21 @@ struct PreprocessData {
     std::shared_ptr<PreprocessState> state;
 };
 
+// Device buffers of a preprocessed database, valid until gpu_setup_server
+// adopts them (then until gpu_free_server): the encoded u16 DB (row-major
+// db_rows x db_cols) and, per group g, the a part at a + g * a_group_stride
+// ([limb][N] u32, NTT form) and D_final at d_final + g * d_final_group_stride
+// ([limb][digit][N] u32).  D_plus / D_minus are held as tensor-core byte
+// planes (ipir_b200_export_precomp returns them in the reference layout).
+struct PreprocessDevicePointers {
+    uint16_t* db;
+    uint32_t* a;
+    size_t a_group_stride;
+    uint32_t* d_final;
+    size_t d_final_group_stride;
+};
+PreprocessDevicePointers preprocess_device_pointers(const PreprocessData& precomp);
+
 struct GpuServerConfig {  // src/gpu_protocol.h:22-24
     size_t max_batch = 16;
 };

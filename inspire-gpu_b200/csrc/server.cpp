@@ -71,17 +71,44 @@ void alloc_precomp(Precomp& P, cudaStream_t s) {
     P.pre_df = A.alloc<uint32_t>(G * kGroupStrideF);
 }
 
-static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s) {
+// P.pp is the geometry P holds.  For a group shard (global != null), P.pp
+// covers groups [g0, g0 + P.pp.n_packed) of the global database: the encode
+// mixes the D_act column polynomials of each row block across groups, so it
+// runs over full global rows (row chunks) and keeps the shard's column slab;
+// every later stage is per group and runs on the slab alone.
+static void preprocess_into(Precomp& P, const uint16_t* db_host, cudaStream_t s, const Params* global = nullptr,
+                            size_t g0 = 0) {
     const Params& pp = P.pp;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
-    const size_t d_act = std::min(pp.D, G);
+    const Params& gp = global ? *global : pp;
+    const size_t d_act = std::min(gp.D, gp.n_packed);
+    const size_t Cg = gp.db_cols, col0 = g0 * kN;  // global width, first column of this slab
     alloc_precomp(P, s);
 
     DevArena tmp;
     try {
         // ---- encode (in-place inverse DFT over D_act column polys per row block)
         if (d_act <= 1) {
-            IPB_CK(cudaMemcpyAsync(P.db, db_host, R * C * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+            IPB_CK(cudaMemcpy2DAsync(P.db, C * sizeof(uint16_t), db_host + col0, Cg * sizeof(uint16_t),
+                                     C * sizeof(uint16_t), R, cudaMemcpyHostToDevice, s));
+        } else if (global) {
+            int logd = 0;
+            while (((size_t)1 << logd) < d_act) ++logd;
+            const int nlA = std::min(logd, 4), nlB = logd - nlA;
+            const uint32_t dinv = inv_mod_p((uint32_t)d_act);
+            const size_t row_bytes = Cg * sizeof(uint16_t);
+            const size_t chunk_rows = std::max<size_t>(1, std::min<size_t>(R, (size_t)(256u << 20) / row_bytes));
+            uint16_t* staging = tmp.alloc<uint16_t>(chunk_rows * Cg);
+            uint16_t* enc = tmp.alloc<uint16_t>(chunk_rows * Cg);
+            for (size_t r0 = 0; r0 < R; r0 += chunk_rows) {
+                const size_t nr = std::min(chunk_rows, R - r0);
+                IPB_CK(cudaMemcpyAsync(staging, db_host + r0 * Cg, nr * row_bytes, cudaMemcpyHostToDevice, s));
+                IPB_CK(launch_encode_pass(staging, enc, nr, Cg, d_act, logd, 0, nlA, true, nlB == 0, dinv, s));
+                if (nlB > 0)
+                    IPB_CK(launch_encode_pass(nullptr, enc, nr, Cg, d_act, logd, nlA, nlB, false, true, dinv, s));
+                IPB_CK(cudaMemcpy2DAsync(P.db + r0 * C, C * sizeof(uint16_t), enc + col0, row_bytes,
+                                         C * sizeof(uint16_t), nr, cudaMemcpyDeviceToDevice, s));
+            }
         } else {
             int logd = 0;
             while (((size_t)1 << logd) < d_act) ++logd;
@@ -305,7 +332,7 @@ static void stage_queries(Server* S, const ipir_query_view* qs, size_t count) {
 // query buffer.  One 2-D copy when each query's parts are back to back in
 // host memory at a constant stride between queries (a flat batch array),
 // else one copy per host-contiguous run.
-static void stage_parts(const Server& S, const ipir_query_view* qs, size_t count, int p0, int np, cudaStream_t st) {
+void stage_parts(const Server& S, const ipir_query_view* qs, size_t count, int p0, int np, cudaStream_t st) {
     const size_t R = S.pp.db_rows;
     const size_t len[5] = {R, R, kBlk, kBlk, 4 * kBlk};
     const size_t off[5] = {0, R, 2 * R, 2 * R + kBlk, 2 * R + 2 * kBlk};
@@ -372,8 +399,8 @@ std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
 // rows (tp_out) and key table are shared by slices run one after the other.
 // qprep_parts: 3 prepares keys and RGSW parts here, 1 the keys only (the
 // RGSW parts are prepared elsewhere).
-static int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t q_off, size_t count, cudaStream_t st,
-                        cudaEvent_t* ev, cudaEvent_t lwe_ready = nullptr, int qprep_parts = 3) {
+int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t q_off, size_t count, cudaStream_t st,
+                 cudaEvent_t* ev, cudaEvent_t lwe_ready, int qprep_parts) {
     const Params& pp = S.pp;
     const Precomp& P = *S.pre;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
@@ -590,7 +617,7 @@ static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
 
 // A kernel whose pipeline wait ran out of iterations leaves a code in the
 // device error word; report it (the responses are then not valid).
-static void check_device_error(Lane& L) {
+void check_device_error(Lane& L) {
     int e = 0;
     IPB_CK(cudaMemcpy(&e, L.d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
@@ -769,6 +796,33 @@ static int validate_batch(const Server* S, const ipir_query_view* qs, size_t cou
     return 0;
 }
 
+Params shard_params(const Params& global, size_t g0, size_t g1) {
+    if (g1 <= g0 || g1 > global.n_packed) throw std::invalid_argument("group shard: need 0 <= lo < hi <= n_packed");
+    Params p = global;
+    p.db_cols = (g1 - g0) * kN;
+    p.n_packed = g1 - g0;
+    p.D = p.n_packed;  // a shard runs no Horner chain
+    p.num_cts = 1;
+    return p;
+}
+
+std::shared_ptr<Precomp> run_preprocess_shard(const Params& global, const uint16_t* db, size_t g0, size_t g1) {
+    if (!db) throw std::invalid_argument("gpu_preprocess: null db");
+    auto P = std::make_shared<Precomp>();
+    P->pp = shard_params(global, g0, g1);
+    IPB_CK(cudaGetDevice(&P->device));
+    cudaStream_t s = nullptr;
+    IPB_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    try {
+        preprocess_into(*P, db, s, &global, g0);
+    } catch (...) {
+        cudaStreamDestroy(s);
+        throw;
+    }
+    cudaStreamDestroy(s);
+    return P;
+}
+
 static std::shared_ptr<Precomp> run_preprocess(const Params& pp, const uint16_t* db) {
     if (!db) throw std::invalid_argument("gpu_preprocess: null db");
     auto P = std::make_shared<Precomp>();
@@ -845,6 +899,12 @@ PreprocessData gpu_preprocess(const PublicParams& pp, const uint16_t* db) {
     d.state = std::make_shared<PreprocessState>();
     d.state->p = ipb::run_preprocess(to_ipb(pp), db);
     return d;
+}
+
+PreprocessDevicePointers preprocess_device_pointers(const PreprocessData& precomp) {
+    if (!precomp.state || !precomp.state->p) throw std::invalid_argument("preprocess_device_pointers: empty or adopted");
+    const ipb::Precomp& P = *precomp.state->p;
+    return PreprocessDevicePointers{P.db, P.pre_a, ipb::kGroupStrideA, P.pre_df, ipb::kGroupStrideF};
 }
 
 GpuServerCtx* gpu_setup_server(const PublicParams& pp, const PreprocessData& precomp) {

@@ -194,6 +194,23 @@ constexpr int kPhaseDb = 1, kPhaseHorner = 2, kPhaseAll = 3;
 // stage events are recorded).
 int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
                  int phases = kPhaseAll, size_t n_ev = 6);
+// The DB-bound phase (query prep, mat-vec, tensor pass, finalize) of lane
+// slots [q_off, q_off + count) on st: packed ciphertext b parts into
+// L.packed_b.  lwe_ready: an event the mat-vec waits for (the key side runs
+// first); qprep_parts: 3 keys and RGSW parts, 1 keys only.  Returns launches.
+int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t q_off, size_t count, cudaStream_t st,
+                 cudaEvent_t* ev, cudaEvent_t lwe_ready = nullptr, int qprep_parts = 3);
+// H2D of parts [p0, p0 + np) (0, 1: LWE limbs, 2: KSK5, 3: KSK-1, 4: RGSW) of
+// each query into the handle's lane, one copy per contiguous host run.
+void stage_parts(const Server& S, const ipir_query_view* qs, size_t count, int p0, int np, cudaStream_t st);
+// Throws (and clears the word) if a kernel's bounded wait ran out.
+void check_device_error(Lane& L);
+// Geometry of the group shard [g0, g1) of a database (its column slab).
+Params shard_params(const Params& global, size_t g0, size_t g1);
+// gpu_preprocess of the group shard [g0, g1) of the host DB db (global
+// geometry): the encoded column slab and the shard's tensors.
+std::shared_ptr<Precomp> run_preprocess_shard(const Params& global, const uint16_t* db, size_t g0, size_t g1);
+
 // H2D of one flat query into query slot i of lane L.
 void stage_query_flat(const Server& S, Lane& L, size_t i, const uint64_t* flat, cudaStream_t st);
 // Schedule table (index = batch size, 0 unused) for a lane of `cap` queries

@@ -140,6 +140,19 @@ _L.ipir_serve_stats.argtypes = [C.c_void_p, C.POINTER(IpirServeCounters)]
 _L.ipir_serve_db_info.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                   C.POINTER(IpirSchedule), C.c_size_t]
 _L.ipir_serve_destroy.argtypes = [C.c_void_p]
+_L.ipir_b200_shard_create.restype = C.c_void_p
+_L.ipir_b200_shard_create.argtypes = [C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, u16p, u8p, C.c_size_t,
+                                      C.c_size_t, C.c_void_p]
+_L.ipir_b200_shard_export_a.argtypes = [C.c_void_p, u32p]
+_L.ipir_b200_shard_export_a.restype = C.c_int
+_L.ipir_b200_shard_pack.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+_L.ipir_b200_shard_pack.restype = C.c_int
+_L.ipir_b200_shard_destroy.argtypes = [C.c_void_p]
+_L.ipir_b200_horner_create.restype = C.c_void_p
+_L.ipir_b200_horner_create.argtypes = [C.c_void_p, u32p, C.c_size_t]
+_L.ipir_b200_horner_answer.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, u64p, C.c_void_p]
+_L.ipir_b200_horner_answer.restype = C.c_int
+_L.ipir_b200_horner_destroy.argtypes = [C.c_void_p]
 _L.ipir_serve_replace_db.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
 _L.ipir_b200_save_server.argtypes = [C.c_void_p, C.c_char_p]
 _L.ipir_b200_save_server.restype = C.c_int
@@ -167,7 +180,9 @@ EXPORTED = [
     "ipir_serve_stats", "ipir_serve_db_info", "ipir_serve_trace", "ipir_serve_destroy", "ipir_b200_matvec_ex",
     "ipir_b200_fill_db_device", "ipir_b200_set_schedule", "ipir_b200_wire_sizes", "ipir_b200_answer_wire",
     "ipir_serve_replace_db", "ipir_b200_save_server", "ipir_b200_load_server",
-    "ipir_b200_kernel_binary_version",
+    "ipir_b200_kernel_binary_version", "ipir_b200_shard_create", "ipir_b200_shard_export_a",
+    "ipir_b200_shard_pack", "ipir_b200_shard_destroy", "ipir_b200_horner_create", "ipir_b200_horner_answer",
+    "ipir_b200_horner_destroy",
 ]
 
 
@@ -634,3 +649,123 @@ def matvec_noalloc_rc(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0)
     32768, count <= 8); the first call on a device sets it up."""
     return _L.ipir_b200_matvec_noalloc(C.c_void_p(db_ptr), rows, cols, C.c_void_p(queries_ptr), count,
                                        C.c_void_p(out_ptr), C.c_void_p(stream or 0))
+
+
+# ------------------------------------------------------------------ group shards
+def group_ranges(n_packed, world):
+    """Contiguous group ranges [lo, hi) of a database split over `world`
+    GPUs, as equal as possible (the first n_packed % world get one more)."""
+    if world < 1 or world > n_packed:
+        raise ValueError(f"cannot split {n_packed} groups over {world} shards")
+    base, extra = divmod(n_packed, world)
+    out, lo = [], 0
+    for r in range(world):
+        hi = lo + base + (1 if r < extra else 0)
+        out.append((lo, hi))
+        lo = hi
+    return out
+
+
+class Shard:
+    """Groups [lo, hi) of one database on the current CUDA device
+    (ipir_b200_shard_create): pack() gives the b parts of those groups'
+    packed ciphertexts for a batch, in device memory."""
+
+    def __init__(self, n_entries, entry_bytes, db, group_lo, group_hi, crs_seed, db_rows=0, max_batch=16):
+        db = np.ascontiguousarray(db, dtype=np.uint16)
+        if len(crs_seed) != 64:
+            raise ValueError("crs_seed must be 64 bytes")
+        seed = np.frombuffer(bytes(crs_seed), np.uint8).copy()
+        p = IpirParams()
+        h = _L.ipir_b200_shard_create(n_entries, entry_bytes, db_rows, max_batch, _ptr(db, u16p), _ptr(seed, u8p),
+                                      group_lo, group_hi, C.byref(p))
+        if not h:
+            raise InspireError(f"ipir_b200_shard_create failed: {last_error()}")
+        self._h = h
+        self.params = p.as_dict()
+        self.lo, self.hi = group_lo, group_hi
+        self.max_batch = max_batch
+
+    @property
+    def groups(self):
+        return self.hi - self.lo
+
+    def packed_u32s(self, count):
+        return count * self.groups * 2 * RING_N
+
+    def export_a(self):
+        out = np.zeros(self.groups * 2 * RING_N, np.uint32)
+        rc = _L.ipir_b200_shard_export_a(self._h, _ptr(out, u32p))
+        if rc:
+            raise InspireError(f"shard_export_a rc={rc}: {last_error()}")
+        return out
+
+    def pack(self, queries, out_ptr):
+        """queries: flat u64 queries; out_ptr: device pointer (int) to
+        count * groups * 2 * N u32 ([query][group][limb][N])."""
+        arr = (IpirQueryView * max(1, len(queries)))()
+        keep = [np.ascontiguousarray(q, np.uint64) for q in queries]
+        for i, f in enumerate(keep):
+            arr[i] = query_view_from_flat(self.params, f)
+        rc = _L.ipir_b200_shard_pack(self._h, arr, len(keep), C.c_void_p(out_ptr))
+        if rc:
+            raise InspireError(f"shard_pack rc={rc}: {last_error()}")
+
+    def close(self):
+        if self._h:
+            _L.ipir_b200_shard_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HornerOwner:
+    """The Horner chains of a sharded database (ipir_b200_horner_create) on
+    the current CUDA device, from the gathered b parts of every group."""
+
+    def __init__(self, params, a_all, max_batch=16):
+        p = IpirParams()
+        for f, _ in IpirParams._fields_:
+            if f == "seed":
+                p.seed[:] = list(params["seed"])
+            else:
+                setattr(p, f, params[f])
+        a_all = np.ascontiguousarray(a_all, np.uint32)
+        if a_all.size != params["n_packed"] * 2 * RING_N:
+            raise ValueError("a_all must hold n_packed * 2 * N u32")
+        h = _L.ipir_b200_horner_create(C.byref(p), _ptr(a_all, u32p), max_batch)
+        if not h:
+            raise InspireError(f"ipir_b200_horner_create failed: {last_error()}")
+        self._h = h
+        self.params = dict(params)
+        self.max_batch = max_batch
+
+    def answer(self, packed_ptr, queries, stream=0, out=None):
+        """packed_ptr: device pointer to count * n_packed * 2 * N u32; returns
+        (count, num_cts * 4 * N) u64 responses."""
+        keep = [np.ascontiguousarray(q, np.uint64) for q in queries]
+        arr = (IpirQueryView * max(1, len(keep)))()
+        for i, f in enumerate(keep):
+            arr[i] = query_view_from_flat(self.params, f)
+        if out is None:
+            out = np.zeros((len(keep), response_u64s(self.params)), np.uint64)
+        rc = _L.ipir_b200_horner_answer(self._h, C.c_void_p(packed_ptr), arr, len(keep), _ptr(out, u64p),
+                                        C.c_void_p(stream or 0))
+        if rc:
+            raise InspireError(f"horner_answer rc={rc}: {last_error()}")
+        return out
+
+    def close(self):
+        if self._h:
+            _L.ipir_b200_horner_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

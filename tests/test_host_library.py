@@ -125,3 +125,16 @@ def test_wire_sizes_match_reference_client(ref, args):
     assert (a.value, b.value, c.value) == (L.ipir_query_packed_bytes(C.byref(rp)),
                                            L.ipir_response_packed_bytes(C.byref(rp)),
                                            L.ipir_response_compressed_bytes(C.byref(rp)))
+
+
+def test_reference_cpp_consumer_links_this_projects_library():
+    """The reference-typed C++ API: the consumer built against it resolves
+    the reference's server functions from libinspire_b200_refapi.so (over
+    libinspire_b200.so), not from the reference's GPU library."""
+    import subprocess
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_consumer_b200")
+    if not os.path.exists(exe):
+        pytest.skip("consumer not built (needs the reference's headers)")
+    out = subprocess.run(["ldd", exe], capture_output=True, text=True).stdout
+    assert "libinspire_b200_refapi.so" in out and "libinspire_b200.so" in out and "not found" not in out
+    assert "libinspire_ref_gpu" not in out
