@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--serve-config", default="mixed", choices=["mixed", "16gb"])
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-rates", default="")
+    ap.add_argument("--query-pool", action="store_true",
+                    help="serve mode: replay a pool of 32 queries per database instead of one fresh query per "
+                         "request from the GPU load generator")
     ap.add_argument("--serve-lanes", type=int, default=2)
     ap.add_argument("--serve-max-batch", type=int, default=64)
     ap.add_argument("--serve-overlap", action="store_true",
@@ -351,7 +354,8 @@ def serve_check(ib, srv, params, qbuf, plain_lat_ms, seconds=8.0):
         rng = random.Random(7)
         rates = []
         for x in (3, 5):
-            r = serve_rate(ib, loop, [srv], views, alone, [1.0], x * r1, seconds, rng)
+            r = serve_rate(ib, loop, [srv], PoolSource(views, alone, random.Random(8 + x)), [1.0], x * r1, seconds,
+                           rng)
             rates.append({"x_plain_rate": x, "offered_q_per_s": r["offered_q_per_s"],
                           "sustained_q_per_s": r["sustained_q_per_s"], "requests": r["requests"],
                           "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
@@ -555,11 +559,135 @@ def run_ours(args):
 
 
 # ------------------------------------------------------------------ serving loop
-def serve_rate(ib, loop, servers, views, alone, split, rate, seconds, rng):
+class PoolSource:
+    """Requests drawn from a pool of queries per database; every response is
+    compared with the plain answer of its pool query (alone[db][index])."""
+
+    def __init__(self, views, alone, rng):
+        self.views, self.alone, self.rng = views, alone, rng
+
+    def pick(self, k):
+        qi = self.rng.randrange(len(self.views[k]))
+        return qi, self.views[k][qi]
+
+    def verify(self, k, key, out):
+        return np.array_equal(out, self.alone[k][key])
+
+
+class FreshSource:
+    """One fresh synthetic query per request from the GPU load generator
+    (ipir_b200_synth_queries): a producer thread per database generates
+    chunks of queries on a side stream and copies them into pinned host
+    buffers, which the submitter hands to the serving loop (it copies each
+    request at submit).  Each response's 64-bit hash is recorded; check()
+    later regenerates every request's query from its id, answers it through
+    the blocking answer of the same database handle (batches of up to 32,
+    bit-identical to single answers) and compares hashes."""
+    CH = 32
+
+    def __init__(self, ib, servers, seed):
+        import queue
+        import torch
+        self.ib, self.servers, self.seed = ib, servers, seed
+        self.qn = [ib.query_u64s(s.params) for s in servers]
+        self.next_id = [0] * len(servers)
+        self.ready = [queue.Queue(maxsize=2) for _ in servers]
+        self.free = [queue.Queue() for _ in servers]
+        self.dev = [torch.empty((self.CH, q), dtype=torch.int64, device="cuda") for q in self.qn]
+        for k, q in enumerate(self.qn):
+            for _ in range(3):
+                self.free[k].put(torch.empty((self.CH, q), dtype=torch.int64, pin_memory=True))
+        self.cur = [None] * len(servers)
+        rng = np.random.default_rng(seed)
+        self.W = [rng.integers(0, 2 ** 63, ib.response_u64s(s.params), dtype=np.uint64) | np.uint64(1)
+                  for s in servers]
+        self.tag = 0                 # the offered rate the requests belong to
+        self.hashes = {}             # (db, id) -> (tag, hash)
+        self.stop = False
+        self.device = torch.cuda.current_device()
+        self.threads = [threading.Thread(target=self._produce, args=(k,), daemon=True) for k in range(len(servers))]
+        for t in self.threads:
+            t.start()
+
+    def _gen(self, k, first, n, host, stream):
+        self.ib.synth_queries_device(self.servers[k].params["db_rows"], self.seed + k, first, n,
+                                     self.dev[k].data_ptr(), stream.cuda_stream)
+        host[:n].copy_(self.dev[k][:n], non_blocking=True)
+        stream.synchronize()
+
+    def _produce(self, k):
+        import queue
+        import torch
+        torch.cuda.set_device(self.device)
+        stream = torch.cuda.Stream()
+        first = 0
+        while not self.stop:
+            try:
+                buf = self.free[k].get(timeout=0.1)
+            except queue.Empty:
+                continue
+            with torch.cuda.stream(stream):
+                self._gen(k, first, self.CH, buf, stream)
+            self.ready[k].put((first, buf))
+            first += self.CH
+
+    def pick(self, k):
+        c = self.cur[k]
+        if c is None or c[2] == self.CH:
+            if c is not None:
+                self.free[k].put(c[1])
+            first, buf = self.ready[k].get()
+            arr = buf.numpy().view(np.uint64)
+            c = self.cur[k] = [first, buf, 0, arr]
+        i = c[2]
+        c[2] += 1
+        qid = c[0] + i
+        return qid, self.ib.query_view_from_flat(self.servers[k].params, c[3][i])
+
+    def _hash(self, k, out):
+        with np.errstate(over="ignore"):
+            return int((out.view(np.uint64) * self.W[k]).sum(dtype=np.uint64))
+
+    def verify(self, k, key, out):
+        self.hashes[(k, key)] = (self.tag, self._hash(k, out))
+        return None
+
+    def close(self):
+        self.stop = True
+        for t in self.threads:
+            t.join(timeout=5)
+
+    def check(self):
+        """Mismatches and checked requests per tag."""
+        import torch
+        bad, checked = {}, {}
+        stream = torch.cuda.Stream()
+        host = torch.empty((self.CH, max(self.qn)), dtype=torch.int64, pin_memory=True)
+        for k, srv in enumerate(self.servers):
+            ids = sorted(i for (kk, i) in self.hashes if kk == k)
+            out = np.zeros((self.CH, self.ib.response_u64s(srv.params)), np.uint64)
+            pos = 0
+            while pos < len(ids):
+                first = ids[pos] - ids[pos] % self.CH
+                chunk = [i for i in ids[pos:pos + self.CH] if i < first + self.CH]
+                hbuf = host[:, :self.qn[k]]
+                with torch.cuda.stream(stream):
+                    self._gen(k, first, self.CH, hbuf, stream)
+                arr = hbuf.numpy().view(np.uint64)
+                got = srv.answer_batch([arr[i - first] for i in chunk], out=out[:len(chunk)])
+                for j, i in enumerate(chunk):
+                    tag, h = self.hashes[(k, i)]
+                    checked[tag] = checked.get(tag, 0) + 1
+                    if self._hash(k, got[j]) != h:
+                        bad[tag] = bad.get(tag, 0) + 1
+                pos += len(chunk)
+        return bad, checked
+
+
+def serve_rate(ib, loop, servers, source, split, rate, seconds, rng):
     """Open-loop Poisson arrivals at `rate` q/s for `seconds` on a serving
-    loop; every response is compared with the plain answer of its query
-    (alone[db][pool index])."""
-    pool_n = len(views[0])
+    loop; every response is checked by `source.verify` (a pool query against
+    its plain answer, or a fresh query's hash recorded for a later check)."""
     s0 = loop.stats()
     tickets = []          # (ticket, db, pool index)
     lock = threading.Lock()
@@ -590,7 +718,7 @@ def serve_rate(ib, loop, servers, views, alone, split, rate, seconds, rng):
                 done["queue"].append(lq[1])
                 if lq[0] > 10.0:
                     done["slow"].append((round(t_arr - t_start, 3), round(lq[0], 2), round(lq[1], 2), k))
-                if not np.array_equal(outs[k], alone[k][qi]):
+                if source.verify(k, qi, outs[k]) is False:
                     done["bad"] += 1
             done["n"] += 1
             i += 1
@@ -610,9 +738,9 @@ def serve_rate(ib, loop, servers, views, alone, split, rate, seconds, rng):
                 break
             time.sleep(min(d, 0.001) if d > 0.0015 else 0)
         k = 0 if rng.random() < split[0] else 1 if len(servers) > 1 else 0
-        qi = rng.randrange(pool_n)
+        qi, view = source.pick(k)
         while True:
-            rc, t = loop.submit_view(k, views[k][qi])
+            rc, t = loop.submit_view(k, view)
             if rc != ib.SERVE_FULL:
                 break
             full += 1
@@ -672,7 +800,7 @@ def run_serve(args):
     for k, (ne, w, dseed, cseed) in enumerate(dbs):
         p = ib.setup(ne, w)
         db = ib.fill_db(p["db_rows"] * p["db_cols"], dseed)
-        srv = ib.Server(ne, w, db, max_batch=1, crs_seed=cseed)
+        srv = ib.Server(ne, w, db, max_batch=32, crs_seed=cseed)
         del db
         servers.append(srv)
         qs = np.zeros((pool_n, ib.query_u64s(p)), np.uint64)
@@ -703,10 +831,22 @@ def run_serve(args):
              for k in range(len(dbs))]
     results = []
     rng = random.Random(6)
-    for rate in rates:
-        results.append(serve_rate(ib, loop, servers, views, alone, split, rate, args.serve_seconds, rng))
+    source = PoolSource(views, alone, random.Random(7)) if args.query_pool else FreshSource(ib, servers, 6000)
+    for tag, rate in enumerate(rates):
+        source.tag = tag
+        results.append(serve_rate(ib, loop, servers, source, split, rate, args.serve_seconds, rng))
     infos = [loop.db_info(k) for k in range(len(dbs))]
     loop.close()
+    if not args.query_pool:
+        source.close()
+        t0 = time.perf_counter()
+        bad, checked = source.check()
+        for tag, r in enumerate(results):
+            r["mismatches"] = bad.get(tag, 0)
+            r["checked"] = checked.get(tag, 0)
+        t_check = time.perf_counter() - t0
+    else:
+        t_check = 0.0
     for s in servers:
         s.close()
     line = {"metric": "serving loop: p50/p95/p99 latency and sustained q/s under open-loop Poisson arrivals",
@@ -715,8 +855,12 @@ def run_serve(args):
                                         "max_batch": args.serve_max_batch, "lanes_per_db": args.serve_lanes,
                                         "overlap_db_passes": args.serve_overlap,
                                         "scan_segments": args.serve_scan, "autotune": not args.no_autotune},
-            "n_gpus": 1, "unit": "ms", "data": "synthetic queries (pool of 32 per database)",
-            "plain": plain, "rates": results, "create_s": t_create,
+            "n_gpus": 1, "unit": "ms",
+            "data": ("synthetic queries (pool of 32 per database)" if args.query_pool else
+                     "fresh synthetic queries from the GPU load generator (ipir_b200_synth_queries), one per "
+                     "request; every response checked afterwards against the blocking answer of its regenerated "
+                     "query by 64-bit hash"),
+            "plain": plain, "rates": results, "create_s": t_create, "check_s": t_check,
             "lanes": [{"lanes": i["lanes"], "max_batch": i["max_batch"]} for i in infos],
             "bit_exact_vs_alone": all(r["mismatches"] == 0 and r["failed"] == 0 for r in results)}
     print(json.dumps(line), flush=True)

@@ -213,6 +213,19 @@ int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t cols, const
  * null argument, 4 CUDA error.  No counterpart in the reference. */
 int ipir_b200_kernel_binary_version(int* out);
 
+/* Synthetic queries for load generation, written by a kernel on `stream`
+ * (enqueued, not waited for) into the DEVICE buffer
+ * out[count][2 db_rows + 6 * 2 * 2 * N] u64 in the flat query layout: word k
+ * of query id = first_id + j is splitmix64(splitmix64(seed ^ id *
+ * 0xd1b54a32d192ed03) ^ k) mod q_l (l: the word's limb), so any query can be
+ * regenerated from its id.  Uniform residues, not encryptions: the server's
+ * work does not depend on the values, and the reference's query() stays the
+ * client for every correctness check.  No counterpart in the reference.
+ * Returns 0, 1 null out, 2 db_rows not a positive multiple of N, 4 CUDA
+ * error. */
+int ipir_b200_synth_queries(size_t db_rows, uint64_t seed, uint64_t first_id, size_t count, uint64_t* out,
+                            void* stream);
+
 /* Synthetic database for benchmarks and tests: out[k] = splitmix64(seed ^ k)
  * mod 65535 for k < count, filled on all host threads. */
 int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed);

@@ -148,6 +148,10 @@ cudaError_t launch_collapse_final(const uint32_t* ends, const uint32_t* kn1, con
 // ---------------------------------------------------------------- primitives
 // out[k] = splitmix64(seed ^ k) mod 65535 for k < count (the host
 // ipir_b200_fill_db formula), on the device.
+// Synthetic flat queries (uniform residues per limb) for ids first_id ..
+// first_id + count - 1 into out[count][2 rows + 6 * 2 * 2 * N].
+cudaError_t launch_synth_queries(uint64_t* out, size_t rows, size_t count, uint64_t seed, uint64_t first_id,
+                                 cudaStream_t s);
 cudaError_t launch_fill_db(uint16_t* out, size_t count, uint64_t seed, cudaStream_t s);
 // In-place forward/inverse NTT of n polys of N u32 (< q); limb of poly i is
 // (i / limb_run) & 1.

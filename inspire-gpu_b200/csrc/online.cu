@@ -676,7 +676,42 @@ __global__ void __launch_bounds__(256) fill_db_kernel(uint16_t* __restrict__ out
     }
 }
 
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+    x += 0x9e3779b97f4a7c15ULL;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+    return x ^ (x >> 31);
+}
+
+// Synthetic queries for load generation: word k of query `id` (flat layout
+// [b limb0: R][b limb1: R][6 blocks of [digit][limb][N]]) is
+// splitmix64(splitmix64(seed ^ id * C) ^ k) mod q_l, l the limb of word k.
+// Grid-stride over count * qstride words, coalesced writes.
+__global__ void __launch_bounds__(256) synth_query_kernel(uint64_t* __restrict__ out, size_t rows, size_t qstride,
+                                                          size_t count, uint64_t seed, uint64_t first_id) {
+    const size_t total = count * qstride;
+    for (size_t w = (size_t)blockIdx.x * 256 + threadIdx.x; w < total; w += (size_t)gridDim.x * 256) {
+        const size_t j = w / qstride, k = w - j * qstride;
+        const uint64_t h = splitmix64(seed ^ ((first_id + j) * 0xd1b54a32d192ed03ULL));
+        const uint64_t x = splitmix64(h ^ k);
+        const int l = k < rows ? 0 : k < 2 * rows ? 1 : (int)(((k - 2 * rows) / kN) & 1);
+        out[w] = x % (l ? kQ1 : kQ0);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_synth_queries(uint64_t* out, size_t rows, size_t count, uint64_t seed, uint64_t first_id,
+                                 cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    const size_t qstride = 2 * rows + 6 * (size_t)kDeff * 2 * kN;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t blocks = std::min<size_t>((count * qstride + 255) / 256, (size_t)sms * 16);
+    synth_query_kernel<<<(unsigned)blocks, 256, 0, s>>>(out, rows, qstride, count, seed, first_id);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fill_db(uint16_t* out, size_t count, uint64_t seed, cudaStream_t s) {
     if (count == 0) return cudaSuccess;

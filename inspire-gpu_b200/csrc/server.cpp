@@ -1389,6 +1389,22 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
         4);
 }
 
+int ipir_b200_synth_queries(size_t db_rows, uint64_t seed, uint64_t first_id, size_t count, uint64_t* out,
+                            void* stream) {
+    if (!out && count) return 1;
+    if (db_rows == 0 || db_rows % ipb::kN) {
+        ipb::g_last_error = "ipir_b200_synth_queries: db_rows must be a positive multiple of 2048";
+        return 2;
+    }
+    if (count == 0) return 0;
+    return guarded(
+        [&]() -> int {
+            IPB_CK(ipb::launch_synth_queries(out, db_rows, count, seed, first_id, static_cast<cudaStream_t>(stream)));
+            return 0;
+        },
+        4);
+}
+
 int ipir_b200_fill_db(uint16_t* out, size_t count, uint64_t seed) {
     if (!out && count) return 1;
     // splitmix64(seed ^ k) mod 65535 at flat index k, on all host threads.

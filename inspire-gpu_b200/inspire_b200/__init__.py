@@ -153,6 +153,8 @@ _L.ipir_b200_horner_create.argtypes = [C.c_void_p, u32p, C.c_size_t]
 _L.ipir_b200_horner_answer.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, u64p, C.c_void_p]
 _L.ipir_b200_horner_answer.restype = C.c_int
 _L.ipir_b200_horner_destroy.argtypes = [C.c_void_p]
+_L.ipir_b200_synth_queries.argtypes = [C.c_size_t, C.c_uint64, C.c_uint64, C.c_size_t, C.c_void_p, C.c_void_p]
+_L.ipir_b200_synth_queries.restype = C.c_int
 _L.ipir_serve_replace_db.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
 _L.ipir_b200_save_server.argtypes = [C.c_void_p, C.c_char_p]
 _L.ipir_b200_save_server.restype = C.c_int
@@ -182,7 +184,7 @@ EXPORTED = [
     "ipir_serve_replace_db", "ipir_b200_save_server", "ipir_b200_load_server",
     "ipir_b200_kernel_binary_version", "ipir_b200_shard_create", "ipir_b200_shard_export_a",
     "ipir_b200_shard_pack", "ipir_b200_shard_destroy", "ipir_b200_horner_create", "ipir_b200_horner_answer",
-    "ipir_b200_horner_destroy",
+    "ipir_b200_horner_destroy", "ipir_b200_synth_queries",
 ]
 
 
@@ -631,6 +633,37 @@ def fill_db_device(ptr, count, seed, stream=0):
     rc = _L.ipir_b200_fill_db_device(C.c_void_p(ptr), count, seed, C.c_void_p(stream or 0))
     if rc:
         raise InspireError(f"fill_db_device rc={rc}: {last_error()}")
+
+
+def synth_queries_device(db_rows, seed, first_id, count, out_ptr, stream=0):
+    """Synthetic flat queries (uniform residues per limb) for ids first_id ..
+    first_id + count - 1, written by a kernel into device memory at out_ptr
+    (enqueued on `stream`)."""
+    rc = _L.ipir_b200_synth_queries(db_rows, seed, first_id, count, C.c_void_p(out_ptr), C.c_void_p(stream or 0))
+    if rc:
+        raise InspireError(f"synth_queries rc={rc}: {last_error()}")
+
+
+def synth_queries_host(db_rows, seed, first_id, count):
+    """The same values computed on the host (numpy), for checks."""
+    qn = 2 * db_rows + 6 * D_EFF * 2 * RING_N
+    k = np.arange(qn, dtype=np.uint64)
+    limb = np.where(k < db_rows, 0, np.where(k < 2 * db_rows, 1, ((k - 2 * db_rows) // RING_N) & 1))
+    q = np.where(limb == 1, np.uint64(Q1), np.uint64(Q0)).astype(np.uint64)
+    out = np.empty((count, qn), np.uint64)
+    with np.errstate(over="ignore"):
+        for j in range(count):
+            h = _splitmix64(np.uint64(seed) ^ (np.uint64(first_id + j) * np.uint64(0xD1B54A32D192ED03)))
+            out[j] = _splitmix64(h ^ k) % q
+    return out
+
+
+def _splitmix64(x):
+    with np.errstate(over="ignore"):
+        x = np.asarray(x, np.uint64) + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return x ^ (x >> np.uint64(31))
 
 
 def kernel_binary_version():

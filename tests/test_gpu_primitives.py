@@ -67,3 +67,20 @@ def test_kernels_loaded_as_sm100():
     """The CUDA runtime loaded the library's sm_100a cubin (binaryVersion 100)."""
     import inspire_b200 as ib
     assert ib.kernel_binary_version() == 100
+
+
+def test_synth_queries_kernel_matches_host_formula():
+    """The load generator's kernel writes what its host restatement gives,
+    residues below each word's limb modulus, distinct per query id."""
+    import torch
+    import inspire_b200 as ib
+    rows, n, first = 2048, 3, 1_000_003
+    qn = ib.query_u64s({"db_rows": rows})
+    buf = torch.zeros(n * qn, dtype=torch.int64, device="cuda")
+    ib.synth_queries_device(rows, 77, first, n, buf.data_ptr())
+    torch.cuda.synchronize()
+    got = buf.cpu().numpy().view(np.uint64).reshape(n, qn)
+    want = ib.synth_queries_host(rows, 77, first, n)
+    assert (got == want).all()
+    assert (got[:, :rows] < QS[0]).all() and (got[:, rows:2 * rows] < QS[1]).all()
+    assert not (got[0] == got[1]).all()

@@ -138,3 +138,15 @@ def test_reference_cpp_consumer_links_this_projects_library():
     out = subprocess.run(["ldd", exe], capture_output=True, text=True).stdout
     assert "libinspire_b200_refapi.so" in out and "libinspire_b200.so" in out and "not found" not in out
     assert "libinspire_ref_gpu" not in out
+
+
+def test_synth_queries_host_formula_ranges():
+    import inspire_b200 as ib
+    from oracle_lib import Q0, Q1
+    rows = 4096
+    q = ib.synth_queries_host(rows, 5, 0, 2)
+    blocks = q[:, 2 * rows:].reshape(2, -1, 2048)
+    assert (q[:, :rows] < Q0).all() and (q[:, rows:2 * rows] < Q1).all()
+    assert (blocks[:, 0::2] < Q0).all() and (blocks[:, 1::2] < Q1).all()
+    assert (q[:, rows:2 * rows] >= Q0).any()          # limb 1 uses its own modulus
+    assert (ib.synth_queries_host(rows, 5, 1, 1)[0] == q[1]).all()   # a query regenerates from its id
