@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--mv-batches", default="1,16,32,64,128,256")
     ap.add_argument("--n-entries", type=int, default=1 << 29)
     ap.add_argument("--entry-bytes", type=int, default=30)
+    ap.add_argument("--db-rows", type=int, default=0,
+                    help="db_rows for setup() (0: its default); e.g. 2048 with --n-entries 8388608 --entry-bytes 120 "
+                         "gives the 16 GB geometry's 128 groups on a 1 GB DB")
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
@@ -381,12 +384,12 @@ def run_ours(args):
     B = args.batch
     sweep = [] if args.no_sweep else [b for b in SWEEP if b != B]
     max_b = max([B] + sweep)
-    params = ib.setup(args.n_entries, args.entry_bytes)
+    params = ib.setup(args.n_entries, args.entry_bytes, args.db_rows)
     R, Ccols, G = params["db_rows"], params["db_cols"], params["n_packed"]
     db = ib.fill_db(R * Ccols, 0)
     seed = bytes(range(64))
     t0 = time.perf_counter()
-    srv = ib.Server(args.n_entries, args.entry_bytes, db, max_batch=max_b, crs_seed=seed)
+    srv = ib.Server(args.n_entries, args.entry_bytes, db, db_rows=args.db_rows, max_batch=max_b, crs_seed=seed)
     t_pre = time.perf_counter() - t0
     del db
     t_tune = 0.0

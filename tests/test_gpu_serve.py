@@ -222,3 +222,37 @@ def test_generation_swap(env):
             loop.close()
     finally:
         sa2.close()
+
+
+def test_hbm_budget_halves_batch_then_lanes_then_refuses(env):
+    """Admission capacity is sized against the HBM budget at create: as the
+    budget shrinks the loop first halves max_batch (64, 32, ... 1), then
+    drops lanes (2 -> 1), then refuses to start (nothing is allocated per
+    request afterwards, so no later check is needed); a loop sized down
+    still answers bit-exactly."""
+    import inspire_b200 as ib
+    ca, cb, sa, sb, reqs, alone = env
+    seen = []
+    budget = 1 << 36
+    while budget >= 1 << 16:
+        try:
+            loop = ib.ServeLoop([sa, sb], max_batch=64, lanes_per_db=2, hbm_budget_bytes=budget, graphs=False,
+                                autotune=False)
+        except ib.InspireError as e:
+            assert "exceeds the HBM budget" in str(e)
+            seen.append((0, 0))
+            break
+        info = loop.db_info(0)
+        seen.append((info["max_batch"], info["lanes"]))
+        if info["max_batch"] < 64 and not any(s[0] < 64 for s in seen[:-1]):   # the first shrunk loop answers
+            d, _, q, _ = reqs[0]
+            out = np.zeros_like(alone[0])
+            loop.wait(loop.submit(d, q), out=out)
+            assert (out == alone[0]).all()
+        loop.close()
+        budget //= 2
+    assert seen[0] == (64, 2) and seen[-1] == (0, 0), seen
+    order = [(-mb, -ln) for mb, ln in seen[:-1]]
+    assert order == sorted(order), seen              # capacity only shrinks as the budget does
+    lanes_at = [ln for mb, ln in seen[:-1]]
+    assert 1 in lanes_at and all(mb == 1 for mb, ln in seen[:-1] if ln == 1), seen  # lanes drop only at batch 1
