@@ -207,6 +207,18 @@ int ipir_b200_matvec_ex(const uint16_t* db, size_t rows, size_t cols, const uint
 int ipir_b200_matvec_noalloc(const uint16_t* db, size_t rows, size_t cols, const uint64_t* queries,
                              size_t count, uint32_t* out, void* stream);
 
+/* HornerEval (the reference's src/crypto.cpp:264-279, GPU form
+ * src/gpu_online.cu:474-540) on caller data, through the server's Horner
+ * kernels: acc = cts[L - 1]; for i = L - 2 .. 0: acc = ExtProd(rgsw, acc) +
+ * cts[i]; out = acc.  rgsw: 4 * D_EFF * 2 * N u64
+ * ([top_a|top_b|bot_a|bot_b][digit][limb][coeff], NTT form); cts: L * 4 * N
+ * u64 ([ct][a|b][limb][coeff], NTT form); out: 4 * N u64.  L = 2 with
+ * cts[0] = 0 is one ExtProd (src/crypto.cpp:219-257).  variant: 0 one CTA
+ * per chain, 1 a 4-CTA cluster, 2 an 8-CTA cluster.  A parity primitive: it
+ * allocates and synchronises.  Returns 0, 1 null argument or L = 0, 2 bad
+ * variant or L > 4096, 4 CUDA error. */
+int ipir_b200_horner_eval(const uint64_t* rgsw, const uint64_t* cts, size_t L, uint64_t* out, int variant);
+
 /* Target of the library's device code as the CUDA runtime loaded it:
  * *out = cudaFuncAttributes.binaryVersion of its tensor-core mat-vec kernel
  * (100 for the sm_100a cubins this library is built from).  Returns 0, 1

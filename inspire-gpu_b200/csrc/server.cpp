@@ -1262,6 +1262,57 @@ int ipir_b200_decomp(const uint32_t* in, uint32_t* out, size_t n) {
         4);
 }
 
+int ipir_b200_horner_eval(const uint64_t* rgsw, const uint64_t* cts, size_t L, uint64_t* out, int variant) {
+    if (!rgsw || !cts || !out || L == 0) return 1;
+    if (variant < 0 || variant > 2 || L > 4096) {
+        ipb::g_last_error = "ipir_b200_horner_eval: variant 0..2, 1 <= L <= 4096";
+        return 2;
+    }
+    return guarded(
+        [&]() -> int {
+            using ipb::kN;
+            const size_t blk = (size_t)ipb::kDeff * 2 * kN;
+            // residues as u32: a and b halves of each ciphertext, the RGSW parts
+            std::vector<uint32_t> a(L * 2 * kN), b(L * 2 * kN), rg(4 * blk);
+            for (size_t g = 0; g < L; ++g)
+                for (size_t x = 0; x < 2 * kN; ++x) {
+                    const uint64_t q = (x / kN) ? ipb::kQ1 : ipb::kQ0;
+                    a[g * 2 * kN + x] = (uint32_t)(cts[g * 4 * kN + x] % q);
+                    b[g * 2 * kN + x] = (uint32_t)(cts[g * 4 * kN + 2 * kN + x] % q);
+                }
+            for (size_t i = 0; i < 4 * blk; ++i) rg[i] = (uint32_t)(rgsw[i] % (((i / kN) & 1) ? ipb::kQ1 : ipb::kQ0));
+            ipb::DevArena A;
+            try {
+                ipb::DevTables* T = ipb::upload_tables(A, 0);
+                uint32_t* da = A.alloc<uint32_t>(a.size());
+                uint32_t* db = A.alloc<uint32_t>(b.size());
+                uint32_t* dr = A.alloc<uint32_t>(rg.size());
+                uint64_t* dout = A.alloc<uint64_t>(4 * kN);
+                int* err = A.alloc<int>(1);
+                IPB_CK(cudaMemcpy(da, a.data(), a.size() * 4, cudaMemcpyHostToDevice));
+                IPB_CK(cudaMemcpy(db, b.data(), b.size() * 4, cudaMemcpyHostToDevice));
+                IPB_CK(cudaMemcpy(dr, rg.data(), rg.size() * 4, cudaMemcpyHostToDevice));
+                IPB_CK(cudaMemset(err, 0, sizeof(int)));
+                if (variant == 0)
+                    IPB_CK(ipb::launch_horner(da, db, L * 2 * kN, dr, T, L, L, 1, dout, 4 * kN, 1, 0));
+                else if (variant == 1)
+                    IPB_CK(ipb::launch_horner_cluster(da, db, L * 2 * kN, dr, T, L, L, 1, dout, 4 * kN, 1, err, 0));
+                else
+                    IPB_CK(ipb::launch_horner_cluster8(da, db, L * 2 * kN, dr, T, L, L, 1, dout, 4 * kN, 1, err, 0));
+                int h_err = 0;
+                IPB_CK(cudaMemcpy(out, dout, 4 * kN * 8, cudaMemcpyDeviceToHost));
+                IPB_CK(cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost));
+                if (h_err) throw std::runtime_error("device pipeline wait timed out");
+            } catch (...) {
+                A.free_all();
+                throw;
+            }
+            A.free_all();
+            return 0;
+        },
+        4);
+}
+
 namespace {
 // Scratch of ipir_b200_matvec, cached per device and grown on demand.
 struct MvScratch {

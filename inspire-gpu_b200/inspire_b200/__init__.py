@@ -155,6 +155,8 @@ _L.ipir_b200_horner_answer.restype = C.c_int
 _L.ipir_b200_horner_destroy.argtypes = [C.c_void_p]
 _L.ipir_b200_synth_queries.argtypes = [C.c_size_t, C.c_uint64, C.c_uint64, C.c_size_t, C.c_void_p, C.c_void_p]
 _L.ipir_b200_synth_queries.restype = C.c_int
+_L.ipir_b200_horner_eval.argtypes = [u64p, u64p, C.c_size_t, u64p, C.c_int]
+_L.ipir_b200_horner_eval.restype = C.c_int
 _L.ipir_serve_replace_db.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
 _L.ipir_b200_save_server.argtypes = [C.c_void_p, C.c_char_p]
 _L.ipir_b200_save_server.restype = C.c_int
@@ -184,7 +186,7 @@ EXPORTED = [
     "ipir_serve_replace_db", "ipir_b200_save_server", "ipir_b200_load_server",
     "ipir_b200_kernel_binary_version", "ipir_b200_shard_create", "ipir_b200_shard_export_a",
     "ipir_b200_shard_pack", "ipir_b200_shard_destroy", "ipir_b200_horner_create", "ipir_b200_horner_answer",
-    "ipir_b200_horner_destroy", "ipir_b200_synth_queries",
+    "ipir_b200_horner_destroy", "ipir_b200_synth_queries", "ipir_b200_horner_eval",
 ]
 
 
@@ -664,6 +666,20 @@ def _splitmix64(x):
         x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
         x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         return x ^ (x >> np.uint64(31))
+
+
+def horner_eval(rgsw, cts, L, variant=1):
+    """HornerEval on host arrays through the server's Horner kernels
+    (variant 0: one CTA, 1: 4-CTA cluster, 2: 8-CTA cluster); returns 4 N u64."""
+    rgsw = np.ascontiguousarray(rgsw, np.uint64)
+    cts = np.ascontiguousarray(cts, np.uint64)
+    if rgsw.size != 4 * D_EFF * 2 * RING_N or cts.size != L * 4 * RING_N:
+        raise ValueError("rgsw must hold 4 * D_EFF * 2 * N u64 and cts L * 4 * N u64")
+    out = np.zeros(4 * RING_N, np.uint64)
+    rc = _L.ipir_b200_horner_eval(_ptr(rgsw, u64p), _ptr(cts, u64p), L, _ptr(out, u64p), variant)
+    if rc:
+        raise InspireError(f"horner_eval rc={rc}: {last_error()}")
+    return out
 
 
 def kernel_binary_version():
