@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the shortened runs of configurations 2 (1 GB single-query path), 5 (mixed serving, "
+                         "5 s per rate) and 4 (64 GB mat-vec) that the default run appends under `configs`")
     ap.add_argument("--no-serve-check", action="store_true",
                     help="skip the serving-loop check (cyclic scan at 3x and 5x the plain rate) of the default run")
     ap.add_argument("--serve-config", default="mixed", choices=["mixed", "16gb"])
@@ -555,6 +558,17 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.n_entries, args.entry_bytes)
     srv.close()
+    if rank == 0 and world == 1 and not args.no_configs:
+        # the other configurations, shortened, so one default run records them all
+        import argparse as _ap
+        a5 = _ap.Namespace(**vars(args))
+        a5.serve_config, a5.serve_seconds, a5.serve_rates, a5.serve_scan = "mixed", 5.0, "", None
+        a5.query_pool, a5.no_autotune, a5.serve_max_batch, a5.serve_lanes, a5.serve_overlap = False, False, 64, 2, False
+        line["configs"] = {
+            "config2_1gb_single_query": config2(ib),
+            "config5_mixed_serving_5s_per_rate": serve_sweep(a5),
+            "config4_matvec_64gb": matvec_sweep(1 << 31, [1, 16, 32, 64, 128, 256], cuda_core_max_b=16, quick=True),
+        }
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -786,6 +800,12 @@ def serve_rate(ib, loop, servers, source, split, rate, seconds, rng):
 
 def run_serve(args):
     """Open-loop Poisson load on the continuous-batching serving loop."""
+    print(json.dumps(serve_sweep(args)), flush=True)
+
+
+def serve_sweep(args):
+    """The serving loop under open-loop Poisson arrivals at each offered rate
+    (configuration 5 with --serve-config mixed); returns the JSON object."""
     import torch
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
@@ -866,7 +886,64 @@ def run_serve(args):
             "plain": plain, "rates": results, "create_s": t_create, "check_s": t_check,
             "lanes": [{"lanes": i["lanes"], "max_batch": i["max_batch"]} for i in infos],
             "bit_exact_vs_alone": all(r["mismatches"] == 0 and r["failed"] == 0 for r in results)}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def config2(ib, n_queries=256):
+    """Configuration 2, the single-query path at 1 GB: setup(2^25, 30), DB
+    from seed 0, gpu_preprocess timed (ipir_server_create from the host DB),
+    then n_queries sequential plain answers through ipir_answer_batch (fresh
+    synthetic queries from the GPU load generator, seed 3), and the batch-1
+    DB pass in GB/s from the stage timers.  Bit-exactness at this geometry
+    against the reference's own GPU build is the parity test
+    tests/test_gpu_vs_reference_gpu_geoms.py (cfg2)."""
+    import torch
+    p = ib.setup(1 << 25, 30)
+    R, Cc = p["db_rows"], p["db_cols"]
+    db = ib.fill_db(R * Cc, 0)
+    t0 = time.perf_counter()
+    srv = ib.Server(1 << 25, 30, db, max_batch=1, crs_seed=bytes([1] * 64))
+    t_pre = time.perf_counter() - t0
+    del db
+    qn = ib.query_u64s(p)
+    dq = torch.empty((n_queries, qn), dtype=torch.int64, device="cuda")
+    ib.synth_queries_device(R, 3, 0, n_queries, dq.data_ptr())
+    hq = dq.cpu().numpy().view(np.uint64)
+    del dq
+    out = np.zeros(ib.response_u64s(p), np.uint64)
+    views = (ib.IpirQueryView * n_queries)()
+    for i in range(n_queries):
+        views[i] = ib.query_view_from_flat(p, hq[i])
+    for i in range(3):
+        srv.answer_batch_rc(views, 1, out)
+    lat = []
+    for i in range(n_queries):
+        t1 = time.perf_counter()
+        rc = srv.answer_batch_rc(C_view(views, i), 1, out)
+        lat.append((time.perf_counter() - t1) * 1e3)
+        assert rc == 0
+    srv.enable_stage_timing(True)
+    st = []
+    for i in range(5):
+        srv.answer_batch_rc(C_view(views, i), 1, out)
+        st.append(srv.stage_times())
+    srv.enable_stage_timing(False)
+    srv.close()
+    stm = {k: statistics.median(x[k] for x in st) for k in st[0]}
+    peak, kind = measured_peaks()
+    lat.sort()
+    gbs = R * Cc * 2 / (stm["matvec"] * 1e-3) / 1e9
+    return {"workload": describe(p), "preprocess_s": t_pre, "answers": n_queries,
+            "p50_ms_e2e": lat[len(lat) // 2], "p99_ms_e2e": lat[min(len(lat) - 1, int(0.99 * (len(lat) - 1)))],
+            "q_per_s_e2e": n_queries * 1e3 / sum(lat), "stage_ms_b1": stm, "db_pass_gbs": gbs,
+            "db_pass_frac": gbs / peak, "peak_source": kind,
+            "parity": "bit-exact vs the reference GPU build at this geometry: tests/test_gpu_vs_reference_gpu_geoms.py"}
+
+
+def C_view(views, i):
+    """The query view array starting at element i (ctypes pointer arithmetic)."""
+    import ctypes as C
+    return C.cast(C.addressof(views) + i * C.sizeof(views._type_), C.POINTER(views._type_))
 
 
 def splitmix_mod(idx, seed):
@@ -880,18 +957,23 @@ def splitmix_mod(idx, seed):
 
 
 def run_matvec(args):
-    """Exact mat-vec microbench: DB x B queries on the tensor cores and on the
-    CUDA cores, each B's schedule autotuned, sampled columns checked against
-    exact host dot products."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(matvec_sweep(args.mv_entries, [int(x) for x in args.mv_batches.split(",")])), flush=True)
+
+
+def matvec_sweep(mv_entries, Bs, cuda_core_max_b=None, quick=False):
+    """Exact mat-vec microbench (configuration 4): DB x B queries on the
+    tensor cores and on the CUDA cores, each B's schedule autotuned (quick:
+    the default schedule only), sampled columns checked against exact host
+    dot products.  Returns the JSON object."""
     import torch
     import inspire_b200 as ib
-    torch.cuda.set_device(0)
-    params = ib.setup(args.mv_entries, 30)
+    params = ib.setup(mv_entries, 30)
     R, Cc = params["db_rows"], params["db_cols"]
     db_seed, q_seed = 0, 5
     db = torch.empty(R * Cc, dtype=torch.int16, device="cuda")
     ib.fill_db_device(db.data_ptr(), R * Cc, db_seed)
-    Bs = [int(x) for x in args.mv_batches.split(",")]
     Bmax = max(Bs)
     rng = np.random.default_rng(q_seed)
     qh = np.empty((Bmax, 2, R), np.uint64)
@@ -936,9 +1018,13 @@ def run_matvec(args):
     for B in Bs:
         row = {}
         for path in (0, 1):
-            if path == 0:
+            if path == 1 and cuda_core_max_b is not None and B > cuda_core_max_b:
+                continue
+            if path == 0 and not quick:
                 qpps = sorted({min(B, 32)} | ({16, 8} if B > 16 else set()) | ({B} if B < 32 else set()))
                 kcs = [0] + [k for k in (8192, 16384) if R % k == 0 and k < R]
+            elif path == 0:
+                qpps, kcs = [min(B, 32)], [0]
             else:
                 qpps, kcs = [min(B, 4)], [0]
             best = None
@@ -964,16 +1050,17 @@ def run_matvec(args):
                 d["int8_frac"] = d["int8_tops"] / int8_peak
             row["tensor_cores" if path == 0 else "cuda_cores"] = d
         results[str(B)] = row
-    line = {"metric": "exact mat-vec microbench: ms, q/s, HBM GB/s and int8 TOPS per batch (tensor vs CUDA cores)",
+    del db, q, out
+    torch.cuda.empty_cache()
+    return {"metric": "exact mat-vec microbench: ms, q/s, HBM GB/s and int8 TOPS per batch (tensor vs CUDA cores)",
             "mode": "matvec", "n_gpus": 1, "data": "synthetic",
-            "config": {"workload": f"setup(2^{args.mv_entries.bit_length() - 1}, w=30): {R} x {Cc} u16 DB "
+            "config": {"workload": f"setup(2^{mv_entries.bit_length() - 1}, w=30): {R} x {Cc} u16 DB "
                                    f"({db_bytes / 1e9:.1f} GB, splitmix64 seed {db_seed}), queries uniform in [0, q) "
                                    f"per limb (seed {q_seed})",
                        "check": "24 sampled columns x all queries x both limbs vs exact host dot products"},
             "peaks": {"hbm_gbs": hbm_peak, "hbm_source": peak_kind, "int8_tops": int8_peak, "int8_source": int8_kind},
             "results": results,
             "bit_exact": all(v[p]["sampled_mismatches"] == 0 for v in results.values() for p in v)}
-    print(json.dumps(line), flush=True)
 
 
 def run_refgpu(args):
