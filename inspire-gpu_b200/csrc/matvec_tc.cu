@@ -31,9 +31,6 @@
 // simply take fewer items instead of delaying the whole pass.
 #include <cuda.h>
 
-#include <cstdio>
-#include <cstdlib>
-
 #include "ipb_common.cuh"
 #include "host_util.h"
 #include "ipb_launch.h"
@@ -65,8 +62,7 @@ struct TcParams {
     int n_mtiles;
     int n_kchunks;
     int kchunk_rows;
-    int stages_a;          // DB ring: slots of two 128-byte m' boxes x kKT rows (16 KB)
-    int stages_b;          // query-plane ring: slots of npad x kKT bytes
+    int stages;
     int acc_stages;
     uint32_t tmem_cols;
     int* err;
@@ -80,19 +76,16 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                                                        const __grid_constant__ CUtensorMap map_b, TcParams P) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int SA = P.stages_a, SB = P.stages_b;
+    const int S = P.stages;
     const uint32_t a_bytes = kKT * 128;              // one 128-byte m' box x kKT rows
     const uint32_t b_bytes = (uint32_t)P.npad * kKT;
-    const uint32_t slot_a = 2 * a_bytes;
-    uint8_t* ring_b = smem + (size_t)SA * slot_a;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(ring_b + (size_t)SB * b_bytes);
-    uint64_t* afull = bars;                 // DB slot landed
-    uint64_t* aempty = bars + SA;           // DB slot consumed by the MMAs
-    uint64_t* bfull = bars + 2 * SA;        // query-plane slot landed
-    uint64_t* bempty = bars + 2 * SA + SB;  // query-plane slot consumed
-    uint64_t* tfull = bars + 2 * SA + 2 * SB;
-    uint64_t* tempty = tfull + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tfull + 4);
+    const uint32_t stage_bytes = 2 * a_bytes + b_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)S * stage_bytes);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + S;
+    uint64_t* tfull = bars + 2 * S;
+    uint64_t* tempty = bars + 2 * S + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 4);
     __shared__ volatile int abort_flag;
     __shared__ volatile int item_ring[kRing];
     __shared__ uint64_t ifull[kRing], iempty[kRing];
@@ -101,11 +94,9 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         abort_flag = 0;
-        for (int s = 0; s < SA; ++s) { mbar_init(&afull[s], 1); mbar_init(&aempty[s], 1); }
-        for (int s = 0; s < SB; ++s) { mbar_init(&bfull[s], 1); mbar_init(&bempty[s], 1); }
+        for (int s = 0; s < S; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 128); }
-        // readers of each published item: the plane producer, the MMA issuer, 128 epilogue threads
-        for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 1 + 128); }
+        for (int r = 0; r < kRing; ++r) { mbar_init(&ifull[r], 1); mbar_init(&iempty[r], 1 + 128); }
         mbar_init(&mma_done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -142,59 +133,32 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                 const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
                 const int m0 = mt * kMT;
                 for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&aempty[s], ph ^ 1, P.err, 1)) { abort_flag = 1; break; }
-                    uint8_t* st = smem + (size_t)s * slot_a;
-                    mbar_expect_tx(&afull[s], slot_a);
+                    if (!mbar_wait(&empty[s], ph ^ 1, P.err, 1)) { abort_flag = 1; break; }
+                    uint8_t* st = smem + (size_t)s * stage_bytes;
+                    mbar_expect_tx(&full[s], stage_bytes);
                     const int k0 = kc * P.kchunk_rows + kt * kKT;
-                    tma_load_2d(st, &map_a, &afull[s], m0, k0);
-                    tma_load_2d(st + a_bytes, &map_a, &afull[s], m0 + 128, k0);
+                    tma_load_2d(st, &map_a, &full[s], m0, k0);
+                    tma_load_2d(st + a_bytes, &map_a, &full[s], m0 + 128, k0);
+                    tma_load_2d(st + 2 * a_bytes, &map_b, &full[s], k0, 0);
                     ++issued;
-                    if (++s == SA) { s = 0; ph ^= 1; }
+                    if (++s == S) { s = 0; ph ^= 1; }
                 }
             }
             // Drain: every issued load has landed in shared memory before the
             // CTA exits, also when the MMA issuer stopped early (a timeout) and
-            // never consumed them.  Load n went to slot n % SA with phase
-            // (n / SA) & 1; no later load reuses a slot, so each wait is exact.
-            for (unsigned i = 0; i < (unsigned)SA && i < issued; ++i) {
+            // never consumed them.  Load n went to stage n % S with phase
+            // (n / S) & 1; no later load reuses a stage, so each wait is exact.
+            for (unsigned i = 0; i < (unsigned)S && i < issued; ++i) {
                 const unsigned n = issued - 1 - i;
-                mbar_wait(&afull[n % SA], (n / SA) & 1u, P.err, 2);
-            }
-        }
-    } else if (warp == 2) {
-        // ---------------- query-plane producer: its own ring, so the DB ring
-        // (the long-latency HBM stream) can run further ahead than the
-        // planes (L2-resident, re-read by every work item)
-        if (lane == 0) {
-            int s = 0;
-            uint32_t ph = 0;
-            unsigned issued = 0;
-            for (int it = 0;; ++it) {
-                const int r = it % kRing;
-                if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 10)) { abort_flag = 1; break; }
-                const int item = item_ring[r];
-                mbar_arrive(&iempty[r]);
-                if (item < 0 || abort_flag) break;
-                const int kc = item / P.n_mtiles;
-                for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&bempty[s], ph ^ 1, P.err, 11)) { abort_flag = 1; break; }
-                    mbar_expect_tx(&bfull[s], b_bytes);
-                    tma_load_2d(ring_b + (size_t)s * b_bytes, &map_b, &bfull[s], kc * P.kchunk_rows + kt * kKT, 0);
-                    ++issued;
-                    if (++s == SB) { s = 0; ph ^= 1; }
-                }
-            }
-            for (unsigned i = 0; i < (unsigned)SB && i < issued; ++i) {
-                const unsigned n = issued - 1 - i;
-                mbar_wait(&bfull[n % SB], (n / SB) & 1u, P.err, 12);
+                mbar_wait(&full[n % S], (n / S) & 1u, P.err, 2);
             }
         }
     } else if (warp == 1) {
         // ---------------- MMA issuer
         if (lane == 0) {
             const uint32_t idesc = idesc_i8(P.npad);
-            int s = 0, sb = 0, as = 0;
-            uint32_t ph = 0, phb = 0, aph = 0;
+            int s = 0, as = 0;
+            uint32_t ph = 0, aph = 0;
             bool it_mma = false;  // any MMA issued
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
@@ -206,13 +170,9 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                 tc_fence_after();
                 const uint32_t d0 = tmem_base + (uint32_t)(as * 2 * P.npad);
                 for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&afull[s], ph, P.err, 4) || !mbar_wait(&bfull[sb], phb, P.err, 13)) {
-                        abort_flag = 1;
-                        break;
-                    }
+                    if (!mbar_wait(&full[s], ph, P.err, 4)) { abort_flag = 1; break; }
                     tc_fence_after();
-                    const uint8_t* st = smem + (size_t)s * slot_a;
-                    const uint8_t* bt = ring_b + (size_t)sb * b_bytes;
+                    const uint8_t* st = smem + (size_t)s * stage_bytes;
 #pragma unroll
                     for (int kk = 0; kk < kKT / 32; ++kk) {
                         // A: MN-major, rows of 128 bytes, 8-row swizzle atoms (SBO 1024 B);
@@ -220,16 +180,14 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                         const uint64_t a0 = smem_desc(st + kk * 4096, 0, 1024);
                         const uint64_t a1 = smem_desc(st + a_bytes + kk * 4096, 0, 1024);
                         // B: K-major, 64-byte rows (SWIZZLE_64B), 8-row groups 512 B apart; K advances 32 bytes.
-                        const uint64_t b = smem_desc_sw64(bt + kk * 32, 512);
+                        const uint64_t b = smem_desc_sw64(st + 2 * a_bytes + kk * 32, 512);
                         const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
                         mma_i8(d0, a0, b, idesc, acc);
                         mma_i8(d0 + (uint32_t)P.npad, a1, b, idesc, acc);
                     }
                     it_mma = true;
-                    mma_commit(&aempty[s]);  // both slots free once these MMAs complete
-                    mma_commit(&bempty[sb]);
-                    if (++s == SA) { s = 0; ph ^= 1; }
-                    if (++sb == SB) { sb = 0; phb ^= 1; }
+                    mma_commit(&empty[s]);
+                    if (++s == S) { s = 0; ph ^= 1; }
                 }
                 mma_commit(&tfull[as]);
                 if (++as == P.acc_stages) { as = 0; aph ^= 1; }
@@ -479,36 +437,11 @@ cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, s
     P.err = err;
     P.tiles = tiles;
     P.T = T;
-    const size_t slot_a = 2 * (size_t)kKT * 128, slot_b = (size_t)npad * kKT;
+    const size_t stage_bytes = 2 * (size_t)kKT * 128 + (size_t)npad * kKT;
     const size_t budget = 200 * 1024;
-    // Ring depths.  At few queries the plane slots are small and both rings
-    // take as many slots as fit together (at most 8).  With many queries the
-    // plane slots (npad x 64 B, 14 KB at 32 queries) would crowd the DB out
-    // of shared memory: the DB ring keeps 8 slots (128 KB of the HBM stream
-    // in flight per SM) and the plane ring takes what is left, since its
-    // loads come from L2 with a much shorter latency.
-    int sa, sb;
-    if (npad <= 32) {
-        sa = sb = (int)std::min<size_t>(8, budget / (slot_a + slot_b));
-    } else {
-        sa = 8;
-        sb = (int)std::min<size_t>(8, (budget - sa * slot_a) / slot_b);
-        while (sb < 3 && sa > 2) {
-            --sa;
-            sb = (int)std::min<size_t>(8, (budget - sa * slot_a) / slot_b);
-        }
-    }
-    if (const char* r = std::getenv("IPB_MV_RINGS")) {  // "a,b": explicit ring depths (tuning experiments)
-        int a = 0, b = 0;
-        if (std::sscanf(r, "%d,%d", &a, &b) == 2 && a >= 2 && b >= 2 && a * slot_a + b * slot_b <= budget) {
-            sa = a;
-            sb = b;
-        }
-    }
-    if (sa < 2 || sb < 2) return cudaErrorInvalidValue;
-    P.stages_a = sa;
-    P.stages_b = sb;
-    const size_t smem = 1024 + (size_t)sa * slot_a + (size_t)sb * slot_b + (2 * (size_t)(sa + sb) + 4) * 8 + 16;
+    P.stages = (int)std::min<size_t>(8, budget / stage_bytes);
+    if (P.stages < 2) return cudaErrorInvalidValue;
+    const size_t smem = 1024 + (size_t)P.stages * stage_bytes + (2 * P.stages + 4) * 8 + 16;
     cudaError_t e = allow_max_smem(mv_tc_kernel);
     if (e) return e;
     const int items = P.n_mtiles * P.n_kchunks;
