@@ -374,6 +374,57 @@ def serve_check(ib, srv, params, qbuf, plain_lat_ms, seconds=8.0):
             "bit_exact": all(r["mismatches"] == 0 and r["failed"] == 0 for r in rates)}
 
 
+def serve_saturated(ib, srv, params, qbuf, seconds=3.0, outstanding=128):
+    """The serving loop's capacity at batch 32: lane batches on two lanes
+    (one batch's Horner chains overlap the next batch's DB pass), closed
+    loop with `outstanding` requests always submitted, for `seconds`; wall
+    clock, host copies included.  Every response is compared with the plain
+    answer of its pool query."""
+    pool_n = min(32, len(qbuf))
+    alone = np.stack([srv.answer(qbuf[i]) for i in range(pool_n)])
+    views = [ib.query_view_from_flat(params, qbuf[i]) for i in range(pool_n)]
+    loop = ib.ServeLoop([srv], max_batch=32, lanes_per_db=2, queue_slots=outstanding + 32, scan_segments=0)
+    out = np.zeros(ib.response_u64s(params), np.uint64)
+    bad = done = 0
+    try:
+        from collections import deque
+        pend = deque()
+        k = 0
+
+        def submit():
+            nonlocal k
+            rc, t = loop.submit_view(0, views[k % pool_n])
+            assert rc == 0, (rc, ib.last_error())
+            pend.append((t, k % pool_n))
+            k += 1
+
+        for _ in range(outstanding):
+            submit()
+        t0 = time.perf_counter()
+        s0 = loop.stats()
+        while time.perf_counter() - t0 < seconds:
+            t, qi = pend.popleft()
+            loop.wait(t, out=out)
+            bad += not np.array_equal(out, alone[qi])
+            done += 1
+            submit()
+        wall = time.perf_counter() - t0
+        s1 = loop.stats()
+        while pend:
+            t, qi = pend.popleft()
+            loop.wait(t, out=out)
+            bad += not np.array_equal(out, alone[qi])
+        info = loop.db_info(0)
+    finally:
+        loop.close()
+    nb = s1["batches"] - s0["batches"]
+    return {"mode": "lane batches, 2 lanes, max_batch 32, closed loop", "outstanding": outstanding,
+            "seconds": seconds, "q_per_s": done / wall, "requests": done,
+            "mean_batch": (s1["batched_queries"] - s0["batched_queries"]) / max(1, nb),
+            "lanes": info["lanes"], "mismatches": bad, "bit_exact": bad == 0,
+            "timing": "wall clock over the loop's responses, host copies included (not CUDA events)"}
+
+
 def run_ours(args):
     import torch
     rank, local_rank, world = dist_env()
@@ -515,6 +566,7 @@ def run_ours(args):
     serving = None
     if rank == 0 and world == 1 and not args.no_serve_check:
         serving = serve_check(ib, srv, params, qbuf, lat)
+        serving["saturated"] = serve_saturated(ib, srv, params, qbuf)
 
     mv1 = st1["matvec"]
     db_bytes = R * Ccols * 2
