@@ -198,10 +198,10 @@ class ClockSampler:
 
 
 # DRAM bytes per algorithmic byte of mv_tc_kernel, from one ncu capture of a
-# batch-1 launch on the 1 GB geometry (dram__bytes_read.sum 1,074,672,384 +
-# dram__bytes_write.sum 4,067,840 for 1,074,266,112 algorithmic bytes); the
+# batch-1 launch on the 1 GB geometry (dram__bytes_read.sum 1,074,709,760 +
+# dram__bytes_write.sum 5,927,168 for 1,074,266,112 algorithmic bytes); the
 # kernel streams the DB once, so its traffic scales with the DB size.
-MV_TC_TRAFFIC_RATIO = (1074672384 + 4067840) / 1074266112
+MV_TC_TRAFFIC_RATIO = (1074709760 + 5927168) / 1074266112
 
 
 def measured_peaks():
