@@ -1,5 +1,6 @@
 // host_util.cpp -- host helpers of the B200 InsPIRe server: SHAKE-256 (FIPS
 // 202) for the CRS expansion, NTT tables, and setup() geometry.
+#include <cstdlib>
 #include "host_util.h"
 
 #include <cstring>
@@ -190,6 +191,12 @@ cudaError_t allow_max_dynamic_smem(const void* kernel, size_t* max_dynamic) {
     }
     if (max_dynamic) *max_dynamic = it->second;
     return cudaSuccess;
+}
+
+int test_abort_after_items() {
+    const char* v = std::getenv("IPB_TEST_ABORT_AFTER_ITEMS");
+    const int n = v ? std::atoi(v) : 0;
+    return n > 0 ? n : 0;
 }
 
 }  // namespace ipb

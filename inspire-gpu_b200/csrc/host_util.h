@@ -34,6 +34,10 @@ void build_tables(DevTables& T);
 int setup_geometry(size_t n_entries, size_t w, size_t db_rows, Params* out, const char** why);
 // Sets the calling thread's text for ipir_b200_last_error().
 void set_last_error(const char* msg);
+// Test hook for the tensor-core kernels' abort path: the value of
+// IPB_TEST_ABORT_AFTER_ITEMS (> 0: the MMA issuer stops after that many work
+// items and the launch reports a device wait failure), else 0.
+int test_abort_after_items();
 
 // Raises a kernel's dynamic shared-memory limit to the device's opt-in
 // maximum (less the kernel's static shared memory), once per kernel and

@@ -70,6 +70,8 @@ struct TcParams {
     const DevTables* T;
     int has_qmap;          // output row of pass query q: qmap[q] (else q)
     uint8_t qmap[32];
+    int abort_after;       // > 0: the MMA issuer stops after this many items and reports code 99 (a test of
+                           // the abort path, IPB_TEST_ABORT_AFTER_ITEMS); 0: off
 };
 
 __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ CUtensorMap map_a,
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
                 int item = -1;
-                if (!abort_flag && mbar_wait(&iempty[r], ((uint32_t)(it / kRing) & 1) ^ 1, P.err, 6)) {
+                if (!abort_flag && mbar_wait_ab(&iempty[r], ((uint32_t)(it / kRing) & 1) ^ 1, P.err, 6, &abort_flag)) {
                     const unsigned t = atomicAdd(P.tiles, 1u);
                     if (t < (unsigned)n_items) item = (int)t;
                 } else {
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                 const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
                 const int m0 = mt * kMT;
                 for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&empty[s], ph ^ 1, P.err, 1)) { abort_flag = 1; break; }
+                    if (!mbar_wait_ab(&empty[s], ph ^ 1, P.err, 1, &abort_flag)) { abort_flag = 1; break; }
                     uint8_t* st = smem + (size_t)s * stage_bytes;
                     mbar_expect_tx(&full[s], stage_bytes);
                     const int k0 = kc * P.kchunk_rows + kt * kKT;
@@ -162,15 +164,23 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
             bool it_mma = false;  // any MMA issued
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
-                if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 7)) { abort_flag = 1; break; }
+                if (!mbar_wait_ab(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 7, &abort_flag)) {
+                    abort_flag = 1;
+                    break;
+                }
                 const int item = item_ring[r];
                 mbar_arrive(&iempty[r]);
                 if (item < 0 || abort_flag) break;
-                if (!mbar_wait(&tempty[as], aph ^ 1, P.err, 3)) { abort_flag = 1; break; }
+                if (P.abort_after > 0 && it >= P.abort_after) {  // test hook: the designed early stop
+                    atomicCAS(P.err, 0, 99);
+                    abort_flag = 1;
+                    break;
+                }
+                if (!mbar_wait_ab(&tempty[as], aph ^ 1, P.err, 3, &abort_flag)) { abort_flag = 1; break; }
                 tc_fence_after();
                 const uint32_t d0 = tmem_base + (uint32_t)(as * 2 * P.npad);
                 for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&full[s], ph, P.err, 4)) { abort_flag = 1; break; }
+                    if (!mbar_wait_ab(&full[s], ph, P.err, 4, &abort_flag)) { abort_flag = 1; break; }
                     tc_fence_after();
                     const uint8_t* st = smem + (size_t)s * stage_bytes;
 #pragma unroll
@@ -208,11 +218,11 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
         const uint64_t cr0 = P.T->limb[0].cr, cr1 = P.T->limb[1].cr;
         for (int it = 0;; ++it) {
             const int r = it % kRing;
-            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 8)) { abort_flag = 1; break; }
+            if (!mbar_wait_ab(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 8, &abort_flag)) { abort_flag = 1; break; }
             const int item = item_ring[r];
             mbar_arrive(&iempty[r]);
             if (item < 0) break;
-            if (!mbar_wait(&tfull[as], aph, P.err, 5)) { abort_flag = 1; break; }
+            if (!mbar_wait_ab(&tfull[as], aph, P.err, 5, &abort_flag)) { abort_flag = 1; break; }
             tc_fence_after();
             const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
             for (int mb = 0; mb < 2; ++mb) {
@@ -419,6 +429,7 @@ cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, s
         for (int q = 0; q < nq; ++q) P.qmap[q] = qmap[q];
     P.nq = nq;
     P.npad = npad;
+    P.abort_after = test_abort_after_items();
     {
         const uint32_t qs[2] = {kQ0, kQ1};
         for (int l = 0; l < 2; ++l) {

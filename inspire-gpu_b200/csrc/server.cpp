@@ -617,20 +617,24 @@ static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
 
 // A kernel whose pipeline wait ran out of iterations leaves a code in the
 // device error word; report it (the responses are then not valid).
-void check_device_error(Lane& L) {
+void check_device_error(Lane& L, cudaStream_t st) {
     int e = 0;
-    IPB_CK(cudaMemcpy(&e, L.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    IPB_CK(cudaMemcpyAsync(&e, L.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    IPB_CK(cudaStreamSynchronize(st));
     if (e) {
-        IPB_CK(cudaMemset(L.d_err, 0, sizeof(int)));
+        IPB_CK(cudaMemsetAsync(L.d_err, 0, sizeof(int), st));  // ordered before the next batch's kernels
+        IPB_CK(cudaStreamSynchronize(st));
         throw std::runtime_error("device pipeline wait timed out (code " + std::to_string(e) + ")");
     }
 }
 
+// The error word is read first, once the batch has run: a batch whose
+// kernels stopped early writes nothing into the caller's buffer.
 static void fetch(Server* S, size_t count, uint64_t* out) {
     IPB_CK(cudaSetDevice(S->device));
+    check_device_error(S->lane, S->stream);
     IPB_CK(cudaMemcpyAsync(out, S->lane.resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, S->stream));
     IPB_CK(cudaStreamSynchronize(S->stream));
-    check_device_error(S->lane);
     if (S->timing && S->timed_slices)  // stage times summed over the batch's slices
         for (int i = 0; i < 5; ++i) {
             S->stage_ms[i] = 0.f;
@@ -734,8 +738,7 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
             }
             best.emplace_back(b, pick);
         }
-        IPB_CK(cudaStreamSynchronize(st));
-        check_device_error(L);
+        check_device_error(L, st);
     } catch (...) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -771,19 +774,22 @@ static void answer_wire(Server* S, const uint8_t* packed, size_t count, int fmt,
     IPB_CK(cudaMemcpyAsync(L.wire_in, packed, count * S->wire_q, cudaMemcpyHostToDevice, st));
     IPB_CK(launch_query_unpack(L.wire_in, S->wire_q, S->pp.db_rows, L.qraw, S->qstride, (int)count, P.tables, st));
     run_pipeline(S, count);
-    if (fmt == 0) {
-        IPB_CK(cudaMemcpyAsync(out, L.resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, st));
-    } else if (fmt == 1) {
+    const void* src = L.resp;
+    size_t bytes = count * S->resp_qstride * 8;
+    if (fmt == 1) {
         IPB_CK(launch_response_pack(L.resp, S->resp_qstride, S->pp.num_cts, L.wire_out, S->wire_r, (int)count,
                                     P.tables, st));
-        IPB_CK(cudaMemcpyAsync(out, L.wire_out, count * S->wire_r, cudaMemcpyDeviceToHost, st));
-    } else {
+        src = L.wire_out;
+        bytes = count * S->wire_r;
+    } else if (fmt == 2) {
         IPB_CK(launch_response_compress(L.resp, S->resp_qstride, S->pp.num_cts, L.codec_tmp, L.wire_out, S->wire_c,
                                         (int)count, P.tables, st));
-        IPB_CK(cudaMemcpyAsync(out, L.wire_out, count * S->wire_c, cudaMemcpyDeviceToHost, st));
+        src = L.wire_out;
+        bytes = count * S->wire_c;
     }
+    check_device_error(L, st);  // nothing is written if a kernel stopped early
+    IPB_CK(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, st));
     IPB_CK(cudaStreamSynchronize(st));
-    check_device_error(L);
 }
 
 static int validate_batch(const Server* S, const ipir_query_view* qs, size_t count, const void* out) {
@@ -1410,12 +1416,14 @@ int ipir_b200_matvec_ex(const uint16_t* db, size_t rows, size_t cols, const uint
                                                        s));
             }
             if (sync) {
+                int e = 0;  // read and cleared on the caller's stream, after the launches above
+                IPB_CK(cudaMemcpyAsync(&e, M.err, sizeof(int), cudaMemcpyDeviceToHost, s));
                 IPB_CK(cudaStreamSynchronize(s));
-                int e = 0;
-                IPB_CK(cudaMemcpy(&e, M.err, sizeof(int), cudaMemcpyDeviceToHost));
                 if (e) {
-                    IPB_CK(cudaMemset(M.err, 0, sizeof(int)));
-                    ipb::g_last_error = "ipir_b200_matvec: device pipeline wait timed out";
+                    IPB_CK(cudaMemsetAsync(M.err, 0, sizeof(int), s));
+                    IPB_CK(cudaStreamSynchronize(s));
+                    ipb::g_last_error = "ipir_b200_matvec: a kernel's pipeline wait timed out or it stopped early "
+                                        "(code " + std::to_string(e) + ")";
                     return 5;
                 }
             }

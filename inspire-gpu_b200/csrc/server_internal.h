@@ -203,8 +203,9 @@ int run_db_phase(const Server& S, Lane& L, const Sched& sc, size_t q_off, size_t
 // H2D of parts [p0, p0 + np) (0, 1: LWE limbs, 2: KSK5, 3: KSK-1, 4: RGSW) of
 // each query into the handle's lane, one copy per contiguous host run.
 void stage_parts(const Server& S, const ipir_query_view* qs, size_t count, int p0, int np, cudaStream_t st);
-// Throws (and clears the word) if a kernel's bounded wait ran out.
-void check_device_error(Lane& L);
+// Waits for the work enqueued on st, then throws (and clears the word, on
+// st) if a kernel's bounded wait ran out or a kernel stopped early.
+void check_device_error(Lane& L, cudaStream_t st);
 // Geometry of the group shard [g0, g1) of a database (its column slab).
 Params shard_params(const Params& global, size_t g0, size_t g1);
 // gpu_preprocess of the group shard [g0, g1) of the host DB db (global

@@ -135,10 +135,10 @@ int ipir_b200_shard_pack(ipir_shard* sh, const ipir_query_view* queries, size_t 
             S->launches += (unsigned long long)ipb::run_db_phase(*S, L, sc, q0, std::min(slice, count - q0),
                                                                  S->stream, nullptr, nullptr, 1);
         }
+        ipb::check_device_error(L, S->stream);  // nothing is written if a kernel stopped early
         IPB_CK(cudaMemcpyAsync(out_packed_b, L.packed_b, count * S->pb_qstride * 4, cudaMemcpyDeviceToDevice,
                                S->stream));
         IPB_CK(cudaStreamSynchronize(S->stream));
-        ipb::check_device_error(L);
         return 0;
     });
 }
@@ -195,9 +195,9 @@ int ipir_b200_horner_answer(ipir_horner* h, const uint32_t* packed_b, const ipir
                                 L.resp + q0 * S->resp_qstride, n, L.d_err, S->stream);
         }
         S->launches += 1 + ns;
+        ipb::check_device_error(L, S->stream);
         IPB_CK(cudaMemcpyAsync(out_resp, L.resp, count * S->resp_qstride * 8, cudaMemcpyDeviceToHost, S->stream));
         IPB_CK(cudaStreamSynchronize(S->stream));
-        ipb::check_device_error(L);
         return 0;
     });
 }

@@ -40,6 +40,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int* err
     atomicCAS(err, 0, code);
     return false;
 }
+// The same, and also false (without touching *err) as soon as *abort is set
+// by another role of the CTA, so that after one role stops every other role
+// leaves its loop at once instead of running out its own limit.
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t* b, uint32_t parity, int* err, int code,
+                                             const volatile int* abort) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+        if (mbar_try(b, parity)) return true;
+        if (*abort) return false;
+    }
+    atomicCAS(err, 0, code);
+    return false;
+}
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(

@@ -194,6 +194,8 @@ struct TpParams {
     uint32_t c[2][7];      // 256^k mod q_l
     uint64_t cr[2];
     uint32_t q[2];
+    int abort_after;       // > 0: the MMA issuer stops after this many items and reports code 99 (a test of
+                           // the abort path, IPB_TEST_ABORT_AFTER_ITEMS); 0: off
 };
 
 __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_constant__ CUtensorMap map_a, TpParams P) {
@@ -273,11 +275,11 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
         uint32_t aph = 0;
         for (int it = 0;; ++it) {
             const int r = it % kRing;
-            if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 18)) { abort_flag = 1; break; }
+            if (!mbar_wait_ab(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 18, &abort_flag)) { abort_flag = 1; break; }
             const int item = item_ring[r];
             mbar_arrive(&iempty[r]);
             if (item < 0) break;
-            if (!mbar_wait(&tfull[as], aph, P.err, 15)) { abort_flag = 1; break; }
+            if (!mbar_wait_ab(&tfull[as], aph, P.err, 15, &abort_flag)) { abort_flag = 1; break; }
             tc_fence_after();
             const int li0 = P.li0 + (item / P.n_mg) * P.spi, mg = item % P.n_mg;
             const int l = li0 / kN;
@@ -336,7 +338,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
                 int item = -1;
-                if (!abort_flag && mbar_wait(&iempty[r], ((uint32_t)(it / kRing) & 1) ^ 1, P.err, 16)) {
+                if (!abort_flag && mbar_wait_ab(&iempty[r], ((uint32_t)(it / kRing) & 1) ^ 1, P.err, 16, &abort_flag)) {
                     const unsigned t = atomicAdd(P.tiles, 1u);
                     if (t < (unsigned)n_items) item = (int)t;
                 } else {
@@ -348,7 +350,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                 const int li = P.li0 + (item / P.n_mg) * P.spi, mg = item % P.n_mg;
                 const int rowa = li * slot_rows + mg * P.mti * 128;
                 for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&empty[s], ph ^ 1, P.err, 11)) { abort_flag = 1; break; }
+                    if (!mbar_wait_ab(&empty[s], ph ^ 1, P.err, 11, &abort_flag)) { abort_flag = 1; break; }
                     uint8_t* st = smem + (size_t)s * stage_bytes;
                     mbar_expect_tx(&full[s], tx_bytes);
                     for (int mt = 0; mt < P.mti; ++mt)
@@ -377,15 +379,20 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
             bool any_mma = false;
             for (int it = 0;; ++it) {
                 const int r = it % kRing;
-                if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 17)) { abort_flag = 1; break; }
+                if (!mbar_wait_ab(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 17, &abort_flag)) { abort_flag = 1; break; }
                 const int item = item_ring[r];
                 mbar_arrive(&iempty[r]);
                 if (item < 0 || abort_flag) break;
-                if (!mbar_wait(&tempty[as], aph ^ 1, P.err, 13)) { abort_flag = 1; break; }
+                if (P.abort_after > 0 && it >= P.abort_after) {  // test hook: the designed early stop
+                    atomicCAS(P.err, 0, 99);
+                    abort_flag = 1;
+                    break;
+                }
+                if (!mbar_wait_ab(&tempty[as], aph ^ 1, P.err, 13, &abort_flag)) { abort_flag = 1; break; }
                 tc_fence_after();
                 const uint32_t d0 = tmem_base + (uint32_t)(as * acc_cols);
                 for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait(&full[s], ph, P.err, 14) || !mbar_wait(&bfull[s], ph, P.err, 21)) {
+                    if (!mbar_wait_ab(&full[s], ph, P.err, 14, &abort_flag) || !mbar_wait_ab(&bfull[s], ph, P.err, 21, &abort_flag)) {
                         abort_flag = 1;
                         break;
                     }
@@ -445,7 +452,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
             int base = 0;  // stages issued before this item
             for (int it = 0;; ++it, base += ktiles) {
                 const int r = it % kRing;
-                if (!mbar_wait(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 19)) { abort_flag = 1; break; }
+                if (!mbar_wait_ab(&ifull[r], (uint32_t)(it / kRing) & 1, P.err, 19, &abort_flag)) { abort_flag = 1; break; }
                 const int item = item_ring[r];
                 mbar_arrive(&iempty[r]);
                 if (item < 0) break;
@@ -455,7 +462,7 @@ __global__ void __launch_bounds__(kTpThreads, 1) tp_tc_kernel(const __grid_const
                 for (int kt = grp; grp < ngrp && kt < ktiles; kt += ngrp) {
                     const int seq = base + kt, s = seq % S;
                     const uint32_t ph = (uint32_t)(seq / S) & 1;
-                    if (!mbar_wait(&empty[s], ph ^ 1, P.err, 20)) { abort_flag = 1; break; }
+                    if (!mbar_wait_ab(&empty[s], ph ^ 1, P.err, 20, &abort_flag)) { abort_flag = 1; break; }
                     uint8_t* bt = smem + (size_t)s * stage_bytes + a_region;
                     for (int unit = gk; unit < units; unit += kKeyGroup) {
                         const int u4 = unit & 31, sq = unit >> 5;
@@ -628,6 +635,7 @@ cudaError_t launch_tensor_pass_slots(const uint8_t* Dt, size_t G, int li0, int n
     P.tmem_cols = tc;
     P.err = err;
     P.tiles = tiles;
+    P.abort_after = test_abort_after_items();
     const uint32_t qs[2] = {kQ0, kQ1};
     for (int l = 0; l < 2; ++l) {
         for (int k = 0; k < 7; ++k) P.c[l][k] = powmod_host(256, k, qs[l]);
