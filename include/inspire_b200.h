@@ -436,6 +436,14 @@ int ipir_b200_shard_export_a(const ipir_shard* shard, uint32_t* out);
  * Blocking.  Returns 0, 1 null argument, 2 count > max_batch, 3 null view
  * field, 4 CUDA error or device wait timeout. */
 int ipir_b200_shard_pack(ipir_shard* shard, const ipir_query_view* queries, size_t count, uint32_t* out_packed_b);
+/* For a database of several response ciphertexts, a shard whose groups
+ * cover whole Horner chunks (group_lo a multiple of min(D, n_packed), and
+ * group_hi one too or n_packed) answers its own ciphertexts with no
+ * exchange: out_resp[count][its ciphertexts][a|b][limb][N] u64 (NTT form),
+ * ciphertexts (group_lo / D_act) onward; a query's full response is the
+ * shards' parts in group order.  Returns ipir_answer_batch's codes, or 6
+ * when the range does not cover whole ciphertexts. */
+int ipir_b200_shard_answer(ipir_shard* shard, const ipir_query_view* queries, size_t count, uint64_t* out_resp);
 void ipir_b200_shard_destroy(ipir_shard* shard);
 
 /* The Horner owner of a sharded database (params as ipir_b200_shard_create

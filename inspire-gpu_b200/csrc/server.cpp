@@ -802,13 +802,25 @@ static int validate_batch(const Server* S, const ipir_query_view* qs, size_t cou
     return 0;
 }
 
+bool shard_whole_cts(const Params& global, size_t g0, size_t g1) {
+    const size_t d_act = std::min(global.D, global.n_packed);
+    return g0 % d_act == 0 && (g1 % d_act == 0 || g1 == global.n_packed);
+}
+
 Params shard_params(const Params& global, size_t g0, size_t g1) {
     if (g1 <= g0 || g1 > global.n_packed) throw std::invalid_argument("group shard: need 0 <= lo < hi <= n_packed");
     Params p = global;
     p.db_cols = (g1 - g0) * kN;
     p.n_packed = g1 - g0;
-    p.D = p.n_packed;  // a shard runs no Horner chain
-    p.num_cts = 1;
+    if (shard_whole_cts(global, g0, g1)) {
+        // whole Horner chunks: the shard's own pipeline answers its ciphertexts
+        const size_t d_act = std::min(global.D, global.n_packed);
+        p.D = global.D;
+        p.num_cts = (p.n_packed + d_act - 1) / d_act;
+    } else {
+        p.D = p.n_packed;  // packs only: the Horner chains run on the owner
+        p.num_cts = 1;
+    }
     return p;
 }
 

@@ -206,7 +206,10 @@ void stage_parts(const Server& S, const ipir_query_view* qs, size_t count, int p
 // Waits for the work enqueued on st, then throws (and clears the word, on
 // st) if a kernel's bounded wait ran out or a kernel stopped early.
 void check_device_error(Lane& L, cudaStream_t st);
-// Geometry of the group shard [g0, g1) of a database (its column slab).
+// Whether [g0, g1) covers whole Horner chunks (response ciphertexts).
+bool shard_whole_cts(const Params& global, size_t g0, size_t g1);
+// Geometry of the group shard [g0, g1) of a database (its column slab);
+// for whole chunks its D and num_cts are those of its own ciphertexts.
 Params shard_params(const Params& global, size_t g0, size_t g1);
 // gpu_preprocess of the group shard [g0, g1) of the host DB db (global
 // geometry): the encoded column slab and the shard's tensors.

@@ -143,6 +143,18 @@ int ipir_b200_shard_pack(ipir_shard* sh, const ipir_query_view* queries, size_t 
     });
 }
 
+int ipir_b200_shard_answer(ipir_shard* sh, const ipir_query_view* queries, size_t count, uint64_t* out_resp) {
+    if (!sh || !queries || !out_resp) return 1;
+    if (!ipb::shard_whole_cts(sh->global, sh->g0, sh->g1)) {
+        ipb::set_last_error("ipir_b200_shard_answer: the shard's groups do not cover whole response ciphertexts");
+        return 6;
+    }
+    // the shard handle is a server over its own groups: the plain pipeline
+    // (with its Horner chains) answers its ciphertexts
+    ipir_server tmp{sh->s};
+    return ipir_answer_batch(&tmp, queries, count, out_resp);
+}
+
 void ipir_b200_shard_destroy(ipir_shard* sh) {
     if (!sh) return;
     ipb::DeviceRestore keep_device;

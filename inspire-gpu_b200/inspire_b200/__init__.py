@@ -148,6 +148,8 @@ _L.ipir_b200_shard_export_a.restype = C.c_int
 _L.ipir_b200_shard_pack.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
 _L.ipir_b200_shard_pack.restype = C.c_int
 _L.ipir_b200_shard_destroy.argtypes = [C.c_void_p]
+_L.ipir_b200_shard_answer.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, u64p]
+_L.ipir_b200_shard_answer.restype = C.c_int
 _L.ipir_b200_horner_create.restype = C.c_void_p
 _L.ipir_b200_horner_create.argtypes = [C.c_void_p, u32p, C.c_size_t]
 _L.ipir_b200_horner_answer.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, u64p, C.c_void_p]
@@ -186,7 +188,7 @@ EXPORTED = [
     "ipir_serve_replace_db", "ipir_b200_save_server", "ipir_b200_load_server",
     "ipir_b200_kernel_binary_version", "ipir_b200_shard_create", "ipir_b200_shard_export_a",
     "ipir_b200_shard_pack", "ipir_b200_shard_destroy", "ipir_b200_horner_create", "ipir_b200_horner_answer",
-    "ipir_b200_horner_destroy", "ipir_b200_synth_queries", "ipir_b200_horner_eval",
+    "ipir_b200_horner_destroy", "ipir_b200_synth_queries", "ipir_b200_horner_eval", "ipir_b200_shard_answer",
 ]
 
 
@@ -701,6 +703,23 @@ def matvec_noalloc_rc(db_ptr, rows, cols, queries_ptr, count, out_ptr, stream=0)
 
 
 # ------------------------------------------------------------------ group shards
+def chunk_ranges(n_packed, d_act, world):
+    """Group ranges of whole Horner chunks (response ciphertexts) over
+    `world` GPUs, contiguous and as even as possible, for databases of at
+    least `world` ciphertexts: every rank answers its ciphertexts, with no
+    exchange before Horner."""
+    n_cts = -(-n_packed // d_act)
+    if world < 1 or world > n_cts:
+        raise ValueError(f"cannot split {n_cts} ciphertexts over {world} shards")
+    base, extra = divmod(n_cts, world)
+    out, c = [], 0
+    for r in range(world):
+        c1 = c + base + (1 if r < extra else 0)
+        out.append((c * d_act, min(n_packed, c1 * d_act)))
+        c = c1
+    return out
+
+
 def group_ranges(n_packed, world):
     """Contiguous group ranges [lo, hi) of a database split over `world`
     GPUs, as equal as possible (the first n_packed % world get one more)."""
@@ -759,6 +778,27 @@ class Shard:
         rc = _L.ipir_b200_shard_pack(self._h, arr, len(keep), C.c_void_p(out_ptr))
         if rc:
             raise InspireError(f"shard_pack rc={rc}: {last_error()}")
+
+    def cts(self):
+        """Response ciphertexts this shard answers itself (0 if its range does
+        not cover whole Horner chunks)."""
+        d_act = min(self.params["interp_d"], self.params["n_packed"])
+        whole = self.lo % d_act == 0 and (self.hi % d_act == 0 or self.hi == self.params["n_packed"])
+        return -(-self.groups // d_act) if whole else 0
+
+    def answer(self, queries, out=None):
+        """Its own ciphertexts of each query's response (whole-chunk shards):
+        (count, cts * 4 N) u64."""
+        keep = [np.ascontiguousarray(q, np.uint64) for q in queries]
+        arr = (IpirQueryView * max(1, len(keep)))()
+        for i, f in enumerate(keep):
+            arr[i] = query_view_from_flat(self.params, f)
+        if out is None:
+            out = np.zeros((len(keep), self.cts() * 4 * RING_N), np.uint64)
+        rc = _L.ipir_b200_shard_answer(self._h, arr, len(keep), _ptr(out, u64p))
+        if rc:
+            raise InspireError(f"shard_answer rc={rc}: {last_error()}")
+        return out
 
     def close(self):
         if self._h:

@@ -77,3 +77,36 @@ def test_sharded_server_on_a_one_rank_nccl_group():
         assert (got == want).all()
     finally:
         dist.destroy_process_group()
+
+
+def test_whole_chunk_shards_answer_their_own_ciphertexts():
+    """A database of two response ciphertexts (G = 512 groups, D = 256) in
+    two shards of whole Horner chunks: each answers its own ciphertext with
+    no exchange, and the two side by side are the whole server's response;
+    a shard that does not cover whole chunks refuses (code 6)."""
+    import inspire_b200 as ib
+    c = get_case("g512")
+    qs = [c.query(i, 990 + k)[0] for k, i in enumerate([11, 33554431])]
+    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=2, crs_seed=c.seed)
+    try:
+        want = srv.answer_batch(qs)
+    finally:
+        srv.close()
+    ranges = ib.chunk_ranges(c.G, min(c.D, c.G), 2)
+    assert ranges == [(0, 256), (256, 512)]
+    parts = []
+    for lo, hi in ranges:
+        sh = ib.Shard(c.n_entries, c.w, c.db, lo, hi, c.seed, db_rows=2048, max_batch=2)
+        try:
+            assert sh.cts() == 1
+            parts.append(sh.answer(qs))
+        finally:
+            sh.close()
+    assert (np.concatenate(parts, axis=1) == want).all()
+    sh = ib.Shard(c.n_entries, c.w, c.db, 0, 100, c.seed, db_rows=2048, max_batch=2)
+    try:
+        assert sh.cts() == 0
+        with pytest.raises(ib.InspireError, match="rc=6"):
+            sh.answer(qs)
+    finally:
+        sh.close()

@@ -107,3 +107,43 @@ def test_sharded_gather_reproduces_the_single_process_answer(tmp_path, case, wor
     for p, out in zip(procs, outs):
         assert p.returncode == 0, out[-3000:]
     assert "RANK0 ok" in outs[0]
+
+
+CHUNK_WORKER = r"""
+import datetime, os, sys
+sys.path.insert(0, os.path.join({repo!r}, "inspire-gpu_b200"))
+import numpy as np, torch.distributed as dist
+from inspire_b200 import chunk_ranges
+from inspire_b200.sharded import gather_responses
+rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+ranges = chunk_ranges(1300, 256, world)          # 6 ciphertexts, the last of 20 groups
+cts = [-(-(h - l) // 256) for l, h in ranges]
+full = np.random.default_rng(1).integers(0, 2 ** 27, (3, 6 * 4 * 2048), dtype=np.uint64)
+lo_ct = ranges[rank][0] // 256
+own = full[:, lo_ct * 4 * 2048:(lo_ct + cts[rank]) * 4 * 2048]
+got = gather_responses(own, cts, rank, 0, dist)
+if rank == 0:
+    assert sum(cts) == 6 and ranges[-1][1] == 1300
+    assert (got == full).all()
+    print("RANK0 ok", flush=True)
+dist.barrier()
+dist.destroy_process_group()
+"""
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_chunk_shards_gather_responses_in_ciphertext_order(tmp_path, world):
+    script = tmp_path / "chunk_worker.py"
+    script.write_text(CHUNK_WORKER.format(repo=REPO))
+    port = _free_port()
+    procs = []
+    for rank in range(world):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(world),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, str(script)], env=env, stdout=subprocess.PIPE,
+                                      stderr=subprocess.STDOUT, text=True))
+    outs = [p.communicate(timeout=120)[0] for p in procs]
+    for p, out in zip(procs, outs):
+        assert p.returncode == 0, out[-3000:]
+    assert "RANK0 ok" in outs[0]
