@@ -304,7 +304,7 @@ def line_config(params, B, world):
     """The `config` both arms report (the same workload)."""
     db_bytes = params["db_rows"] * params["db_cols"] * 2
     return {"workload": describe(params) + f"; batch {B}",
-            "model": "InsPIRe PIR server", "global_batch": B * world, "seq_len": 0,
+            "server": "InsPIRe PIR server", "global_batch": B * world,
             "parallelism": f"replicas x{world}",
             "l2": f"inputs larger than L2 ({db_bytes / 1e9:.1f} GB DB read per step)"}
 
@@ -333,7 +333,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC,
             "value": v, "unit": "q/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32/u64 modular (exact)", "data": "synthetic",
+            "dtype": "u64 mod q (exact, u128 dot products)", "data": "synthetic",
             "config": line_config(params, args.batch, 1),
             "queries_per_step": 1,
             "ms_per_step_p50": statistics.median(ts) * 1e3, "fill_s": cq.fill_s,
@@ -580,7 +580,7 @@ def run_ours(args):
         "metric": METRIC,
         "value": value, "unit": "q/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": msB, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u32/u64 modular (exact)", "data": "synthetic",
+        "dtype": "u32 mod q (exact: int8 limb MMAs with s32 accumulation, u64 reductions)", "data": "synthetic",
         "config": line_config(params, B, world),
         "plain_b1": {"q_per_s": 1000.0 / ms1, "ms": ms1, "p50_ms_e2e": p50, "p99_ms_e2e": p99},
         "served": {"batch": B, "ms_per_batch": msB, "q_per_s": value / world},
