@@ -51,6 +51,7 @@ namespace inspire {
 struct GpuServerCtx {
     inspire_b200::GpuServerCtx* s = nullptr;
     PublicParams pp;
+    size_t max_batch = 0;
     std::vector<uint64_t> flat;  // staging for one batch of flattened queries
     std::vector<uint64_t> resp;  // flat responses of one batch
 };
@@ -182,6 +183,7 @@ GpuServerCtx* gpu_setup_server(const PublicParams& pp, const PreprocessData& pre
         throw;
     }
     ctx->pp = pp;
+    ctx->max_batch = cfg.max_batch;
     // Ownership moved to the context: clear the caller's pointers, as the
     // reference does (src/gpu_protocol.cu:856-885).
     PreprocessData& mut = const_cast<PreprocessData&>(precomp);
@@ -212,7 +214,7 @@ std::vector<std::vector<RlweCt>> gpu_answer_batch(GpuServerCtx* ctx, const Query
     if (!ctx) throw std::invalid_argument("gpu_answer_batch: null ctx");
     if (count == 0) return {};
     if (!queries) throw std::invalid_argument("gpu_answer_batch: null queries");
-    if (count > inspire_b200::gpu_server_caps(ctx->s).max_batch)
+    if (count > ctx->max_batch)
         throw std::invalid_argument("gpu_answer_batch: count exceeds max_batch (set GpuServerConfig.max_batch)");
     // All or nothing: every query is validated and flattened before any
     // device work; one host array, so each part side crosses in one copy.
