@@ -96,15 +96,25 @@ cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_
 
 // Same on a cluster of four CTAs per chain (one per polynomial and limb);
 // *err receives a nonzero code if a wait for a peer's data times out.
+// A sub-range of a Horner chain (one ciphertext's groups, i = d_act - 1 .. 0):
+// i_first < 0 starts from the top (acc = packed[d_act - 1], then
+// i = d_act - 2), else the chain resumes from acc in state and runs
+// i = i_first .. i_last; i_last == 0 ends it (the response is written),
+// else acc goes to state [query][ct][a|b][limb][N] u32 for the next range.
+struct HornerRange {
+    long i_first = -1;
+    long i_last = 0;
+    uint32_t* state = nullptr;
+};
 cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                                   size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
-                                  cudaStream_t s);
+                                  cudaStream_t s, HornerRange hr = HornerRange{});
 // Same on a cluster of eight CTAs per chain (polynomial x limb x digit).
 cudaError_t launch_horner_cluster8(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
                                    const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                                    size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
-                                   cudaStream_t s);
+                                   cudaStream_t s, HornerRange hr = HornerRange{});
 
 // ---------------------------------------------------------------- wire codecs (codec.cu)
 // Byte sizes of the client library's formats: packed query, packed

@@ -361,7 +361,7 @@ __device__ __forceinline__ bool hb_wait(uint64_t* b, uint32_t parity, int* err, 
 __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
     horner_cl_kernel(const uint32_t* __restrict__ pre_a, const uint32_t* __restrict__ packed_b, size_t pb_qstride,
                      const uint32_t* __restrict__ rgsw32, const DevTables* __restrict__ T, size_t groups,
-                     size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride, int* err) {
+                     size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride, int* err, HornerRange hr) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint2* twf = reinterpret_cast<uint2*>(smem);
     uint2* twi = twf + kN;
@@ -409,14 +409,16 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
         r_oth_p[e] = (uint32_t)(((uint64_t)r_oth[e] << 32) / q);
     }
     uint32_t acc[8];
-    if (gp == 0) ld8(src_of(start + len - 1) + 8 * t, acc);
+    uint32_t* const st_part = hr.state + (((size_t)b * (gridDim.x >> 2) + ct) * 4 + p * 2 + l) * kN;
+    if (gp == 0) ld8((hr.i_first < 0 ? src_of(start + len - 1) : st_part) + 8 * t, acc);
+    const long i_first = hr.i_first < 0 ? (long)len - 2 : (long)hr.i_first;
     cluster_sync_all();  // every CTA runs and its mbarriers are initialised before any remote access
     const uint32_t peer_x = map_peer(xc, rank_limb);       // partner's xc base
     const uint32_t peer_c = map_peer(cin, rank_poly);      // other poly CTA's cin base
     const uint32_t peer_mbx = map_peer(mbx, rank_limb);
     const uint32_t peer_mbc = map_peer(mbc, rank_poly);
     int step = 0;
-    for (long i = (long)len - 2; i >= 0; --i, ++step) {
+    for (long i = i_first; i >= (long)hr.i_last; --i, ++step) {
         const int par = step & 1;
         const uint32_t ph = (uint32_t)(step >> 1) & 1;
         uint32_t* xown = xc + (par * 2 + 0) * kN;
@@ -476,11 +478,13 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 1)
                 acc[e] = add_mod(add_mod(add_mod(v0[e], v1[e], q), add_mod(w0[e], w1[e], q), q), pk[e], q);
         }
     }
-    if (gp == 0) {
+    if (gp == 0 && hr.i_last == 0) {
         uint64_t* dst = resp + (size_t)b * resp_qstride + ((size_t)ct * 4 + p * 2 + l) * kN + 8 * t;
 #pragma unroll
         for (int e = 0; e < 8; e += 2)
             *reinterpret_cast<ulonglong2*>(dst + e) = make_ulonglong2(acc[e], acc[e + 1]);
+    } else if (gp == 0) {
+        st8(st_part + 8 * t, acc);  // the chain resumes from here in the next launch
     }
     cluster_sync_all();  // no CTA leaves while a peer may still write into its shared memory
 }
@@ -507,7 +511,7 @@ constexpr size_t kHornerCl8Smem =
 __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
     horner_cl8_kernel(const uint32_t* __restrict__ pre_a, const uint32_t* __restrict__ packed_b, size_t pb_qstride,
                       const uint32_t* __restrict__ rgsw32, const DevTables* __restrict__ T, size_t groups,
-                      size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride, int* err) {
+                      size_t d_act, uint64_t* __restrict__ resp, size_t resp_qstride, int* err, HornerRange hr) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint2* twf = reinterpret_cast<uint2*>(smem);
     uint2* twi = twf + kN;
@@ -554,7 +558,9 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
         r_oth_p[e] = (uint32_t)(((uint64_t)r_oth[e] << 32) / q);
     }
     uint32_t acc[8];
-    ld8(src_of(start + len - 1) + 8 * t, acc);
+    uint32_t* const st_part = hr.state + (((size_t)b * (gridDim.x >> 3) + ct) * 4 + p * 2 + l) * kN;
+    ld8((hr.i_first < 0 ? src_of(start + len - 1) : st_part) + 8 * t, acc);
+    const long i_first = hr.i_first < 0 ? (long)len - 2 : (long)hr.i_first;
     cluster_sync_all();  // every CTA runs and its mbarriers are initialised before any remote access
     const uint32_t peer_x = map_peer(xc, rank_limb);
     const uint32_t peer_mbx = map_peer(mbx, rank_limb);
@@ -562,7 +568,7 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
     const uint32_t o0_c = map_peer(cin, rank_o0), o0_mbc = map_peer(mbc, rank_o0);
     const uint32_t o1_c = map_peer(cin, rank_o1), o1_mbc = map_peer(mbc, rank_o1);
     int step = 0;
-    for (long i = (long)len - 2; i >= 0; --i, ++step) {
+    for (long i = i_first; i >= (long)hr.i_last; --i, ++step) {
         const int par = step & 1;
         const uint32_t ph = (uint32_t)(step >> 1) & 1;
         uint32_t* xown = xc + (par * 2 + 0) * kN;
@@ -618,11 +624,13 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(256, 1)
         for (int e = 0; e < 8; ++e)
             acc[e] = add_mod(add_mod(add_mod(es[e], v1[e], q), add_mod(w0[e], w1[e], q), q), pk[e], q);
     }
-    if (j == 0) {
+    if (j == 0 && hr.i_last == 0) {
         uint64_t* dst = resp + (size_t)b * resp_qstride + ((size_t)ct * 4 + p * 2 + l) * kN + 8 * t;
 #pragma unroll
         for (int e = 0; e < 8; e += 2)
             *reinterpret_cast<ulonglong2*>(dst + e) = make_ulonglong2(acc[e], acc[e + 1]);
+    } else if (j == 0) {
+        st8(st_part + 8 * t, acc);  // the chain resumes from here in the next launch
     }
     cluster_sync_all();  // no CTA leaves while a peer may still write into its shared memory
 }
@@ -798,28 +806,35 @@ cudaError_t launch_horner(const uint32_t* pre_a, const uint32_t* packed_b, size_
     return cudaGetLastError();
 }
 
+static bool horner_range_ok(const HornerRange& hr, size_t d_act) {
+    if (hr.i_first < 0 && hr.i_last == 0) return true;  // the whole chain
+    return hr.state && hr.i_last >= 0 && hr.i_first < (long)d_act - 1 && (hr.i_first < 0 || hr.i_first >= hr.i_last);
+}
+
 cudaError_t launch_horner_cluster(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
                                   const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                                   size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, HornerRange hr) {
     if (nq <= 0) return cudaSuccess;
+    if (!horner_range_ok(hr, d_act)) return cudaErrorInvalidValue;
     cudaError_t e = allow_max_smem(horner_cl_kernel);
     if (e) return e;
     horner_cl_kernel<<<dim3((unsigned)(4 * num_cts), nq), 512, kHornerClSmem, s>>>(pre_a, packed_b, pb_qstride,
                                                                                    rgsw32, T, groups, d_act, resp,
-                                                                                   resp_qstride, err);
+                                                                                   resp_qstride, err, hr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_horner_cluster8(const uint32_t* pre_a, const uint32_t* packed_b, size_t pb_qstride,
                                    const uint32_t* rgsw32, const DevTables* T, size_t groups, size_t d_act,
                                    size_t num_cts, uint64_t* resp, size_t resp_qstride, int nq, int* err,
-                                   cudaStream_t s) {
+                                   cudaStream_t s, HornerRange hr) {
     if (nq <= 0) return cudaSuccess;
+    if (!horner_range_ok(hr, d_act)) return cudaErrorInvalidValue;
     cudaError_t e = allow_max_smem(horner_cl8_kernel);
     if (e) return e;
     horner_cl8_kernel<<<dim3((unsigned)(8 * num_cts), nq), 256, kHornerCl8Smem, s>>>(
-        pre_a, packed_b, pb_qstride, rgsw32, T, groups, d_act, resp, resp_qstride, err);
+        pre_a, packed_b, pb_qstride, rgsw32, T, groups, d_act, resp, resp_qstride, err, hr);
     return cudaGetLastError();
 }
 

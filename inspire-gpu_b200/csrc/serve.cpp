@@ -926,6 +926,7 @@ int ipir_serve_db_info(ipir_serve* sv, size_t db, size_t* lanes, size_t* max_bat
             sched[c].horner_cluster = d.sched[c].horner_cluster;
             sched[c].tp_sms = d.sched[c].tp_sms;
             sched[c].slice = d.sched[c].slice;
+            sched[c].hchunks = d.sched[c].hchunks;
         }
     return 0;
 }

@@ -244,6 +244,9 @@ void alloc_lane(const Server& S, Lane& L, size_t cap, int gt_pass) {
     IPB_CK(cudaEventCreateWithFlags(&L.fork, cudaEventDisableTiming));
     IPB_CK(cudaEventCreateWithFlags(&L.join, cudaEventDisableTiming));
     IPB_CK(cudaEventCreateWithFlags(&L.rgsw_ready, cudaEventDisableTiming));
+    IPB_CK(cudaStreamCreateWithFlags(&L.hstream, cudaStreamNonBlocking));
+    IPB_CK(cudaEventCreateWithFlags(&L.hjoin, cudaEventDisableTiming));
+    for (auto& e : L.hev) IPB_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     // Defined contents before any pipeline run (the autotuner runs on them).
     IPB_CK(cudaMemset(L.qraw, 0, cap * S.qstride * 8));
     IPB_CK(cudaMemset(L.planes, 0, mv_tc_planes_bytes(R, (int)cap)));
@@ -477,6 +480,79 @@ static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t q_
     return 1;
 }
 
+// Whether a batch of `count` can run with its Horner chunks trailing the DB
+// pass (Sched::hchunks): one ciphertext, one slice, the tensor-core mat-vec
+// and a cluster Horner kernel (those resume a chain from memory).
+static bool chunked_ok(const Server& S, const Sched& sc, size_t count) {
+    return sc.hchunks > 1 && sc.matvec_tc && sc.horner_cluster != 0 && sc.tp_sms == 0 && S.pp.num_cts == 1 &&
+           S.pp.n_packed <= S.pp.D && count <= kSliceQueries && S.pp.n_packed >= 2;
+}
+
+// The plain pipeline with the Horner chain trailing the DB pass.  The
+// tensor pass runs first for all groups; then the mat-vec and finalize run
+// in chunks of groups from the top group down, and as soon as a chunk's
+// packed ciphertexts are final its Horner steps run on the lane's Horner
+// stream, which resumes the chain from the accumulators of the previous
+// chunk (kept in the lane's codec buffer, unused until the pipeline ends).
+// The chain consumes groups from the top (acc = packed[G - 1], then
+// i = G - 2 .. 0), so it follows the DB pass instead of waiting for all of
+// it.  Same kernels and the same arithmetic: identical responses.  The
+// mat-vec keeps every SM: its tiles are handed out from a counter, so a
+// Horner cluster that takes a few SMs first only shifts their tiles to the
+// other CTAs (keeping SMs free for the clusters measured no faster).
+// lwe_ready / rgsw_ready (optional): the blocking path's copies, on other
+// streams, of the LWE vectors (the mat-vec waits) and of the prepared RGSW
+// parts (the first Horner chunk waits).  qprep_parts as run_db_phase's.
+static int run_chunked(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st,
+                       cudaEvent_t lwe_ready = nullptr, cudaEvent_t rgsw_ready = nullptr, int qprep_parts = 3) {
+    const Params& pp = S.pp;
+    const Precomp& P = *S.pre;
+    const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
+    const int nq = (int)count;
+    int launches = 0;
+    IPB_CK(launch_qprep_parts(L.qraw, S.qstride, R, P.tables, L.keys, L.rgsw32, nq, qprep_parts, st));
+    ++launches;
+    for (size_t c0 = 0; c0 < count; c0 += (size_t)sc.tp_pass) {
+        const int n = (int)std::min<size_t>((size_t)sc.tp_pass, count - c0);
+        IPB_CK(launch_tensor_pass(P.pre_dt, G, L.keys + c0 * kKeyStride, kKeyStride, n, nq, (int)c0, L.keyt,
+                                  L.tp_out, L.d_err, L.tiles + 1, S.num_sms, st));
+        launches += 2;
+    }
+    if (lwe_ready) IPB_CK(cudaStreamWaitEvent(st, lwe_ready, 0));
+    IPB_CK(launch_qplanes(L.qraw, S.qstride, R, P.tables, L.planes, nq, st));
+    ++launches;
+    const size_t nc = std::min<size_t>(std::min<size_t>((size_t)sc.hchunks, kMaxHChunks), G);
+    const size_t per = (G + nc - 1) / nc;
+    IPB_CK(cudaEventRecord(L.hjoin, st));               // the Horner stream starts after this batch's prep
+    IPB_CK(cudaStreamWaitEvent(L.hstream, L.hjoin, 0));
+    if (rgsw_ready) IPB_CK(cudaStreamWaitEvent(L.hstream, rgsw_ready, 0));
+    const size_t d_act = std::min(pp.D, G);
+    uint32_t* state = L.codec_tmp;
+    for (size_t c = 0; c < nc; ++c) {
+        const size_t hi = G - c * per, lo = hi > per ? hi - per : 0;
+        IPB_CK(launch_matvec_tc_range(P.db, R, C, lo * kN, hi * kN, L.planes, nq, P.tables, L.mvpart, S.mv_qstride,
+                                      nullptr, L.d_err, L.tiles, S.num_sms, S.tc_kchunk_rows, st));
+        IPB_CK(launch_finalize_range(L.mvpart, S.mv_qstride, S.tc_kchunks, C, L.tp_out, nq, 0, P.pre_df, L.keys,
+                                     kKeyStride, P.tables, L.packed_b, S.pb_qstride, G, lo, hi - lo, nq, st));
+        IPB_CK(cudaEventRecord(L.hev[c], st));
+        IPB_CK(cudaStreamWaitEvent(L.hstream, L.hev[c], 0));
+        HornerRange hr;
+        hr.i_first = c == 0 ? -1 : (long)hi - 1;
+        hr.i_last = (long)lo;
+        hr.state = state;
+        if (sc.horner_cluster == 2)
+            IPB_CK(launch_horner_cluster8(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, 1, L.resp,
+                                          S.resp_qstride, nq, L.d_err, L.hstream, hr));
+        else
+            IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, 1, L.resp,
+                                         S.resp_qstride, nq, L.d_err, L.hstream, hr));
+        launches += 3;
+    }
+    IPB_CK(cudaEventRecord(L.hjoin, L.hstream));
+    IPB_CK(cudaStreamWaitEvent(st, L.hjoin, 0));
+    return launches;
+}
+
 void enqueue_horner(const Server& S, const Sched& sc, const uint32_t* packed_b, const uint32_t* rgsw32,
                     uint64_t* resp, size_t count, int* err, cudaStream_t st) {
     const Params& pp = S.pp;
@@ -546,6 +622,9 @@ int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaSt
     if (count > L.cap || sc.tp_pass < 1 || sc.tp_pass > L.gt_pass)
         throw std::invalid_argument("run_pipeline: batch exceeds the lane or its tensor-pass buffer");
     const size_t ns = slices_of(count, sc), slice = sc.slice > 0 ? (size_t)sc.slice : count;
+    // Stage timing needs the stages one after the other: it times the
+    // unchunked pipeline.
+    if (phases == kPhaseAll && !ev && chunked_ok(S, sc, count)) return run_chunked(S, L, sc, count, st);
     if (phases != kPhaseAll || 6 * ns > n_ev) ev = nullptr;
     int launches = 0;
     // Slices run one after the other, each its own pipeline on its lane
@@ -603,6 +682,10 @@ static void stage_and_run(Server* S, const ipir_query_view* qs, size_t count) {
     IPB_CK(cudaEventRecord(L.rgsw_ready, L.aux));
     S->staged = count;
     S->launches += 1;
+    if (chunked_ok(*S, sc, count)) {
+        S->launches += (unsigned long long)run_chunked(*S, L, sc, count, S->stream, L.join, L.rgsw_ready, 1);
+        return;
+    }
     // The first slice's key side starts before the LWE vectors land; every
     // slice's RGSW parts were prepared on the second stream above.
     const size_t ns = slices_of(count, sc), slice = sc.slice > 0 ? (size_t)sc.slice : count;
@@ -734,6 +817,30 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
                         b = std::min(b, time_of(split));
                     }
                     if (b < a * 0.97f) pick = split;
+                }
+            }
+            // Then the Horner chain trailing the DB pass in chunks, kept only
+            // if it beats the pick by 2 % in an interleaved head-to-head.
+            {
+                Sched ch = pick;
+                float ch_ms = 1e30f;
+                for (int k : {2, 4, 8}) {
+                    Sched c = pick;
+                    c.hchunks = k;
+                    if (!chunked_ok(S, c, b)) break;
+                    const float ms = time_of(c);
+                    if (ms < ch_ms) {
+                        ch_ms = ms;
+                        ch = c;
+                    }
+                }
+                if (ch.hchunks > 1) {
+                    float a = 1e30f, bb = 1e30f;
+                    for (int r = 0; r < 3; ++r) {
+                        a = std::min(a, time_of(pick));
+                        bb = std::min(bb, time_of(ch));
+                    }
+                    if (bb < a * 0.98f) pick = ch;
                 }
             }
             best.emplace_back(b, pick);
@@ -1166,6 +1273,7 @@ int ipir_b200_get_schedule(const ipir_server* srv, size_t count, ipir_serve_sche
     out->horner_cluster = sc.horner_cluster;
     out->tp_sms = sc.tp_sms;
     out->slice = sc.slice;
+    out->hchunks = sc.hchunks;
     return 0;
 }
 
@@ -1175,13 +1283,14 @@ int ipir_b200_set_schedule(ipir_server* srv, size_t count, const ipir_serve_sche
     if (count == 0 || count > S->max_batch) return 2;
     if (sc->matvec_tc < 0 || sc->matvec_tc > 1 || sc->horner_cluster < 0 || sc->horner_cluster > 2 ||
         sc->tp_pass < 1 || sc->tp_pass > S->lane.gt_pass || sc->tp_sms < 0 || sc->tp_sms >= S->num_sms ||
-        (sc->tp_sms > 0 && !sc->matvec_tc) || (sc->slice != 0 && sc->slice != (int)ipb::kSliceQueries)) {
+        (sc->tp_sms > 0 && !sc->matvec_tc) || (sc->slice != 0 && sc->slice != (int)ipb::kSliceQueries) ||
+        sc->hchunks < 0 || sc->hchunks > ipb::kMaxHChunks) {
         ipb::g_last_error =
             "ipir_b200_set_schedule: matvec_tc 0/1, horner_cluster 0/1/2, tp_pass 1..capacity, "
-            "tp_sms 0..SMs-1 (0 with the CUDA-core mat-vec), slice 0/32";
+            "tp_sms 0..SMs-1 (0 with the CUDA-core mat-vec), slice 0/32, hchunks 0..8";
         return 2;
     }
-    S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster, sc->tp_sms, sc->slice};
+    S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster, sc->tp_sms, sc->slice, sc->hchunks};
     return 0;
 }
 

@@ -107,7 +107,12 @@ struct Sched {
     int slice = 32;          // > 0: a batch larger than this runs as consecutive slices of this many
                              // queries, each its own pipeline (query prep .. Horner) on the lane's slots;
                              // 0: the whole batch in one pipeline
+    int hchunks = 0;         // > 1: the tensor pass first, then the mat-vec and finalize in this many group
+                             // chunks from the top group down, each chunk's Horner steps on a second
+                             // stream as soon as it is final (one ciphertext, cluster Horner, tensor-core
+                             // mat-vec, one slice); 0: off
 };
+constexpr int kMaxHChunks = 8;
 
 // Queries per slice a batch is cut into (one DB pass of the tensor-core
 // mat-vec serves at most this many) and the slices a batch of c needs.
@@ -138,7 +143,14 @@ struct Lane {
     cudaStream_t aux = nullptr;     // second stream: the tensor pass beside the mat-vec
     cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t rgsw_ready = nullptr;  // RGSW parts staged and prepared on aux
+    cudaStream_t hstream = nullptr;    // Horner chunks trailing the DB pass (Sched::hchunks)
+    cudaEvent_t hjoin = nullptr;
+    cudaEvent_t hev[8] = {};           // chunk c's packed ciphertexts are final
     ~Lane() {
+        for (auto& e : hev)
+            if (e) cudaEventDestroy(e);
+        if (hjoin) cudaEventDestroy(hjoin);
+        if (hstream) cudaStreamDestroy(hstream);
         if (rgsw_ready) cudaEventDestroy(rgsw_ready);
         if (join) cudaEventDestroy(join);
         if (fork) cudaEventDestroy(fork);

@@ -95,7 +95,7 @@ _L.ipir_b200_matvec_noalloc.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_
 
 class IpirSchedule(C.Structure):
     _fields_ = [("matvec_tc", C.c_int), ("tp_pass", C.c_int), ("horner_cluster", C.c_int), ("tp_sms", C.c_int),
-                ("slice", C.c_int)]
+                ("slice", C.c_int), ("hchunks", C.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -435,13 +435,15 @@ class Server:
             raise InspireError(f"get_schedule rc={rc}")
         return s.as_dict()
 
-    def set_schedule(self, count, matvec_tc=1, tp_pass=None, horner_cluster=1, tp_sms=0, slice=32):
+    def set_schedule(self, count, matvec_tc=1, tp_pass=None, horner_cluster=1, tp_sms=0, slice=32, hchunks=0):
         """Pin the kernel schedule for batches of `count` queries (tp_sms > 0:
         tensor pass on that many SMs beside the mat-vec; slice 32: batches of
-        more than 32 run as consecutive 32-query pipelines, 0: one pipeline)."""
+        more than 32 run as consecutive 32-query pipelines, 0: one pipeline;
+        hchunks 2..8: the Horner chain trails the DB pass in that many group
+        chunks)."""
         self._check()
         s = IpirSchedule(matvec_tc, tp_pass if tp_pass is not None else self.schedule(count)["tp_pass"],
-                         horner_cluster, tp_sms, slice)
+                         horner_cluster, tp_sms, slice, hchunks)
         rc = _L.ipir_b200_set_schedule(self._h, count, C.byref(s))
         if rc:
             raise InspireError(f"set_schedule rc={rc}: {last_error()}")
