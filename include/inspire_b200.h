@@ -252,9 +252,10 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
  * others (the two read disjoint data: the tensor pass is DRAM-bound, the
  * batched mat-vec tensor-core-bound), 0 runs them one after the other;
  * slice = 32 runs a batch of more than 32 queries as consecutive 32-query
- * pipelines (query prep to Horner), 0 as one pipeline; hchunks = 2..8 runs
- * the tensor pass first and then the mat-vec and finalize in that many
- * group chunks from the top group down, each chunk's Horner steps on a
+ * pipelines (query prep to Horner), 0 as one pipeline; hchunks = 2..16
+ * runs the tensor pass first and then the mat-vec and finalize in at most
+ * that many group chunks (whole waves of mat-vec work) from the top group
+ * down, each chunk's Horner steps on a
  * second stream as soon as its packed ciphertexts are final (databases of
  * one response ciphertext, cluster Horner kernels, batches of at most 32;
  * the blocking and staged paths, not the serving loop's split phases), 0

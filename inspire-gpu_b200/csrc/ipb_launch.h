@@ -35,6 +35,8 @@ cudaError_t launch_matvec(const uint16_t* db, size_t rows, size_t cols, int chun
 size_t mv_tc_planes_bytes(size_t rows, int max_queries);
 size_t mv_tc_planes_offset(size_t first_query, size_t rows);
 int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms);
+// DB columns per mat-vec work item (one m' tile of lo and hi bytes).
+int matvec_tc_item_cols();
 cudaError_t launch_qplanes(const uint64_t* qraw, size_t qstride, size_t rows, const DevTables* T,
                            uint8_t* planes, int nq, cudaStream_t s);
 // tiles: a device counter the launch zeroes and the kernel's CTAs draw work

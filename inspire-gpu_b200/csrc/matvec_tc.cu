@@ -367,6 +367,8 @@ cudaError_t launch_qplanes(const uint64_t* qraw, size_t qstride, size_t rows, co
 }
 
 // nq <= 32 queries whose planes start at `planes` (rows bytes per plane row).
+int matvec_tc_item_cols() { return kMT / 2; }
+
 int matvec_tc_kchunk_rows(size_t rows, size_t cols, int num_sms) {
     // Rows per exact s32 accumulation: at most 32768, halved while the
     // (m'-tile, chunk) work items would leave SMs idle.

@@ -488,18 +488,42 @@ static bool chunked_ok(const Server& S, const Sched& sc, size_t count) {
            S.pp.n_packed <= S.pp.D && count <= kSliceQueries && S.pp.n_packed >= 2;
 }
 
+// Group chunks of the chunked pipeline, top chunk first, at most `cap`.  A
+// chunk's Horner steps run beside the next chunk's DB pass, where the chain
+// takes about 11 us per group (2.5 times its rate alone: its loads meet a
+// saturated memory system) against the DB pass's 18 us per group at 16 GB,
+// and the last chunk's steps follow the DB pass.  So the chunks are whole
+// waves of mat-vec work items (floor(w x groups per wave) groups; a partial
+// wave costs nearly a whole one, since the persistent mat-vec's last items
+// set its end), one wave at the bottom and one wave more per chunk going
+// up, at most four, the top chunk taking the rest: at 128 groups and 148
+// SMs 37 + 37 + 27 + 18 + 9 (14 waves, as many as one unchunked pass).
+static std::vector<size_t> chunk_sizes(size_t G, size_t ipg, int num_sms, size_t cap) {
+    const double per_wave = (double)num_sms / (double)ipg;
+    std::vector<size_t> up;  // bottom chunk first
+    size_t rest = G;
+    for (size_t w = 1; rest > 0 && up.size() + 1 < cap; w = std::min<size_t>(w + 1, 4)) {
+        const size_t n = std::min(rest, std::max<size_t>(1, (size_t)((double)w * per_wave)));
+        up.push_back(n);
+        rest -= n;
+    }
+    if (rest > 0) up.push_back(rest);
+    return std::vector<size_t>(up.rbegin(), up.rend());
+}
+
 // The plain pipeline with the Horner chain trailing the DB pass.  The
 // tensor pass runs first for all groups; then the mat-vec and finalize run
-// in chunks of groups from the top group down, and as soon as a chunk's
-// packed ciphertexts are final its Horner steps run on the lane's Horner
-// stream, which resumes the chain from the accumulators of the previous
-// chunk (kept in the lane's codec buffer, unused until the pipeline ends).
-// The chain consumes groups from the top (acc = packed[G - 1], then
-// i = G - 2 .. 0), so it follows the DB pass instead of waiting for all of
-// it.  Same kernels and the same arithmetic: identical responses.  The
-// mat-vec keeps every SM: its tiles are handed out from a counter, so a
-// Horner cluster that takes a few SMs first only shifts their tiles to the
-// other CTAs (keeping SMs free for the clusters measured no faster).
+// in chunks of groups (chunk_sizes) from the top group down, and as soon as
+// a chunk's packed ciphertexts are final its Horner steps run on the lane's
+// Horner stream, which resumes the chain from the accumulators of the
+// previous chunk (kept in the lane's codec buffer, unused until the
+// pipeline ends).  The chain consumes groups from the top (acc =
+// packed[G - 1], then i = G - 2 .. 0), so it follows the DB pass instead of
+// waiting for all of it.  Same kernels and the same arithmetic: identical
+// responses.  The mat-vec keeps every SM: its tiles are handed out from a
+// counter, so a Horner cluster that takes a few SMs first only shifts their
+// tiles to the other CTAs (keeping SMs free for the clusters measured no
+// faster).
 // lwe_ready / rgsw_ready (optional): the blocking path's copies, on other
 // streams, of the LWE vectors (the mat-vec waits) and of the prepared RGSW
 // parts (the first Horner chunk waits).  qprep_parts as run_db_phase's.
@@ -521,15 +545,17 @@ static int run_chunked(const Server& S, Lane& L, const Sched& sc, size_t count, 
     if (lwe_ready) IPB_CK(cudaStreamWaitEvent(st, lwe_ready, 0));
     IPB_CK(launch_qplanes(L.qraw, S.qstride, R, P.tables, L.planes, nq, st));
     ++launches;
-    const size_t nc = std::min<size_t>(std::min<size_t>((size_t)sc.hchunks, kMaxHChunks), G);
-    const size_t per = (G + nc - 1) / nc;
+    const size_t ipg = (kN / (size_t)matvec_tc_item_cols()) * (size_t)S.tc_kchunks;
+    const std::vector<size_t> sizes =
+        chunk_sizes(G, ipg, S.num_sms, std::min<size_t>((size_t)sc.hchunks, kMaxHChunks));
     IPB_CK(cudaEventRecord(L.hjoin, st));               // the Horner stream starts after this batch's prep
     IPB_CK(cudaStreamWaitEvent(L.hstream, L.hjoin, 0));
     if (rgsw_ready) IPB_CK(cudaStreamWaitEvent(L.hstream, rgsw_ready, 0));
     const size_t d_act = std::min(pp.D, G);
     uint32_t* state = L.codec_tmp;
-    for (size_t c = 0; c < nc; ++c) {
-        const size_t hi = G - c * per, lo = hi > per ? hi - per : 0;
+    size_t hi = G;
+    for (size_t c = 0; c < sizes.size(); hi -= sizes[c], ++c) {
+        const size_t lo = hi - sizes[c];
         IPB_CK(launch_matvec_tc_range(P.db, R, C, lo * kN, hi * kN, L.planes, nq, P.tables, L.mvpart, S.mv_qstride,
                                       nullptr, L.d_err, L.tiles, S.num_sms, S.tc_kchunk_rows, st));
         IPB_CK(launch_finalize_range(L.mvpart, S.mv_qstride, S.tc_kchunks, C, L.tp_out, nq, 0, P.pre_df, L.keys,
@@ -824,7 +850,7 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
             {
                 Sched ch = pick;
                 float ch_ms = 1e30f;
-                for (int k : {2, 4, 8}) {
+                for (int k : {3, 8}) {
                     Sched c = pick;
                     c.hchunks = k;
                     if (!chunked_ok(S, c, b)) break;
@@ -1287,7 +1313,7 @@ int ipir_b200_set_schedule(ipir_server* srv, size_t count, const ipir_serve_sche
         sc->hchunks < 0 || sc->hchunks > ipb::kMaxHChunks) {
         ipb::g_last_error =
             "ipir_b200_set_schedule: matvec_tc 0/1, horner_cluster 0/1/2, tp_pass 1..capacity, "
-            "tp_sms 0..SMs-1 (0 with the CUDA-core mat-vec), slice 0/32, hchunks 0..8";
+            "tp_sms 0..SMs-1 (0 with the CUDA-core mat-vec), slice 0/32, hchunks 0..16";
         return 2;
     }
     S->sched[count] = ipb::Sched{sc->matvec_tc, sc->tp_pass, sc->horner_cluster, sc->tp_sms, sc->slice, sc->hchunks};

@@ -112,7 +112,7 @@ struct Sched {
                              // stream as soon as it is final (one ciphertext, cluster Horner, tensor-core
                              // mat-vec, one slice); 0: off
 };
-constexpr int kMaxHChunks = 8;
+constexpr int kMaxHChunks = 16;
 
 // Queries per slice a batch is cut into (one DB pass of the tensor-core
 // mat-vec serves at most this many) and the slices a batch of c needs.
@@ -145,7 +145,7 @@ struct Lane {
     cudaEvent_t rgsw_ready = nullptr;  // RGSW parts staged and prepared on aux
     cudaStream_t hstream = nullptr;    // Horner chunks trailing the DB pass (Sched::hchunks)
     cudaEvent_t hjoin = nullptr;
-    cudaEvent_t hev[8] = {};           // chunk c's packed ciphertexts are final
+    cudaEvent_t hev[kMaxHChunks] = {};  // chunk c's packed ciphertexts are final
     ~Lane() {
         for (auto& e : hev)
             if (e) cudaEventDestroy(e);

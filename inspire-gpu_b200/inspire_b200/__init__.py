@@ -439,8 +439,8 @@ class Server:
         """Pin the kernel schedule for batches of `count` queries (tp_sms > 0:
         tensor pass on that many SMs beside the mat-vec; slice 32: batches of
         more than 32 run as consecutive 32-query pipelines, 0: one pipeline;
-        hchunks 2..8: the Horner chain trails the DB pass in that many group
-        chunks)."""
+        hchunks 2..16: the Horner chain trails the DB pass in at most that
+        many group chunks)."""
         self._check()
         s = IpirSchedule(matvec_tc, tp_pass if tp_pass is not None else self.schedule(count)["tp_pass"],
                          horner_cluster, tp_sms, slice, hchunks)
