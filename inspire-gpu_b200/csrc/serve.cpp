@@ -169,15 +169,24 @@ void Engine::issue(DbState& d, LaneRun& r) {
     IPB_CK(cudaSetDevice(S.device));
     IPB_CK(cudaEventRecord(r.ev_start, r.st));
     for (size_t i = 0; i < n; ++i) stage_query_flat(S, L, i, slots[r.slots[i]].q, r.st);
-    if (use_graphs)
-        IPB_CK(cudaGraphLaunch(r.graphs_db[n], r.st));
-    else
-        run_pipeline(S, L, d.sched[n], n, r.st, nullptr, kPhaseDb);
-    IPB_CK(cudaEventRecord(r.ev_db, r.st));
-    if (use_graphs)
-        IPB_CK(cudaGraphLaunch(r.graphs_horner[n], r.st));
-    else
-        run_pipeline(S, L, d.sched[n], n, r.st, nullptr, kPhaseHorner);
+    if (runs_chunked(S, d.sched[n], n)) {
+        // One pipeline with the Horner chain trailing the DB pass in chunks;
+        // ev_db is recorded inside, after the last chunk's finalize.
+        if (use_graphs)
+            IPB_CK(cudaGraphLaunch(r.graphs_db[n], r.st));
+        else
+            run_pipeline(S, L, d.sched[n], n, r.st, nullptr, kPhaseAll, 6, r.ev_db);
+    } else {
+        if (use_graphs)
+            IPB_CK(cudaGraphLaunch(r.graphs_db[n], r.st));
+        else
+            run_pipeline(S, L, d.sched[n], n, r.st, nullptr, kPhaseDb);
+        IPB_CK(cudaEventRecord(r.ev_db, r.st));
+        if (use_graphs)
+            IPB_CK(cudaGraphLaunch(r.graphs_horner[n], r.st));
+        else
+            run_pipeline(S, L, d.sched[n], n, r.st, nullptr, kPhaseHorner);
+    }
     const size_t rb = S.resp_qstride * 8;
     for (size_t i = 0; i < n; ++i)
         IPB_CK(cudaMemcpyAsync(slots[r.slots[i]].resp, L.resp + i * S.resp_qstride, rb, cudaMemcpyDeviceToHost,
@@ -577,11 +586,11 @@ Engine::~Engine() {
     if (pinned_err) cudaFreeHost(pinned_err);
 }
 
-cudaGraphExec_t capture_phase(DbState& d, LaneRun& r, size_t c, int phase) {
+cudaGraphExec_t capture_phase(DbState& d, LaneRun& r, size_t c, int phase, cudaEvent_t db_done = nullptr) {
     cudaGraph_t g = nullptr;
     IPB_CK(cudaStreamBeginCapture(r.st, cudaStreamCaptureModeThreadLocal));
     try {
-        run_pipeline(*d.S, r.lane, d.sched[c], c, r.st, nullptr, phase);
+        run_pipeline(*d.S, r.lane, d.sched[c], c, r.st, nullptr, phase, 6, db_done);
     } catch (...) {
         cudaStreamEndCapture(r.st, &g);
         if (g) cudaGraphDestroy(g);
@@ -605,8 +614,12 @@ void capture_graphs(DbState& d, LaneRun& r, bool warm = true) {
     for (size_t c = 1; c <= d.max_batch; ++c) {
         // An eager run first: kernel attributes are set outside the capture.
         if (warm) run_pipeline(*d.S, r.lane, d.sched[c], c, r.st, nullptr);
-        r.graphs_db[c] = capture_phase(d, r, c, kPhaseDb);
-        r.graphs_horner[c] = capture_phase(d, r, c, kPhaseHorner);
+        if (runs_chunked(*d.S, d.sched[c], c)) {
+            r.graphs_db[c] = capture_phase(d, r, c, kPhaseAll, r.ev_db);  // the whole chunked pipeline
+        } else {
+            r.graphs_db[c] = capture_phase(d, r, c, kPhaseDb);
+            r.graphs_horner[c] = capture_phase(d, r, c, kPhaseHorner);
+        }
     }
     IPB_CK(cudaStreamSynchronize(r.st));
 }

@@ -388,6 +388,7 @@ std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
         def.horner_cluster = std::strcmp(h, "cta") == 0 ? 0 : (std::strcmp(h, "cl8") == 0 ? 2 : 1);
     if (const char* t = std::getenv("IPB_TP_SMS"))
         def.tp_sms = def.matvec_tc ? std::max(0, std::min(std::atoi(t), S.num_sms - 1)) : 0;
+    if (const char* h = std::getenv("IPB_HCHUNKS")) def.hchunks = std::max(0, std::min(std::atoi(h), kMaxHChunks));
     return std::vector<Sched>(cap + 1, def);
 }
 
@@ -488,6 +489,16 @@ static bool chunked_ok(const Server& S, const Sched& sc, size_t count) {
            S.pp.n_packed <= S.pp.D && count <= kSliceQueries && S.pp.n_packed >= 2;
 }
 
+bool runs_chunked(const Server& S, const Sched& sc, size_t count) { return chunked_ok(S, sc, count); }
+
+// An event record that becomes an external event node (observable outside
+// the graph) when st is being captured.
+static void record_outside(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    IPB_CK(cudaStreamIsCapturing(st, &cs));
+    IPB_CK(cudaEventRecordWithFlags(e, st, cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0));
+}
+
 // Group chunks of the chunked pipeline, top chunk first, at most `cap`.  A
 // chunk's Horner steps run beside the next chunk's DB pass, where the chain
 // takes about 11 us per group (2.5 times its rate alone: its loads meet a
@@ -528,7 +539,8 @@ static std::vector<size_t> chunk_sizes(size_t G, size_t ipg, int num_sms, size_t
 // streams, of the LWE vectors (the mat-vec waits) and of the prepared RGSW
 // parts (the first Horner chunk waits).  qprep_parts as run_db_phase's.
 static int run_chunked(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st,
-                       cudaEvent_t lwe_ready = nullptr, cudaEvent_t rgsw_ready = nullptr, int qprep_parts = 3) {
+                       cudaEvent_t lwe_ready = nullptr, cudaEvent_t rgsw_ready = nullptr, int qprep_parts = 3,
+                       cudaEvent_t db_done = nullptr) {
     const Params& pp = S.pp;
     const Precomp& P = *S.pre;
     const size_t R = pp.db_rows, C = pp.db_cols, G = pp.n_packed;
@@ -574,6 +586,7 @@ static int run_chunked(const Server& S, Lane& L, const Sched& sc, size_t count, 
                                          S.resp_qstride, nq, L.d_err, L.hstream, hr));
         launches += 3;
     }
+    if (db_done) record_outside(db_done, st);
     IPB_CK(cudaEventRecord(L.hjoin, L.hstream));
     IPB_CK(cudaStreamWaitEvent(st, L.hjoin, 0));
     return launches;
@@ -643,14 +656,15 @@ void enqueue_scan_finalize(const Server& S, Lane& L, const SlotRun& r, cudaStrea
 }
 
 int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
-                 int phases, size_t n_ev) {
+                 int phases, size_t n_ev, cudaEvent_t db_done) {
     if (count == 0) return 0;
     if (count > L.cap || sc.tp_pass < 1 || sc.tp_pass > L.gt_pass)
         throw std::invalid_argument("run_pipeline: batch exceeds the lane or its tensor-pass buffer");
     const size_t ns = slices_of(count, sc), slice = sc.slice > 0 ? (size_t)sc.slice : count;
     // Stage timing needs the stages one after the other: it times the
     // unchunked pipeline.
-    if (phases == kPhaseAll && !ev && chunked_ok(S, sc, count)) return run_chunked(S, L, sc, count, st);
+    if (phases == kPhaseAll && !ev && chunked_ok(S, sc, count))
+        return run_chunked(S, L, sc, count, st, nullptr, nullptr, 3, db_done);
     if (phases != kPhaseAll || 6 * ns > n_ev) ev = nullptr;
     int launches = 0;
     // Slices run one after the other, each its own pipeline on its lane
@@ -669,6 +683,7 @@ int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaSt
             const size_t q0 = k * slice;
             launches += run_horner_phase(S, L, sc, q0, std::min(slice, count - q0), st, ev ? ev + 6 * k : nullptr);
         }
+    if (db_done) record_outside(db_done, st);  // unchunked: at the end (slices interleave the phases)
     return launches;
 }
 

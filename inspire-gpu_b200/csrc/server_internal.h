@@ -204,8 +204,15 @@ constexpr int kPhaseDb = 1, kPhaseHorner = 2, kPhaseAll = 3;
 // ev (6 stage events, used when all phases run) or null.
 // ev holds n_ev events: 6 per slice (fewer than the batch's slices need: no
 // stage events are recorded).
+// db_done (optional): recorded once the DB-bound part is done (after the
+// last finalize when the Horner chain trails the DB pass in chunks, else at
+// the end), as an external event node under stream capture.
 int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaStream_t st, cudaEvent_t* ev,
-                 int phases = kPhaseAll, size_t n_ev = 6);
+                 int phases = kPhaseAll, size_t n_ev = 6, cudaEvent_t db_done = nullptr);
+// Whether the pipeline for `count` queries under sc runs with the Horner
+// chain trailing the DB pass in group chunks (then the DB and Horner phases
+// cannot be run apart).
+bool runs_chunked(const Server& S, const Sched& sc, size_t count);
 // The DB-bound phase (query prep, mat-vec, tensor pass, finalize) of lane
 // slots [q_off, q_off + count) on st: packed ciphertext b parts into
 // L.packed_b.  lwe_ready: an event the mat-vec waits for (the key side runs

@@ -132,6 +132,25 @@ def test_tensor_pass_beside_matvec_in_graphs(env, monkeypatch):
         assert stats["failed"] == 0
 
 
+def test_chunked_horner_in_lanes(env, monkeypatch):
+    """Schedules whose Horner chain trails the DB pass in group chunks run
+    each lane batch as one pipeline (one graph per batch size, the DB-done
+    event recorded inside it after the last chunk's finalize); with graph
+    replay and with direct launches every response equals the plain single
+    answer."""
+    import inspire_b200 as ib
+    ca, cb, sa, sb, reqs, alone = env
+    monkeypatch.setenv("IPB_HCHUNKS", "8")
+    monkeypatch.setenv("IPB_HORNER", "cl8")
+    for graphs in (True, False):
+        out, stats, info = _run_mix(ib, [sa, sb], reqs, random.Random(13), max_batch=4, lanes_per_db=2,
+                                    graphs=graphs, autotune=False)
+        assert all(s["hchunks"] == 8 for db in info for s in db["schedule"].values())
+        for i in range(len(reqs)):
+            assert (out[i] == alone[i]).all(), (graphs, i)
+        assert stats["failed"] == 0
+
+
 def test_slot_and_ticket_codes(env):
     import inspire_b200 as ib
     ca, cb, sa, sb, reqs, alone = env
