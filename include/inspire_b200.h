@@ -255,11 +255,12 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
  * pipelines (query prep to Horner), 0 as one pipeline; hchunks = 2..16
  * runs the tensor pass first and then the mat-vec and finalize in at most
  * that many group chunks (whole waves of mat-vec work) from the top group
- * down, each chunk's Horner steps on a
- * second stream as soon as its packed ciphertexts are final (databases of
- * one response ciphertext, cluster Horner kernels, batches of at most 32;
- * the blocking and staged paths, not the serving loop's split phases), 0
- * off.  Every schedule gives the same responses. */
+ * down, each chunk's Horner steps on a second stream as soon as its packed
+ * ciphertexts are final (databases of one response ciphertext, cluster
+ * Horner kernels, batches of at most 32; the blocking and staged paths and
+ * the serving loop's lane batches), 0 off; the default schedule uses 8 for
+ * batches of up to 16 where the database allows it.  Every schedule gives
+ * the same responses. */
 typedef struct {
     int matvec_tc;
     int tp_pass;

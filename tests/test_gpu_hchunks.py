@@ -70,6 +70,29 @@ def test_chunked_horner_equals_unchunked(name, idx, chunks):
         srv.close()
 
 
+def test_chunked_full_pass_of_32_queries():
+    """32 queries at 128 groups (one whole mat-vec pass, 32 chains of 4- or
+    8-CTA clusters trailing it, 29 leaving a ragged last block): chunked
+    equals unchunked for both cluster kernels."""
+    import inspire_b200 as ib
+    c = get_case("g128")
+    idx = [int(i) for i in np.random.default_rng(21).integers(0, c.n_entries, 32)]
+    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=32, crs_seed=c.seed)
+    try:
+        qs = [c.query(i, 7400 + k)[0] for k, i in enumerate(idx)]
+        for n in (29, 32):
+            srv.set_schedule(n, matvec_tc=1, horner_cluster=1)
+        want = srv.answer_batch(qs)
+        assert (srv.answer_batch(qs[:29]) == want[:29]).all()
+        for hc in (1, 2):
+            for n in (29, 32):
+                srv.set_schedule(n, matvec_tc=1, horner_cluster=hc, hchunks=8)
+            assert (srv.answer_batch(qs) == want).all(), hc
+            assert (_staged(ib, srv, qs[:29]) == want[:29]).all(), hc
+    finally:
+        srv.close()
+
+
 def test_chunking_ignored_where_it_does_not_apply():
     """The one-CTA Horner kernel, the tensor pass beside the mat-vec and the
     CUDA-core mat-vec do not chunk: with hchunks set they run the plain
