@@ -258,9 +258,9 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
  * down, each chunk's Horner steps on a second stream as soon as its packed
  * ciphertexts are final (databases of one response ciphertext, cluster
  * Horner kernels, batches of at most 32; the blocking and staged paths and
- * the serving loop's lane batches), 0 off; the default schedule uses 8 for
- * batches of up to 16 where the database allows it.  Every schedule gives
- * the same responses. */
+ * the serving loop's lane batches), 0 off; the default schedule uses 8 on
+ * such databases of G >= 32 groups for batches of at most min(16, G / 16)
+ * queries.  Every schedule gives the same responses. */
 typedef struct {
     int matvec_tc;
     int tp_pass;

@@ -391,14 +391,18 @@ std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
     if (const char* t = std::getenv("IPB_TP_SMS"))
         def.tp_sms = def.matvec_tc ? std::max(0, std::min(std::atoi(t), S.num_sms - 1)) : 0;
     std::vector<Sched> out(cap + 1, def);
-    // The Horner chain trails the DB pass in chunks by default for batches
-    // of up to 16 where the geometry allows it (at 16 GB it measured 2-8 %
-    // faster from 1 to 16 queries with both cluster kernels, and never
-    // slower); IPB_HCHUNKS sets it for every batch size.
+    // The Horner chain trails the DB pass in chunks by default where the
+    // geometry allows it, the chain is long enough to matter (at least 32
+    // groups) and the batch has at most G / 16 queries (at most 16): the
+    // hidden chain then outweighs the extra launches.  Measured: 128 groups
+    // 2-8 % faster from 1 to 16 queries; 32 groups 4.5 % faster at 1 query
+    // and 1 % slower at 8; 8 groups 4-9 % slower.  IPB_HCHUNKS sets it for
+    // every batch size.
+    const size_t G = S.pp.n_packed;
     for (size_t c = 1; c <= cap; ++c) {
         Sched probe = def;
         probe.hchunks = 8;
-        if (c <= 16 && chunked_ok(S, probe, c)) out[c].hchunks = 8;
+        if (G >= 32 && c <= std::min<size_t>(16, G / 16) && chunked_ok(S, probe, c)) out[c].hchunks = 8;
     }
     if (const char* h = std::getenv("IPB_HCHUNKS"))
         for (auto& sc : out) sc.hchunks = std::max(0, std::min(std::atoi(h), kMaxHChunks));
