@@ -256,11 +256,11 @@ int ipir_b200_fill_db_device(uint16_t* out, size_t count, uint64_t seed, void* s
  * runs the tensor pass first and then the mat-vec and finalize in at most
  * that many group chunks (whole waves of mat-vec work) from the top group
  * down, each chunk's Horner steps on a second stream as soon as its packed
- * ciphertexts are final (databases of one response ciphertext, cluster
- * Horner kernels, batches of at most 32; the blocking and staged paths and
- * the serving loop's lane batches), 0 off; the default schedule uses 8 on
- * such databases of G >= 32 groups for batches of at most min(16, G / 16)
- * queries.  Every schedule gives the same responses. */
+ * ciphertexts are final (databases whose response ciphertexts all chain
+ * the same number of groups L = min(D, G), cluster Horner kernels, batches
+ * of at most 32; the blocking and staged paths and the serving loop's lane
+ * batches), 0 off; the default schedule uses 8 on such databases with
+ * L >= 32 for batches of at most min(16, L / 16) queries.  Every schedule gives the same responses. */
 typedef struct {
     int matvec_tc;
     int tp_pass;

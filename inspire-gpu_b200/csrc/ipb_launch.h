@@ -52,6 +52,13 @@ cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, s
                                    const uint8_t* planes, int nq, const DevTables* T, uint32_t* part,
                                    size_t part_qstride, const uint8_t* qmap, int* err, unsigned* tiles, int num_sms,
                                    int kchunk_rows, cudaStream_t s);
+// The same over n_ranges column ranges of cols_per_range columns, range r
+// starting at c0 + r * range_stride, in one launch (one work-item counter,
+// so the ranges share the SMs); partial sums land at their own columns.
+cudaError_t launch_matvec_tc_ranges(const uint16_t* db, size_t rows, size_t ld, size_t c0, size_t cols_per_range,
+                                    int n_ranges, size_t range_stride, const uint8_t* planes, int nq,
+                                    const DevTables* T, uint32_t* part, size_t part_qstride, const uint8_t* qmap,
+                                    int* err, unsigned* tiles, int num_sms, int kchunk_rows, cudaStream_t s);
 
 // out[q][limb][cols] = sum over chunks of part[q][chunk][limb][cols] mod q.
 cudaError_t launch_mv_chunk_reduce(const uint32_t* part, size_t part_qstride, int chunks, size_t cols,

@@ -60,6 +60,9 @@ struct TcParams {
     int npad;              // N = 16 ceil(7 nq / 16) (<= 224)
     uint32_t c[2][kPlanes];  // 256^k mod q_l
     int n_mtiles;
+    int mt_per_range;      // > 0: the m' tiles cover ranges of this many tiles, range r starting
+    int range_stride_m;    // r * range_stride_m m' rows after the first (several column ranges in one
+                           // launch); 0: one contiguous range
     int n_kchunks;
     int kchunk_rows;
     int stages;
@@ -73,6 +76,13 @@ struct TcParams {
     int abort_after;       // > 0: the MMA issuer stops after this many items and reports code 99 (a test of
                            // the abort path, IPB_TEST_ABORT_AFTER_ITEMS); 0: off
 };
+
+// First m' row (2 x column, relative to the launch's first column) of m'
+// tile mt: tiles of one contiguous range, or of several equal ranges
+// range_stride_m apart.
+__device__ __forceinline__ int mtile_m0(const TcParams& P, int mt) {
+    return P.mt_per_range ? (mt / P.mt_per_range) * P.range_stride_m + (mt % P.mt_per_range) * kMT : mt * kMT;
+}
 
 __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ CUtensorMap map_a,
                                                        const __grid_constant__ CUtensorMap map_b, TcParams P) {
@@ -133,7 +143,7 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
                 mbar_arrive(&ifull[r]);
                 if (item < 0) break;
                 const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
-                const int m0 = mt * kMT;
+                const int m0 = mtile_m0(P, mt);
                 for (int kt = 0; kt < ktiles; ++kt) {
                     if (!mbar_wait_ab(&empty[s], ph ^ 1, P.err, 1, &abort_flag)) { abort_flag = 1; break; }
                     uint8_t* st = smem + (size_t)s * stage_bytes;
@@ -225,8 +235,9 @@ __global__ void __launch_bounds__(256, 1) mv_tc_kernel(const __grid_constant__ C
             if (!mbar_wait_ab(&tfull[as], aph, P.err, 5, &abort_flag)) { abort_flag = 1; break; }
             tc_fence_after();
             const int mt = item % P.n_mtiles, kc = item / P.n_mtiles;
+            const int m0 = mtile_m0(P, mt);
             for (int mb = 0; mb < 2; ++mb) {
-                const size_t j = ((size_t)mt * kMT + mb * 128 + wq * 32 + lane) >> 1;
+                const size_t j = ((size_t)m0 + mb * 128 + wq * 32 + lane) >> 1;
                 for (int q0 = 0; q0 < P.nq; q0 += 8) {
                     // queries q0..q0+7: columns 7 q0 .. 7 q0 + 55, seven 8-column
                     // loads (those at or past N are not loaded: they hold no query)
@@ -389,9 +400,22 @@ cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, s
                                    const uint8_t* planes, int nq, const DevTables* T, uint32_t* part,
                                    size_t part_qstride, const uint8_t* qmap, int* err, unsigned* tiles, int num_sms,
                                    int kchunk_rows, cudaStream_t s) {
+    if (c1 <= c0) return nq <= 0 ? cudaSuccess : cudaErrorInvalidValue;
+    return launch_matvec_tc_ranges(db, rows, ld, c0, c1 - c0, 1, 0, planes, nq, T, part, part_qstride, qmap, err,
+                                   tiles, num_sms, kchunk_rows, s);
+}
+
+cudaError_t launch_matvec_tc_ranges(const uint16_t* db, size_t rows, size_t ld, size_t c0, size_t cols_per_range,
+                                    int n_ranges, size_t range_stride, const uint8_t* planes, int nq,
+                                    const DevTables* T, uint32_t* part, size_t part_qstride, const uint8_t* qmap,
+                                    int* err, unsigned* tiles, int num_sms, int kchunk_rows, cudaStream_t s) {
     if (nq <= 0) return cudaSuccess;
-    if (c1 <= c0 || c1 > ld || c0 % 128) return cudaErrorInvalidValue;
-    const size_t cols = c1 - c0;
+    if (n_ranges < 1 || cols_per_range == 0 || cols_per_range % 128 || c0 % 128 ||
+        (n_ranges > 1 && (range_stride < cols_per_range || range_stride % 128)))
+        return cudaErrorInvalidValue;
+    // the launch's columns span [c0, c0 + cols): the ranges and the gaps between them
+    const size_t cols = (size_t)(n_ranges - 1) * range_stride + cols_per_range;
+    if (c0 + cols > ld) return cudaErrorInvalidValue;
     db += c0;
     part += c0;
     if (nq > 32 || rows % kKT || cols % 128 || !tiles) return cudaErrorInvalidValue;
@@ -439,7 +463,9 @@ cudaError_t launch_matvec_tc_range(const uint16_t* db, size_t rows, size_t ld, s
             for (int k = 0; k < kPlanes; ++k, c = c * 256 % qs[l]) P.c[l][k] = (uint32_t)c;
         }
     }
-    P.n_mtiles = (int)((2 * cols) / kMT);
+    P.mt_per_range = n_ranges > 1 ? (int)((2 * cols_per_range) / kMT) : 0;
+    P.range_stride_m = n_ranges > 1 ? (int)(2 * range_stride) : 0;
+    P.n_mtiles = n_ranges > 1 ? n_ranges * P.mt_per_range : (int)((2 * cols) / kMT);
     P.kchunk_rows = kchunk;
     P.n_kchunks = (int)(rows / kchunk);
     P.acc_stages = (4 * npad <= 512) ? 2 : 1;

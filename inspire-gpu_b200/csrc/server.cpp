@@ -393,16 +393,17 @@ std::vector<Sched> default_sched(const Server& S, size_t cap, int gt_pass) {
     std::vector<Sched> out(cap + 1, def);
     // The Horner chain trails the DB pass in chunks by default where the
     // geometry allows it, the chain is long enough to matter (at least 32
-    // groups) and the batch has at most G / 16 queries (at most 16): the
-    // hidden chain then outweighs the extra launches.  Measured: 128 groups
+    // groups per response ciphertext) and the batch has at most chain / 16
+    // queries (at most 16): the hidden chain then outweighs the extra
+    // launches.  Measured: 128 groups
     // 2-8 % faster from 1 to 16 queries; 32 groups 4.5 % faster at 1 query
     // and 1 % slower at 8; 8 groups 4-9 % slower.  IPB_HCHUNKS sets it for
     // every batch size.
-    const size_t G = S.pp.n_packed;
+    const size_t chain = std::min(S.pp.D, S.pp.n_packed);  // groups per response ciphertext
     for (size_t c = 1; c <= cap; ++c) {
         Sched probe = def;
         probe.hchunks = 8;
-        if (G >= 32 && c <= std::min<size_t>(16, G / 16) && chunked_ok(S, probe, c)) out[c].hchunks = 8;
+        if (chain >= 32 && c <= std::min<size_t>(16, chain / 16) && chunked_ok(S, probe, c)) out[c].hchunks = 8;
     }
     if (const char* h = std::getenv("IPB_HCHUNKS"))
         for (auto& sc : out) sc.hchunks = std::max(0, std::min(std::atoi(h), kMaxHChunks));
@@ -499,11 +500,14 @@ static int run_horner_phase(const Server& S, Lane& L, const Sched& sc, size_t q_
 }
 
 // Whether a batch of `count` can run with its Horner chunks trailing the DB
-// pass (Sched::hchunks): one ciphertext, one slice, the tensor-core mat-vec
-// and a cluster Horner kernel (those resume a chain from memory).
+// pass (Sched::hchunks): every response ciphertext's chain of the same
+// length (one ciphertext, or G a multiple of D), one slice, the tensor-core
+// mat-vec and a cluster Horner kernel (those resume a chain from memory).
 static bool chunked_ok(const Server& S, const Sched& sc, size_t count) {
-    return sc.hchunks > 1 && sc.matvec_tc && sc.horner_cluster != 0 && sc.tp_sms == 0 && S.pp.num_cts == 1 &&
-           S.pp.n_packed <= S.pp.D && count <= kSliceQueries && S.pp.n_packed >= 2;
+    const size_t G = S.pp.n_packed, d_act = std::min(S.pp.D, G);
+    // every response ciphertext's chain covers d_act >= 2 groups (no short last one)
+    return sc.hchunks > 1 && sc.matvec_tc && sc.horner_cluster != 0 && sc.tp_sms == 0 &&
+           G == S.pp.num_cts * d_act && d_act >= 2 && count <= kSliceQueries;
 }
 
 bool runs_chunked(const Server& S, const Sched& sc, size_t count) { return chunked_ok(S, sc, count); }
@@ -574,21 +578,29 @@ static int run_chunked(const Server& S, Lane& L, const Sched& sc, size_t count, 
     if (lwe_ready) IPB_CK(cudaStreamWaitEvent(st, lwe_ready, 0));
     IPB_CK(launch_qplanes(L.qraw, S.qstride, R, P.tables, L.planes, nq, st));
     ++launches;
-    const size_t ipg = (kN / (size_t)matvec_tc_item_cols()) * (size_t)S.tc_kchunks;
+    // Chunks are ranges [lo, hi) of chain positions, the same in every
+    // response ciphertext (ciphertext t's groups t * d_act + [lo, hi)): one
+    // mat-vec launch covers the range in all of them.
+    const size_t nct = pp.num_cts, d_act = std::min(pp.D, G);
+    const size_t ipg = (kN / (size_t)matvec_tc_item_cols()) * (size_t)S.tc_kchunks * nct;
     const std::vector<size_t> sizes =
-        chunk_sizes(G, ipg, S.num_sms, std::min<size_t>((size_t)sc.hchunks, kMaxHChunks));
+        chunk_sizes(d_act, ipg, S.num_sms, std::min<size_t>((size_t)sc.hchunks, kMaxHChunks));
     IPB_CK(cudaEventRecord(L.hjoin, st));               // the Horner stream starts after this batch's prep
     IPB_CK(cudaStreamWaitEvent(L.hstream, L.hjoin, 0));
     if (rgsw_ready) IPB_CK(cudaStreamWaitEvent(L.hstream, rgsw_ready, 0));
-    const size_t d_act = std::min(pp.D, G);
     uint32_t* state = L.codec_tmp;
-    size_t hi = G;
+    size_t hi = d_act;
     for (size_t c = 0; c < sizes.size(); hi -= sizes[c], ++c) {
         const size_t lo = hi - sizes[c];
-        IPB_CK(launch_matvec_tc_range(P.db, R, C, lo * kN, hi * kN, L.planes, nq, P.tables, L.mvpart, S.mv_qstride,
-                                      nullptr, L.d_err, L.tiles, S.num_sms, S.tc_kchunk_rows, st));
-        IPB_CK(launch_finalize_range(L.mvpart, S.mv_qstride, S.tc_kchunks, C, L.tp_out, nq, 0, P.pre_df, L.keys,
-                                     kKeyStride, P.tables, L.packed_b, S.pb_qstride, G, lo, hi - lo, nq, st));
+        IPB_CK(launch_matvec_tc_ranges(P.db, R, C, lo * kN, (hi - lo) * kN, (int)nct, d_act * kN, L.planes, nq,
+                                       P.tables, L.mvpart, S.mv_qstride, nullptr, L.d_err, L.tiles, S.num_sms,
+                                       S.tc_kchunk_rows, st));
+        for (size_t t = 0; t < nct; ++t) {
+            IPB_CK(launch_finalize_range(L.mvpart, S.mv_qstride, S.tc_kchunks, C, L.tp_out, nq, 0, P.pre_df, L.keys,
+                                         kKeyStride, P.tables, L.packed_b, S.pb_qstride, G, t * d_act + lo, hi - lo,
+                                         nq, st));
+            ++launches;
+        }
         IPB_CK(cudaEventRecord(L.hev[c], st));
         IPB_CK(cudaStreamWaitEvent(L.hstream, L.hev[c], 0));
         HornerRange hr;
@@ -596,12 +608,12 @@ static int run_chunked(const Server& S, Lane& L, const Sched& sc, size_t count, 
         hr.i_last = (long)lo;
         hr.state = state;
         if (sc.horner_cluster == 2)
-            IPB_CK(launch_horner_cluster8(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, 1, L.resp,
-                                          S.resp_qstride, nq, L.d_err, L.hstream, hr));
+            IPB_CK(launch_horner_cluster8(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, nct,
+                                          L.resp, S.resp_qstride, nq, L.d_err, L.hstream, hr));
         else
-            IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, 1, L.resp,
-                                         S.resp_qstride, nq, L.d_err, L.hstream, hr));
-        launches += 3;
+            IPB_CK(launch_horner_cluster(P.pre_a, L.packed_b, S.pb_qstride, L.rgsw32, P.tables, G, d_act, nct,
+                                         L.resp, S.resp_qstride, nq, L.d_err, L.hstream, hr));
+        launches += 2;
     }
     if (db_done) record_outside(db_done, st);
     IPB_CK(cudaEventRecord(L.hjoin, L.hstream));

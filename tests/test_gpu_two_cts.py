@@ -52,3 +52,26 @@ def test_two_ciphertexts_wire_formats(env):
         assert (got_p[i] == c.r.wire(p, "ipir_response_pack", want[i], "ipir_response_packed_bytes")).all(), i
         assert (got_c[i] == c.r.wire(p, "ipir_response_compress", want[i], "ipir_response_compressed_bytes")).all(), i
         assert (st.extract_compressed(got_c[i]) == c.expected_slots(idx)).all(), i
+
+
+def test_two_ciphertexts_chunked_horner(env):
+    """The Horner chains trailing the DB pass in chunks with two response
+    ciphertexts: each chunk is the same range of chain positions in both
+    (one mat-vec launch over the two column ranges), both chains resume
+    from memory; every chunking and both cluster kernels give the
+    unchunked responses."""
+    c, srv, qs, sts = env
+    for n in (1, 3):
+        srv.set_schedule(n, matvec_tc=1, horner_cluster=1)
+    want = srv.answer_batch(qs)
+    assert (srv.answer(qs[1]) == want[1]).all()
+    for hc in (1, 2):
+        for k in (2, 3, 8):
+            for n in (1, 3):
+                srv.set_schedule(n, matvec_tc=1, horner_cluster=hc, hchunks=k)
+            assert (srv.answer_batch(qs) == want).all(), (hc, k)
+            assert (srv.answer(qs[1]) == want[1]).all(), (hc, k)
+    for i, st in enumerate(sts):
+        assert (st.extract(want[i]) == c.expected_slots(IDX[i])).all(), i
+    for n in (1, 3):
+        srv.set_schedule(n, matvec_tc=1, horner_cluster=1)
