@@ -74,3 +74,45 @@ def test_answer_abort_writes_nothing_and_recovers(abort_hook):
             assert (out[k] == c.oracle_answer(qs[k])).all(), k
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("hc", [1, 2])
+def test_chunked_pipeline_abort_writes_nothing_and_recovers(abort_hook, hc):
+    """The same with the Horner chain trailing the DB pass in chunks (128
+    groups, 8 chunks): the mat-vec and tensor-pass launches stop early while
+    the Horner stream keeps consuming chunks; the blocking answer and the
+    staged path both report the error with nothing written, and the next
+    calls without the hook give the unchunked answers."""
+    import inspire_b200 as ib
+    c = get_case("g128")
+    srv = ib.Server(c.n_entries, c.w, c.db, db_rows=2048, max_batch=2, crs_seed=c.seed)
+    try:
+        os.environ.pop("IPB_TEST_ABORT_AFTER_ITEMS")
+        qs = [c.query(i, 8200 + k)[0] for k, i in enumerate([9, 8000000])]
+        for n in (1, 2):
+            srv.set_schedule(n, matvec_tc=1, horner_cluster=hc)
+        want = srv.answer_batch(qs)
+        for n in (1, 2):
+            srv.set_schedule(n, matvec_tc=1, horner_cluster=hc, hchunks=8)
+        views = (ib.IpirQueryView * 2)()
+        keep = [np.ascontiguousarray(x) for x in qs]
+        for i, f in enumerate(keep):
+            views[i] = ib.query_view_from_flat(srv.params, f)
+        out = np.full((2, ib.response_u64s(srv.params)), 7, np.uint64)
+        os.environ["IPB_TEST_ABORT_AFTER_ITEMS"] = "2"
+        t0 = time.perf_counter()
+        assert srv.answer_batch_rc(views, 2, out) == 4
+        assert "code 99" in ib.last_error()
+        assert (out == 7).all()
+        srv.stage_views(views, 1)
+        srv.run(1)
+        with pytest.raises(ib.InspireError):
+            srv.fetch(1, out[:1])
+        assert (out == 7).all()
+        assert time.perf_counter() - t0 < 40.0
+        os.environ.pop("IPB_TEST_ABORT_AFTER_ITEMS")
+        assert srv.answer_batch_rc(views, 2, out) == 0
+        assert (out == want).all()
+        assert (srv.answer(qs[1]) == want[1]).all()
+    finally:
+        srv.close()
