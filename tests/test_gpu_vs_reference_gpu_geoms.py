@@ -105,6 +105,15 @@ def test_geometry_bit_exact_vs_reference_gpu(refgpu, name):
             got = srv.answer_batch(qs[:b])
             bad = [k for k in range(b) if not np.array_equal(got[k], want[k])]
             assert not bad, f"{name}: B={b} responses {bad[:8]} differ from the reference GPU server"
+        # the Horner chain trailing the DB pass in chunks, whatever the
+        # autotuner picked: 8 chunks with each cluster Horner kernel
+        for hc in (1, 2):
+            for b in (1, 8):
+                srv.set_schedule(b, matvec_tc=1, horner_cluster=hc, hchunks=8)
+            assert np.array_equal(srv.answer(qs[0]), want[0]), f"{name}: chunked B=1 (Horner kernel {hc})"
+            got = srv.answer_batch(qs[:8])
+            bad = [k for k in range(8) if not np.array_equal(got[k], want[k])]
+            assert not bad, f"{name}: chunked B=8 (Horner kernel {hc}) responses {bad} differ"
     finally:
         srv.close()
     for k, st in enumerate(sts):
