@@ -349,7 +349,10 @@ typedef struct {
                                 columns split into this many multiples of 128: its DB and tensor
                                 passes run as that many segments in rotation on one lane of up to 32
                                 queries, and waiting requests join at the next segment instead of
-                                the next whole pass (default 0: lane batches) */
+                                the next whole pass (default 0: lane batches); < 0: chosen per
+                                database at create from its plain answer's device time (cyclic
+                                scan from 2 ms, in the power of two of segments nearest to that
+                                time in ms, 2 to 16; lane batches below) */
 } ipir_serve_config;
 
 typedef struct {

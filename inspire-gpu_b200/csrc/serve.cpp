@@ -116,6 +116,7 @@ struct ScanState {
 
 struct DbState {
     Server* S = nullptr;
+    size_t scan_ns = 0;               // > 1: cyclic scan in this many segments, else lane batches
     std::unique_ptr<ScanState> scan;  // cyclic scan mode, else lane batches
     size_t max_batch = 0;
     std::vector<Sched> sched;
@@ -706,15 +707,26 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
             // Cyclic scan for databases whose columns split into scan_segments
             // parts of whole 128-column tiles (the tensor pass splits its
             // 2N (limb, slot) indices the same way, in multiples of 32).
-            const size_t ns = cfg.scan_segments > 1 ? (size_t)cfg.scan_segments : 0;
-            auto scan_ok = [&](const ipb::Server& S) {
+            // scan_segments < 0: per database, from its own plain answer.
+            auto splits = [](const ipb::Server& S, size_t ns) {
                 return ns > 1 && S.pp.db_cols % (128 * ns) == 0 && (2 * ipb::kN) % (32 * ns) == 0;
             };
+            for (auto& dp : E->dbs) {
+                ipb::DbState& d = *dp;
+                if (cfg.scan_segments > 1) {
+                    d.scan_ns = splits(*d.S, (size_t)cfg.scan_segments) ? (size_t)cfg.scan_segments : 0;
+                } else if (cfg.scan_segments < 0) {
+                    size_t ns = ipb::auto_scan_segments(ipb::time_plain_answer(*d.S));
+                    while (ns > 1 && !splits(*d.S, ns)) ns /= 2;
+                    d.scan_ns = ns > 1 ? ns : 0;
+                }
+            }
+            auto scan_ok = [&](const ipb::DbState& d) { return d.scan_ns > 1; };
             size_t mb = cfg.max_batch, lanes = cfg.lanes_per_db;
             auto need = [&](size_t b, size_t l) {
                 size_t t = 0;
                 for (auto& d : E->dbs) {
-                    if (scan_ok(*d->S)) {
+                    if (scan_ok(*d)) {
                         const size_t c = std::min<size_t>(b, 32);
                         t += ipb::lane_bytes(*d->S, c, ipb::lane_gt_pass(*d->S, c)) + c * ipb::kKeyStride * 4;
                     } else {
@@ -731,7 +743,7 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
             size_t q_words = 0, r_words = 0;
             for (auto& dp : E->dbs) {
                 ipb::DbState& d = *dp;
-                const bool scan = scan_ok(*d.S);
+                const bool scan = scan_ok(d);
                 d.max_batch = scan ? std::min<size_t>(mb, 32) : mb;
                 q_words = std::max(q_words, d.S->qstride);
                 r_words = std::max(r_words, d.S->resp_qstride);
@@ -752,7 +764,7 @@ ipir_serve* ipir_serve_create(ipir_server* const* dbs, size_t n_dbs, const ipir_
                                        : ipb::default_sched(*d.S, d.max_batch, d.lanes[0]->lane.gt_pass);
                 if (scan) {
                     auto sc = std::make_unique<ipb::ScanState>();
-                    sc->ns = (int)ns;
+                    sc->ns = (int)d.scan_ns;
                     sc->cap = d.max_batch;
                     sc->used.assign(sc->cap, 0);
                     sc->keys_pos = d.lanes[0]->lane.arena.alloc<uint32_t>(sc->cap * ipb::kKeyStride);

@@ -512,6 +512,54 @@ static bool chunked_ok(const Server& S, const Sched& sc, size_t count) {
 
 bool runs_chunked(const Server& S, const Sched& sc, size_t count) { return chunked_ok(S, sc, count); }
 
+float time_plain_answer(Server& S) {
+    IPB_CK(cudaSetDevice(S.device));
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    IPB_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    float best = 1e30f;
+    try {
+        IPB_CK(cudaEventCreate(&e0));
+        IPB_CK(cudaEventCreate(&e1));
+        IPB_CK(cudaStreamSynchronize(S.stream));  // the lane's last use is done
+        const Sched& sc = sched_for(S, 1);
+        run_pipeline(S, S.lane, sc, 1, st, nullptr);  // warm
+        for (int r = 0; r < 3; ++r) {
+            IPB_CK(cudaEventRecord(e0, st));
+            run_pipeline(S, S.lane, sc, 1, st, nullptr);
+            IPB_CK(cudaEventRecord(e1, st));
+            IPB_CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            IPB_CK(cudaEventElapsedTime(&ms, e0, e1));
+            best = std::min(best, ms);
+        }
+    } catch (...) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        cudaStreamDestroy(st);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    return best;
+}
+
+size_t auto_scan_segments(float ms) {
+    // A database whose plain answer takes at least 2 ms (IPB_SCAN_AUTO_MS
+    // overrides the threshold) joins requests at segments of about 1 ms:
+    // the power of two nearest to ms / 1 ms, 2 .. 16.  Measured: the 16 GB
+    // database (about 4 ms) serves with a p99 of 1.6-1.7 plain answers in 4
+    // segments at 3 and 5 times the plain rate, while 1 GB databases (0.4-0.5
+    // ms) keep a lower median on lane batches (0.49 vs 0.67 ms).
+    float threshold = 2.0f;
+    if (const char* t = std::getenv("IPB_SCAN_AUTO_MS")) threshold = (float)std::atof(t);
+    if (!(ms >= threshold)) return 0;
+    size_t ns = 2;
+    while (ns < 16 && (float)(2 * ns) <= ms * 1.41421356f) ns *= 2;
+    return ns;
+}
+
 // An event record that becomes an external event node (observable outside
 // the graph) when st is being captured.
 static void record_outside(cudaEvent_t e, cudaStream_t st) {

@@ -213,6 +213,12 @@ int run_pipeline(const Server& S, Lane& L, const Sched& sc, size_t count, cudaSt
 // chain trailing the DB pass in group chunks (then the DB and Horner phases
 // cannot be run apart).
 bool runs_chunked(const Server& S, const Sched& sc, size_t count);
+// Device time (ms, best of three after one warm run) of one plain answer
+// through the handle's own lane and schedule, on a stream of its own.
+float time_plain_answer(Server& S);
+// Cyclic-scan segment count the serving loop picks for a database whose
+// plain answer takes `ms` (0: lane batches); see serve.cpp.
+size_t auto_scan_segments(float ms);
 // The DB-bound phase (query prep, mat-vec, tensor pass, finalize) of lane
 // slots [q_off, q_off + count) on st: packed ciphertext b parts into
 // L.packed_b.  lwe_ready: an event the mat-vec waits for (the key side runs

@@ -481,7 +481,8 @@ class ServeLoop:
     ipir_serve_* entry points): submit() returns a ticket at once; poll() /
     wait() collect the response and its submit-to-response latency.
     scan_segments > 1: cyclic scan (requests join the running rotation of
-    DB-pass segments) for the databases whose groups split that way."""
+    DB-pass segments) for the databases whose groups split that way; < 0:
+    per database, cyclic scan when its plain answer takes 2 ms or more."""
 
     def __init__(self, servers, max_batch=0, lanes_per_db=0, queue_slots=0, hbm_budget_bytes=0,
                  graphs=True, autotune=True, overlap_db_passes=False, scan_segments=0):

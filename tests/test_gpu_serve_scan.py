@@ -88,6 +88,22 @@ def test_segments_that_do_not_split_fall_back_to_lanes(env):
         assert (out[i] == singles[i]).all(), i
 
 
+@pytest.mark.parametrize("threshold_ms,scan", [("0", True), ("1000", False)])
+def test_auto_scan_choice(env, monkeypatch, threshold_ms, scan):
+    """scan_segments < 0: the loop times each database's plain answer at
+    create and serves it by cyclic scan from a threshold (2 ms, here moved
+    by IPB_SCAN_AUTO_MS to 0 and to 1000 ms) and by lane batches below;
+    either way every response equals the plain single answer."""
+    ib, c, srv, idxs, qs, sts, singles = env
+    monkeypatch.setenv("IPB_SCAN_AUTO_MS", threshold_ms)
+    out, stats, info, _ = _serve(ib, srv, qs[:8], random.Random(17), True, max_batch=8, lanes_per_db=2,
+                                 queue_slots=32, autotune=False, scan_segments=-1)
+    assert info["lanes"] == (1 if scan else 2)
+    for i in range(8):
+        assert (out[i] == singles[i]).all(), (threshold_ms, i)
+    assert stats["failed"] == 0
+
+
 def test_scan_packed_slots_and_generation_swap():
     """G = 4: the tensor pass packs eight (limb, slot) items into one 128-row
     tile, so each segment's slot range is whole packed items.  Scan responses
