@@ -90,7 +90,8 @@ def parse():
     ap.add_argument("--serve-scan", type=int, default=None,
                     help="cyclic scan: DB and tensor passes as this many segments in rotation, requests join "
                          "at the next segment (databases whose columns split into multiples of 128); 0: lane "
-                         "batches; default 4 for --serve-config 16gb, 0 for mixed (the faster of each)")
+                         "batches; -1: chosen per database from its plain answer (scan from 2 ms); default 4 "
+                         "for --serve-config 16gb, 0 for mixed (the faster of each)")
     return ap.parse_args()
 
 
