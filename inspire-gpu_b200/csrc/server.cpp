@@ -937,28 +937,28 @@ std::vector<Sched> autotune(const Server& S, Lane& L, cudaStream_t st) {
                     if (b < a * 0.97f) pick = split;
                 }
             }
-            // Then the Horner chain trailing the DB pass in chunks, kept only
-            // if it beats the pick by 2 % in an interleaved head-to-head.
+            // Then the Horner chain trailing the DB pass in chunks (at most 8,
+            // the schedule that measured best) with either cluster kernel:
+            // the best unchunked kernel need not be the best chunked one.
+            // Kept only if it beats the pick by 2 % in an interleaved
+            // head-to-head.
             {
-                Sched ch = pick;
-                float ch_ms = 1e30f;
-                for (int k : {3, 8}) {
+                std::vector<Sched> chs;
+                for (int hc : {1, 2}) {
                     Sched c = pick;
-                    c.hchunks = k;
-                    if (!chunked_ok(S, c, b)) break;
-                    const float ms = time_of(c);
-                    if (ms < ch_ms) {
-                        ch_ms = ms;
-                        ch = c;
-                    }
+                    c.horner_cluster = hc;
+                    c.hchunks = 8;
+                    if (chunked_ok(S, c, b)) chs.push_back(c);
                 }
-                if (ch.hchunks > 1) {
-                    float a = 1e30f, bb = 1e30f;
+                if (!chs.empty()) {
+                    float a = 1e30f;
+                    std::vector<float> t(chs.size(), 1e30f);
                     for (int r = 0; r < 3; ++r) {
                         a = std::min(a, time_of(pick));
-                        bb = std::min(bb, time_of(ch));
+                        for (size_t i = 0; i < chs.size(); ++i) t[i] = std::min(t[i], time_of(chs[i]));
                     }
-                    if (bb < a * 0.98f) pick = ch;
+                    const size_t i = (size_t)(std::min_element(t.begin(), t.end()) - t.begin());
+                    if (t[i] < a * 0.98f) pick = chs[i];
                 }
             }
             best.emplace_back(b, pick);
