@@ -107,10 +107,10 @@ struct Sched {
     int slice = 32;          // > 0: a batch larger than this runs as consecutive slices of this many
                              // queries, each its own pipeline (query prep .. Horner) on the lane's slots;
                              // 0: the whole batch in one pipeline
-    int hchunks = 0;         // > 1: the tensor pass first, then the mat-vec and finalize in this many group
-                             // chunks from the top group down, each chunk's Horner steps on a second
-                             // stream as soon as it is final (one ciphertext, cluster Horner, tensor-core
-                             // mat-vec, one slice); 0: off
+    int hchunks = 0;         // > 1: the tensor pass first, then the mat-vec and finalize in at most this
+                             // many chunks of chain positions from the top down, each chunk's Horner steps
+                             // on a second stream as soon as it is final (every ciphertext's chain of
+                             // D_act groups, cluster Horner, tensor-core mat-vec, one slice); 0: off
 };
 constexpr int kMaxHChunks = 16;
 
